@@ -1,0 +1,74 @@
+// Device BFS state: the B200 counterpart of BasicIncrementalBFS<DynamicGraph>
+// (include/velographx/incremental/bfs.hpp:13-383).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "graph.cuh"
+
+namespace vxh {
+
+struct BfsCounters {
+  unsigned long long reachable;   // finite distances
+  unsigned long long arcs;        // sum of out-degrees of reached vertices (full BFS)
+  uint32_t levels;
+  uint32_t candidates;            // last_deletion_candidates
+  uint32_t affected;              // last_affected_vertices
+  uint32_t full;                  // last_used_full_recompute
+  uint32_t fallback;              // fixpoint exceeded the fallback limit
+  uint32_t err;
+  // per-level counters of the persistent loops (3-way rotation)
+  uint32_t lvl_n[3];
+  uint32_t lvl_big[3];
+  unsigned long long lvl_m[3];
+  // repair bookkeeping
+  uint32_t cand_n;       // deletion candidates list length
+  uint32_t touched_n;    // vertices whose lost counter is non-zero
+  uint32_t a_n;          // affected list length
+  uint32_t list_n[3];    // rotating frontier lists of the repair loops
+  uint32_t next_seed[3]; // smallest pending seed level (rotating)
+  uint32_t seed_min;     // smallest seed level of the settle phase
+  uint32_t bar[2];       // grid barrier {arrive, generation}
+  uint32_t pad[2];
+};
+
+struct BfsTuning {
+  float alpha = 14.0f;       // top-down -> bottom-up when m_f * alpha > m_u
+  float beta = 24.0f;        // bottom-up -> top-down when n_f * beta < V (shrinking)
+  uint32_t large_row = 4096; // rows this long are expanded by the whole grid
+};
+
+struct Bfs {
+  Graph* g = nullptr;
+  uint32_t source = 0;
+  double frac = 0.35;
+  size_t dist_len = 0;  // the reference's dist_.size()
+  size_t cap = 0;       // allocated per-vertex capacity
+  uint32_t* dist = nullptr;
+  uint32_t* vis = nullptr;
+  uint32_t* fb[3] = {nullptr, nullptr, nullptr};
+  uint32_t* q[3] = {nullptr, nullptr, nullptr};
+  uint32_t* big = nullptr;
+  uint32_t* lst_a = nullptr;  // affected list
+  uint32_t* lst_t = nullptr;  // touched (lost > 0) list
+  uint32_t* old = nullptr;    // pre-repair distance of each affected entry
+  uint32_t* tent = nullptr;   // boundary seed distance of each affected entry
+  uint32_t* lost = nullptr;   // lost-parent counters (zero between batches)
+  uint32_t* aff = nullptr;    // affected bitmap (zero between batches)
+  uint32_t* inq[2] = {nullptr, nullptr};  // queued bitmaps of the decrease propagation
+  BfsCounters* ctr = nullptr;
+  BfsCounters* hctr = nullptr;
+  BfsTuning tune;
+  int grid = 0;
+};
+
+int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac);
+void bfs_destroy(Bfs* b);
+int bfs_recompute(Bfs* b);
+// Incremental apply of the batch staged in b->g->batch (ops already on device).
+int bfs_apply_staged(Bfs* b, size_t n, size_t vertex_bound);
+int bfs_sync(Bfs* b);  // copies counters to hctr (synchronises the stream)
+int bfs_reached_arcs(Bfs* b, unsigned long long* arcs);  // sum of degrees of reached vertices
+
+}  // namespace vxh

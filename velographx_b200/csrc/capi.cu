@@ -1,0 +1,313 @@
+// C ABI (include/vx_b200.h) over the device graph and BFS.
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/vx_b200.h"
+#include "bfs.cuh"
+#include "graph.cuh"
+
+namespace vxh {
+
+static thread_local char g_err[1024] = "";
+static std::atomic<uint64_t> g_launches{0};
+
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+}  // namespace vxh
+
+struct vx_graph {
+  vxh::Graph* g;
+};
+struct vx_bfs {
+  vxh::Bfs* b;
+  vx_graph* owner;
+};
+
+namespace {
+
+int fail(int code, const char* msg) {
+  vxh::set_error("%s", msg);
+  return code;
+}
+
+// Host batch -> device batch buffers; returns the vertex count after the batch.
+int upload_batch(vxh::Graph* g, const uint32_t* src, const uint32_t* dst, const uint8_t* add, size_t n,
+                 size_t* v_after) {
+  size_t vmax = g->V;
+  for (size_t i = 0; i < n; ++i) {
+    if (src[i] == dst[i]) continue;  // self-loops never grow the graph
+    const size_t m = (size_t)std::max(src[i], dst[i]) + 1;
+    if (m > vmax) vmax = m;
+  }
+  if (vmax > vxb::kMaxVertices) return fail(VX_ERR_RANGE, "vertex id beyond the supported maximum (2^31 - 1)");
+  if (int rc = g->batch.ensure(n)) return rc;
+  cudaStream_t s = g->stream;
+  VX_CUDA_TRY(cudaMemcpyAsync(g->batch.src, src, n * 4, cudaMemcpyHostToDevice, s));
+  VX_CUDA_TRY(cudaMemcpyAsync(g->batch.dst, dst, n * 4, cudaMemcpyHostToDevice, s));
+  VX_CUDA_TRY(cudaMemcpyAsync(g->batch.add, add, n, cudaMemcpyHostToDevice, s));
+  *v_after = vmax;
+  return 0;
+}
+
+int stage_device_batch(vxh::Graph* g, const uint32_t* d_src, const uint32_t* d_dst, const uint8_t* d_add, size_t n) {
+  if (int rc = g->batch.ensure(n)) return rc;
+  cudaStream_t s = g->stream;
+  VX_CUDA_TRY(cudaMemcpyAsync(g->batch.src, d_src, n * 4, cudaMemcpyDeviceToDevice, s));
+  VX_CUDA_TRY(cudaMemcpyAsync(g->batch.dst, d_dst, n * 4, cudaMemcpyDeviceToDevice, s));
+  VX_CUDA_TRY(cudaMemcpyAsync(g->batch.add, d_add, n, cudaMemcpyDeviceToDevice, s));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vx_last_error(char* buf, size_t cap) {
+  const size_t n = strlen(vxh::g_err);
+  if (buf && cap) {
+    const size_t m = std::min(n, cap - 1);
+    memcpy(buf, vxh::g_err, m);
+    buf[m] = 0;
+  }
+  return (int)n;
+}
+
+uint64_t vx_launch_count(void) { return vxh::g_launches.load(std::memory_order_relaxed); }
+
+int vx_graph_create(size_t vertices, int directed, vx_graph** out) {
+  if (!out) return fail(VX_ERR_INVALID, "null output pointer");
+  vxh::Graph* g = nullptr;
+  if (int rc = vxh::graph_create(&g, vertices, directed != 0)) return rc;
+  *out = new vx_graph{g};
+  return VX_OK;
+}
+
+int vx_graph_destroy(vx_graph* g) {
+  if (!g) return VX_OK;
+  vxh::graph_destroy(g->g);
+  delete g;
+  return VX_OK;
+}
+
+int vx_graph_vertex_count(vx_graph* g, size_t* out) {
+  if (!g || !out) return fail(VX_ERR_INVALID, "null argument");
+  *out = g->g->V;
+  return VX_OK;
+}
+
+int vx_graph_version(vx_graph* g, uint64_t* out) {
+  if (!g || !out) return fail(VX_ERR_INVALID, "null argument");
+  *out = g->g->version;
+  return VX_OK;
+}
+
+int vx_graph_directed(vx_graph* g, int* out) {
+  if (!g || !out) return fail(VX_ERR_INVALID, "null argument");
+  *out = g->g->directed ? 1 : 0;
+  return VX_OK;
+}
+
+int vx_graph_bulk_load(vx_graph* g, const uint32_t* uv, size_t n) {
+  if (!g || (!uv && n)) return fail(VX_ERR_INVALID, "null argument");
+  uint32_t* d = nullptr;
+  if (cudaMalloc(&d, std::max<size_t>(n, 1) * 8) != cudaSuccess) return fail(VX_ERR_NOMEM, "bulk load upload");
+  int rc = VX_OK;
+  if (n && cudaMemcpy(d, uv, n * 8, cudaMemcpyHostToDevice) != cudaSuccess) rc = fail(VX_ERR_CUDA, "bulk copy");
+  if (!rc) rc = vxh::graph_bulk_load(g->g, d, n);
+  cudaFree(d);
+  return rc;
+}
+
+int vx_graph_bulk_load_device(vx_graph* g, const uint32_t* d_uv, size_t n) {
+  if (!g || (!d_uv && n)) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::graph_bulk_load(g->g, d_uv, n);
+}
+
+int vx_graph_apply(vx_graph* g, const uint32_t* src, const uint32_t* dst, const uint8_t* add, size_t n) {
+  if (!g || (n && (!src || !dst || !add))) return fail(VX_ERR_INVALID, "null argument");
+  if (n == 0) return VX_OK;  // empty batch: no version bump (dynamic_graph.hpp:545)
+  size_t v_after = 0;
+  if (int rc = upload_batch(g->g, src, dst, add, n, &v_after)) return rc;
+  if (int rc = vxh::graph_stage_batch(g->g, n, v_after)) return rc;
+  return vxh::graph_commit_batch(g->g);
+}
+
+int vx_graph_apply_device(vx_graph* g, const uint32_t* d_src, const uint32_t* d_dst, const uint8_t* d_add, size_t n,
+                          size_t vertex_count_after) {
+  if (!g || (n && (!d_src || !d_dst || !d_add))) return fail(VX_ERR_INVALID, "null argument");
+  if (n == 0) return VX_OK;
+  if (vertex_count_after < g->g->V) return fail(VX_ERR_INVALID, "vertex_count_after below vertex_count");
+  if (int rc = stage_device_batch(g->g, d_src, d_dst, d_add, n)) return rc;
+  if (int rc = vxh::graph_stage_batch(g->g, n, vertex_count_after)) return rc;
+  return vxh::graph_commit_batch(g->g);
+}
+
+int vx_graph_neighbors(vx_graph* g, uint32_t u, uint32_t* out, size_t cap, size_t* n) {
+  if (!g || !n) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::graph_row(g->g, 0, u, out, cap, n);
+}
+
+int vx_graph_in_neighbors(vx_graph* g, uint32_t v, uint32_t* out, size_t cap, size_t* n) {
+  if (!g || !n) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::graph_row(g->g, 1, v, out, cap, n);
+}
+
+int vx_graph_has_edge(vx_graph* g, uint32_t u, uint32_t v, int* out) {
+  if (!g || !out) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::graph_has_edge(g->g, u, v, out);
+}
+
+int vx_graph_edge_count_directed(vx_graph* g, size_t* out) {
+  if (!g || !out) return fail(VX_ERR_INVALID, "null argument");
+  if (int rc = vxh::graph_sync_counters(g->g)) return rc;
+  *out = (size_t)vxh::graph_edge_count_directed(g->g);
+  return VX_OK;
+}
+
+int vx_graph_delta_edge_count(vx_graph* g, size_t* out) {
+  if (!g || !out) return fail(VX_ERR_INVALID, "null argument");
+  if (int rc = vxh::graph_sync_counters(g->g)) return rc;
+  *out = (size_t)(g->g->hctr->delta_live[0] + g->g->hctr->tombs[0]);
+  return VX_OK;
+}
+
+int vx_graph_is_compact(vx_graph* g, int* out) {
+  if (!g || !out) return fail(VX_ERR_INVALID, "null argument");
+  if (int rc = vxh::graph_sync_counters(g->g)) return rc;
+  const vxh::GraphCounters* c = g->g->hctr;
+  *out = (c->delta_live[0] + c->tombs[0] + c->delta_live[1] + c->tombs[1]) == 0;
+  return VX_OK;
+}
+
+int vx_graph_dirty_rows(vx_graph* g, size_t* out_rows, size_t* in_rows) {
+  if (!g || !out_rows || !in_rows) return fail(VX_ERR_INVALID, "null argument");
+  if (int rc = vxh::graph_sync_counters(g->g)) return rc;
+  *out_rows = (size_t)g->g->hctr->dirty_rows[0];
+  *in_rows = (size_t)g->g->hctr->dirty_rows[g->g->directed ? 1 : 0];
+  return VX_OK;
+}
+
+int vx_graph_compact(vx_graph* g) {
+  if (!g) return fail(VX_ERR_INVALID, "null argument");
+  int compact = 0;
+  if (int rc = vx_graph_is_compact(g, &compact)) return rc;
+  if (compact) return VX_OK;
+  return vxh::graph_consolidate(g->g);
+}
+
+int vx_graph_maybe_compact(vx_graph* g, double threshold, int* compacted) {
+  if (!g || !compacted) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::graph_maybe_compact(g->g, threshold, compacted);
+}
+
+int vx_graph_stream(vx_graph* g, void** stream) {
+  if (!g || !stream) return fail(VX_ERR_INVALID, "null argument");
+  *stream = (void*)g->g->stream;
+  return VX_OK;
+}
+
+int vx_graph_synchronize(vx_graph* g) {
+  if (!g) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::graph_sync_counters(g->g);
+}
+
+int vx_bfs_create(vx_graph* g, uint32_t source, double frac, vx_bfs** out) {
+  if (!g || !out) return fail(VX_ERR_INVALID, "null argument");
+  vxh::Bfs* b = nullptr;
+  if (int rc = vxh::bfs_create(&b, g->g, source, frac)) return rc;
+  *out = new vx_bfs{b, g};
+  return VX_OK;
+}
+
+int vx_bfs_destroy(vx_bfs* b) {
+  if (!b) return VX_OK;
+  vxh::bfs_destroy(b->b);
+  delete b;
+  return VX_OK;
+}
+
+int vx_bfs_recompute(vx_bfs* b) {
+  if (!b) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::bfs_recompute(b->b);
+}
+
+int vx_bfs_apply(vx_bfs* b, const uint32_t* src, const uint32_t* dst, const uint8_t* add, size_t n) {
+  if (!b || (n && (!src || !dst || !add))) return fail(VX_ERR_INVALID, "null argument");
+  vxh::Graph* g = b->b->g;
+  size_t v_after = g->V;
+  if (n)
+    if (int rc = upload_batch(g, src, dst, add, n, &v_after)) return rc;
+  return vxh::bfs_apply_staged(b->b, n, v_after);
+}
+
+int vx_bfs_apply_device(vx_bfs* b, const uint32_t* d_src, const uint32_t* d_dst, const uint8_t* d_add, size_t n,
+                        size_t vertex_count_after) {
+  if (!b || (n && (!d_src || !d_dst || !d_add))) return fail(VX_ERR_INVALID, "null argument");
+  vxh::Graph* g = b->b->g;
+  if (n) {
+    if (vertex_count_after < g->V) return fail(VX_ERR_INVALID, "vertex_count_after below vertex_count");
+    if (int rc = stage_device_batch(g, d_src, d_dst, d_add, n)) return rc;
+  }
+  return vxh::bfs_apply_staged(b->b, n, std::max<size_t>(vertex_count_after, g->V));
+}
+
+int vx_bfs_distances(vx_bfs* b, uint32_t* host_out, size_t cap, size_t* n) {
+  if (!b || !n) return fail(VX_ERR_INVALID, "null argument");
+  vxh::Bfs* x = b->b;
+  *n = x->dist_len;
+  const size_t m = std::min(cap, x->dist_len);
+  if (host_out && m) {
+    VX_CUDA_TRY(cudaMemcpyAsync(host_out, x->dist, m * 4, cudaMemcpyDeviceToHost, x->g->stream));
+  }
+  return vxh::bfs_sync(x);
+}
+
+int vx_bfs_distances_device(vx_bfs* b, const uint32_t** d_dist, size_t* n) {
+  if (!b || !d_dist || !n) return fail(VX_ERR_INVALID, "null argument");
+  *d_dist = b->b->dist;
+  *n = b->b->dist_len;
+  return VX_OK;
+}
+
+int vx_bfs_stats(vx_bfs* b, vx_bfs_stats_t* out) {
+  if (!b || !out) return fail(VX_ERR_INVALID, "null argument");
+  if (int rc = vxh::bfs_sync(b->b)) return rc;
+  const vxh::BfsCounters* c = b->b->hctr;
+  out->reachable_count = c->reachable;
+  out->last_deletion_candidates = c->candidates;
+  out->last_affected_vertices = c->affected;
+  out->last_used_full_recompute = c->full ? 1 : 0;
+  out->levels = c->levels;
+  out->readback_bytes = (uint32_t)sizeof(vxh::BfsCounters);
+  out->reserved = 0;
+  return VX_OK;
+}
+
+int vx_bfs_reached_arcs(vx_bfs* b, uint64_t* out) {
+  if (!b || !out) return fail(VX_ERR_INVALID, "null argument");
+  unsigned long long a = 0;
+  if (int rc = vxh::bfs_reached_arcs(b->b, &a)) return rc;
+  *out = a;
+  return VX_OK;
+}
+
+int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row) {
+  if (!b || !(alpha > 0.f) || !(beta > 0.f) || large_row < 32) return fail(VX_ERR_INVALID, "invalid tuning");
+  b->b->tune.alpha = alpha;
+  b->b->tune.beta = beta;
+  b->b->tune.large_row = large_row;
+  return VX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,169 @@
+// Shared definitions for the B200 dynamic-BFS library (sm_100a).
+//
+// Device graph layout (one "adjacency" per direction; an undirected graph uses
+// the same adjacency for out- and in-rows):
+//
+//   base CSR     off[Vb+1] (u64) + col[A] (u32).  Bit 31 of a column is the
+//                tombstone: a base arc deleted since the last consolidation.
+//                Rows are sorted by the low 31 bits.
+//   delta rows   drow[v] = {offset, count} into darena, dcap[v] = capacity.
+//                Each delta row is a sorted list of arcs present in the logical
+//                graph but absent from the base CSR.
+//
+// The logical row of u is (base row minus tombstones) U (delta row), which is
+// exactly the reference's base/patch row merged with its PackedDeltaStore
+// overlay (dynamic_graph.hpp:659-681): an overlay "absent" entry is our
+// tombstone, an overlay "present" entry is our delta entry.
+#pragma once
+
+#include <cstdint>
+#include <cstdio>
+#include <cuda_runtime.h>
+
+namespace vxb {
+
+constexpr uint32_t kUnreachable = 0xFFFFFFFFu;
+constexpr uint32_t kTomb = 0x80000000u;
+constexpr uint32_t kIdMask = 0x7FFFFFFFu;
+constexpr uint32_t kMaxVertices = 0x7FFFFFFFu;  // ids must leave bit 31 free
+
+// Device error word bits (VX_DEVERR_* in vx_b200.h mirror these).
+constexpr uint32_t kErrBarrierTimeout = 1u << 0;
+constexpr uint32_t kErrLoopBound = 1u << 1;
+constexpr uint32_t kErrArenaOverflow = 1u << 2;
+constexpr uint32_t kErrBadVertex = 1u << 3;
+constexpr uint32_t kErrQueueOverflow = 1u << 4;
+
+struct DevAdj {
+  const uint64_t* off;  // [Vb + 1]
+  uint32_t* col;        // [off[Vb]]
+  uint32_t Vb;          // vertices covered by the base CSR
+  uint2* drow;          // [Vcap] {offset, count}
+  uint32_t* dcap;       // [Vcap]
+  uint32_t* darena;     // delta arena
+  uint32_t* tcnt;       // [Vcap] tombstones per row
+  uint32_t* dirty;      // [Vcap/32] rows changed since the last consolidation
+};
+
+struct DevGraph {
+  DevAdj out;
+  DevAdj in;  // == out for undirected graphs
+  uint32_t V;
+  int directed;
+};
+
+__device__ __forceinline__ void base_range(const DevAdj& a, uint32_t u, uint64_t& b, uint64_t& e) {
+  if (u < a.Vb) {
+    b = a.off[u];
+    e = a.off[u + 1];
+  } else {
+    b = e = 0;
+  }
+}
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+  return v;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_max(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    T w = __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+
+// Warp-aggregated append: every lane with `pred` gets a unique slot in
+// list[0..*count).  Returns the lane's slot (or UINT32_MAX when !pred).
+__device__ __forceinline__ uint32_t warp_append(bool pred, uint32_t* count) {
+  const uint32_t mask = __ballot_sync(0xFFFFFFFFu, pred);
+  if (mask == 0) return 0xFFFFFFFFu;
+  const uint32_t leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if (lane_id() == leader) base = atomicAdd(count, __popc(mask));
+  base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  return pred ? base + __popc(mask & lanemask_lt()) : 0xFFFFFFFFu;
+}
+
+// Lower bound of x among the low 31 bits of a sorted base row.
+__device__ __forceinline__ uint64_t lower_bound_masked(const uint32_t* a, uint64_t lo, uint64_t hi,
+                                                       uint32_t x) {
+  while (lo < hi) {
+    const uint64_t mid = lo + ((hi - lo) >> 1);
+    if ((a[mid] & kIdMask) < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t lo, uint32_t hi,
+                                                    uint32_t x) {
+  while (lo < hi) {
+    const uint32_t mid = lo + ((hi - lo) >> 1);
+    if (a[mid] < x) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Grid-wide barrier for cooperative (co-resident) launches.  The wait is
+// bounded: after ~2^22 polls with back-off the block records
+// kErrBarrierTimeout in *err and proceeds, so a broken launch ends instead of
+// hanging the device.  `bar` = {arrive count, generation}, zeroed at setup.
+constexpr uint32_t kBarrierSpinLimit = 1u << 22;
+
+__device__ __forceinline__ void grid_barrier(uint32_t* bar, uint32_t nblocks, uint32_t* err) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile uint32_t* vgen = bar + 1;
+    const uint32_t gen = *vgen;
+    __threadfence();
+    const uint32_t arrived = atomicAdd(bar, 1u);
+    if (arrived == nblocks - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      uint32_t spins = 0;
+      while (*vgen == gen) {
+        if (++spins > kBarrierSpinLimit) {
+          atomicOr(err, kErrBarrierTimeout);
+          break;
+        }
+        __nanosleep(spins < 64 ? 20 : 200);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+}  // namespace vxb
+
+// Host-side error plumbing (defined in capi.cu).
+namespace vxh {
+void set_error(const char* fmt, ...);
+// Counts every kernel launch the library issues (read by vx_launch_count).
+void count_launch();
+}
+
+#define VX_CUDA_TRY(expr)                                                          \
+  do {                                                                             \
+    cudaError_t _e = (expr);                                                       \
+    if (_e != cudaSuccess) {                                                       \
+      ::vxh::set_error("%s:%d: %s: %s", __FILE__, __LINE__, #expr, cudaGetErrorString(_e)); \
+      return -3;                                                                   \
+    }                                                                              \
+  } while (0)
