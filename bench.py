@@ -187,6 +187,7 @@ def run_b200(args, rank, world, local):
 
     # ---- direction-optimising full BFS from the roots (GTEPS, roofline) ----
     bfs_ms, arcs, levels = [], [], []
+    trace = None
     for r in roots.tolist():
         b = vx.IncrementalBFS(g, int(r))
         b.recompute()  # warm
@@ -199,6 +200,8 @@ def run_b200(args, rank, world, local):
         bfs_ms.append(s0.elapsed_time(s1))
         arcs.append(b.reached_arcs())
         levels.append(b.stats()["levels"])
+        if trace is None:
+            trace = [(round(us, 1), int(nf), "BU" if bu else "TD") for us, nf, bu in b.level_trace()]
         del b
     bfs_ms = np.array(bfs_ms)
     arcs = np.array(arcs, dtype=np.float64)
@@ -266,7 +269,7 @@ def run_b200(args, rank, world, local):
 
     # ---- exactness: repair vs fresh full BFS after each checked batch ----
     exact = True
-    chk0 = base + 2 * args.warmup + args.steps
+    chk0 = base + args.warmup + args.steps
     for i in range(chk0, chk0 + args.check_batches):
         lo, hi = int(stream.offsets[i]), int(stream.offsets[i + 1])
         b.apply_arrays(stream.src[lo:hi], stream.dst[lo:hi], stream.add[lo:hi])
@@ -309,7 +312,7 @@ def run_b200(args, rank, world, local):
         },
         "bfs": {"roots": int(len(roots)), "gteps": gteps, "ms_mean": float(bfs_ms.mean()),
                 "ms_median": float(np.median(bfs_ms)), "levels_median": float(np.median(levels)),
-                "arcs": int(A)},
+                "arcs": int(A), "level_trace_root0_us_nf_dir": trace},
         "repair_last": {"affected": st["last_affected_vertices"], "candidates": st["last_deletion_candidates"],
                         "full": st["last_used_full_recompute"]},
         "clocks": clocks.summary(),

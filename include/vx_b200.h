@@ -118,6 +118,10 @@ int vx_bfs_stats(vx_bfs* b, vx_bfs_stats_t* out);
 /* Sum of out-degrees of reached vertices (arcs traversed by a full top-down
  * BFS), for TEPS reporting. */
 int vx_bfs_reached_arcs(vx_bfs* b, uint64_t* out);
+/* Per-level trace of the last full BFS: for each level {globaltimer ns,
+ * frontier size | bottom_up << 63}, then a closing timestamp; *n = entries.
+ * No reference counterpart (diagnostics). */
+int vx_bfs_level_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
 /* Direction switch (alpha, beta) and grid-expanded row length of the full BFS.
  * No reference counterpart: the reference BFS is top-down only. */
 int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row);

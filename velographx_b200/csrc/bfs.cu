@@ -62,7 +62,10 @@ struct Params {
   float alpha, beta;
   uint32_t large_row;
   uint32_t nblocks;
+  unsigned long long* trace;  // optional per-level {time, n_f | bottom-up << 63}
 };
+
+constexpr uint32_t kTraceLevels = 256;
 
 __device__ __forceinline__ uint32_t ld_cg(const uint32_t* p) { return __ldcg(p); }
 
@@ -71,7 +74,12 @@ __device__ __forceinline__ uint32_t nthreads() { return gridDim.x * blockDim.x; 
 __device__ __forceinline__ uint32_t gwarp() { return gtid() >> 5; }
 __device__ __forceinline__ uint32_t nwarps() { return nthreads() >> 5; }
 
-__device__ __forceinline__ void sync_grid(const Params& p) { vxb::grid_barrier(p.c->bar, p.nblocks, &p.c->err); }
+// Grid barrier; returns false once any block recorded a device error (a
+// barrier that gave up waiting, a loop bound), so every persistent loop ends.
+__device__ __forceinline__ bool sync_grid(const Params& p) {
+  vxb::grid_barrier(p.c->bar, p.nblocks, &p.c->err);
+  return __ldcg(&p.c->err) == 0u;
+}
 
 __device__ __forceinline__ bool test_bit(const uint32_t* bm, uint32_t v) { return (bm[v >> 5] >> (v & 31)) & 1u; }
 
@@ -81,47 +89,26 @@ __device__ __forceinline__ uint32_t degree_of(const DevAdj& a, uint32_t u) {
   return (uint32_t)(e - b) + a.drow[u].y;
 }
 
-// ------------------------------------------------------------ top-down --
+// --------------------------------------------------- row expansion core --
 
-struct TdCtx {
-  uint32_t level;
-  uint32_t* qout;
-  uint32_t* fbn;
-  uint32_t* cnt_n;
-  bool want_deg;
-  unsigned long long mloc;
-};
+constexpr uint32_t FULL = 0xFFFFFFFFu;
 
-// Claim v (if valid) for the next level.  Warp-uniform call.
-__device__ __forceinline__ void td_visit(const Params& p, TdCtx& t, bool valid, uint32_t v) {
-  bool claim = false;
-  const uint32_t bit = 1u << (v & 31);
-  if (valid) {
-    const uint32_t w = p.vis[v >> 5];
-    if (!(w & bit)) claim = !(atomicOr(&p.vis[v >> 5], bit) & bit);
-  }
-  if (claim) {
-    p.dist[v] = t.level + 1;
-    atomicOr(&t.fbn[v >> 5], bit);
-    if (t.want_deg) t.mloc += degree_of(p.g.out, v);
-  }
-  const uint32_t slot = vxb::warp_append(claim, t.cnt_n);
-  if (claim) t.qout[slot] = v;
-}
-
-// Flattened expansion of per-lane segments arr[start, start+len) (len < 32 is
-// typical; any length works).  Warp-uniform call.
-__device__ __forceinline__ void td_gather(const Params& p, TdCtx& t, const uint32_t* arr, uint64_t start, uint32_t len,
-                                          bool tombs) {
+// Flattened expansion of per-lane segments arr[start, start+len) across the
+// warp (Merrill-style gather: warp scan of the lengths, then each lane finds
+// the owner of element k by a 5-step shuffle search).  f(valid, x, owner) is
+// called warp-uniformly.
+template <class F>
+__device__ __forceinline__ void gather_segments(const uint32_t* arr, uint64_t start, uint32_t len, uint32_t u,
+                                                bool tombs, F& f) {
   const int lane = threadIdx.x & 31;
   uint32_t incl = len;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    const uint32_t y = __shfl_up_sync(FULL, incl, o);
     if (lane >= o) incl += y;
   }
   const uint32_t excl = incl - len;
-  const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  const uint32_t total = __shfl_sync(FULL, incl, 31);
   for (uint32_t k0 = 0; k0 < total; k0 += 32) {
     const uint32_t k = k0 + lane;
     const bool ok = k < total;
@@ -129,17 +116,114 @@ __device__ __forceinline__ void td_gather(const Params& p, TdCtx& t, const uint3
 #pragma unroll
     for (int step = 16; step >= 1; step >>= 1) {
       const int cand = owner + step;
-      const uint32_t ex = __shfl_sync(0xFFFFFFFFu, excl, cand & 31);
+      const uint32_t ex = __shfl_sync(FULL, excl, cand & 31);
       if (cand < 32 && ex <= k) owner = cand;
     }
-    const uint64_t st = __shfl_sync(0xFFFFFFFFu, start, owner);
-    const uint32_t ex = __shfl_sync(0xFFFFFFFFu, excl, owner);
+    const uint64_t st = __shfl_sync(FULL, start, owner);
+    const uint32_t ex = __shfl_sync(FULL, excl, owner);
+    const uint32_t ou = __shfl_sync(FULL, u, owner);
     const uint32_t x = ok ? arr[st + (k - ex)] : kTomb;
-    td_visit(p, t, ok && !(tombs && (x & kTomb)), x & kIdMask);
+    f(ok && !(tombs && (x & kTomb)), x & kIdMask, ou);
   }
 }
 
-__device__ void td_level(const Params& p, TdCtx& t, const uint32_t* qin, uint32_t n_f, uint32_t* cnt_big) {
+// Expands the rows of the (up to) 32 lane vertices: rows of >= 32 arcs are
+// walked by the whole warp, shorter ones flattened across lanes.  Lanes pass
+// an empty range (b == e, dr.y == 0) when they have no row.
+template <class F>
+__device__ __forceinline__ void expand_lanes(const DevAdj& a, uint32_t u, uint64_t b, uint64_t e, uint2 dr, F& f) {
+  const int lane = threadIdx.x & 31;
+  uint32_t blen = (uint32_t)(e - b), dlen = dr.y;
+  uint32_t med = __ballot_sync(FULL, blen >= 32);
+  while (med) {
+    const int l = __ffs(med) - 1;
+    med &= med - 1;
+    const uint64_t bb = __shfl_sync(FULL, b, l), ee = __shfl_sync(FULL, e, l);
+    const uint32_t uu = __shfl_sync(FULL, u, l);
+    for (uint64_t j0 = bb; j0 < ee; j0 += 32) {
+      const uint64_t j = j0 + lane;
+      const uint32_t x = j < ee ? a.col[j] : kTomb;
+      f(!(x & kTomb), x & kIdMask, uu);
+    }
+  }
+  if (blen >= 32) blen = 0;
+  gather_segments(a.col, b, blen, u, true, f);
+  med = __ballot_sync(FULL, dlen >= 32);
+  while (med) {
+    const int l = __ffs(med) - 1;
+    med &= med - 1;
+    const uint32_t bb = __shfl_sync(FULL, dr.x, l), ee = bb + __shfl_sync(FULL, dr.y, l);
+    const uint32_t uu = __shfl_sync(FULL, u, l);
+    for (uint32_t j0 = bb; j0 < ee; j0 += 32) {
+      const uint32_t j = j0 + lane;
+      const bool ok = j < ee;
+      f(ok, ok ? a.darena[j] : 0u, uu);
+    }
+  }
+  if (dlen >= 32) dlen = 0;
+  gather_segments(a.darena, (uint64_t)dr.x, dlen, u, false, f);
+}
+
+// The whole warp walks one row (all lanes pass the same u); f as above.
+template <class F>
+__device__ __forceinline__ void warp_row(const DevAdj& a, uint32_t u, F& f) {
+  const int lane = threadIdx.x & 31;
+  uint64_t b, e;
+  vxb::base_range(a, u, b, e);
+  for (uint64_t j0 = b; j0 < e; j0 += 32) {
+    const uint64_t j = j0 + lane;
+    const uint32_t x = j < e ? a.col[j] : kTomb;
+    f(!(x & kTomb), x & kIdMask, u);
+  }
+  const uint2 dr = a.drow[u];
+  for (uint32_t j0 = dr.x; j0 < dr.x + dr.y; j0 += 32) {
+    const uint32_t j = j0 + lane;
+    const bool ok = j < dr.x + dr.y;
+    f(ok, ok ? a.darena[j] : 0u, u);
+  }
+}
+
+__device__ __forceinline__ uint64_t globaltimer() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// ------------------------------------------------------------ top-down --
+
+struct TdVisit {
+  const Params* p;
+  uint32_t level;
+  uint32_t* qout;
+  uint32_t* fbn;
+  uint32_t* cnt_n;
+  bool want_deg;
+  unsigned long long mloc;
+  // Claim x for the next level (warp-uniform).
+  __device__ __forceinline__ void operator()(bool valid, uint32_t x, uint32_t) {
+    bool claim = false;
+    const uint32_t bit = 1u << (x & 31);
+    if (valid) {
+      const uint32_t w = p->vis[x >> 5];
+      if (!(w & bit)) claim = !(atomicOr(&p->vis[x >> 5], bit) & bit);
+    }
+    if (claim) {
+      p->dist[x] = level + 1;
+      atomicOr(&fbn[x >> 5], bit);
+      if (want_deg) mloc += degree_of(p->g.out, x);
+    }
+    const uint32_t slot = vxb::warp_append(claim, cnt_n);
+    if (claim) qout[slot] = x;
+  }
+  __device__ __forceinline__ void flush(unsigned long long* dst) {
+    if (!want_deg) return;
+    const unsigned long long sum = vxb::warp_sum(mloc);
+    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(dst, sum);
+    mloc = 0;
+  }
+};
+
+__device__ void td_level(const Params& p, TdVisit& t, const uint32_t* qin, uint32_t n_f, uint32_t* cnt_big) {
   const DevAdj& a = p.g.out;
   const int lane = threadIdx.x & 31;
   for (uint32_t base = gwarp() * 32; base < n_f; base += nwarps() * 32) {
@@ -152,68 +236,45 @@ __device__ void td_level(const Params& p, TdCtx& t, const uint32_t* qin, uint32_
       vxb::base_range(a, u, b, e);
       dr = a.drow[u];
     }
-    uint32_t blen = (uint32_t)(e - b), dlen = dr.y;
-    const bool big = act && (uint64_t)blen + dlen >= p.large_row;
+    const bool big = act && (e - b) + dr.y >= p.large_row;
     const uint32_t slot = vxb::warp_append(big, cnt_big);
     if (big) {
       p.big[slot] = u;
-      blen = dlen = 0;
+      b = e = 0;
+      dr = make_uint2(0, 0);
     }
-    // medium base rows: whole warp per row
-    uint32_t med = __ballot_sync(0xFFFFFFFFu, blen >= 32);
-    while (med) {
-      const int l = __ffs(med) - 1;
-      med &= med - 1;
-      const uint64_t bb = __shfl_sync(0xFFFFFFFFu, b, l), ee = __shfl_sync(0xFFFFFFFFu, e, l);
-      for (uint64_t j0 = bb; j0 < ee; j0 += 32) {
-        const uint64_t j = j0 + lane;
-        const uint32_t x = j < ee ? a.col[j] : kTomb;
-        td_visit(p, t, !(x & kTomb), x & kIdMask);
-      }
-    }
-    if (blen >= 32) blen = 0;
-    td_gather(p, t, a.col, b, blen, true);
-    // delta rows
-    med = __ballot_sync(0xFFFFFFFFu, dlen >= 32);
-    while (med) {
-      const int l = __ffs(med) - 1;
-      med &= med - 1;
-      const uint32_t bb = __shfl_sync(0xFFFFFFFFu, dr.x, l), ee = bb + __shfl_sync(0xFFFFFFFFu, dr.y, l);
-      for (uint32_t j0 = bb; j0 < ee; j0 += 32) {
-        const uint32_t j = j0 + lane;
-        const bool ok = j < ee;
-        td_visit(p, t, ok, ok ? a.darena[j] : 0u);
-      }
-    }
-    if (dlen >= 32) dlen = 0;
-    td_gather(p, t, a.darena, dr.x, dlen, false);
+    expand_lanes(a, u, b, e, dr, t);
   }
 }
 
 // Rows of at least large_row arcs: every warp of the grid takes a slice.
-__device__ void td_big_rows(const Params& p, TdCtx& t, uint32_t nbig) {
-  const DevAdj& a = p.g.out;
+template <class F>
+__device__ void grid_rows(const DevAdj& a, const uint32_t* rows, uint32_t n, F& f) {
   const int lane = threadIdx.x & 31;
-  for (uint32_t r = 0; r < nbig; ++r) {
-    const uint32_t u = p.big[r];
+  for (uint32_t r = 0; r < n; ++r) {
+    const uint32_t u = rows[r];
     uint64_t b, e;
     vxb::base_range(a, u, b, e);
     for (uint64_t j0 = b + (uint64_t)gwarp() * 32; j0 < e; j0 += (uint64_t)nwarps() * 32) {
       const uint64_t j = j0 + lane;
       const uint32_t x = j < e ? a.col[j] : kTomb;
-      td_visit(p, t, !(x & kTomb), x & kIdMask);
+      f(!(x & kTomb), x & kIdMask, u);
     }
     const uint2 dr = a.drow[u];
     for (uint32_t j0 = dr.x + gwarp() * 32; j0 < dr.x + dr.y; j0 += nwarps() * 32) {
       const uint32_t j = j0 + lane;
       const bool ok = j < dr.x + dr.y;
-      td_visit(p, t, ok, ok ? a.darena[j] : 0u);
+      f(ok, ok ? a.darena[j] : 0u, u);
     }
   }
 }
 
 // ----------------------------------------------------------- bottom-up --
 
+// One warp per 32 unvisited-candidate vertices (a visited-bitmap word).  Rows
+// of at most 32 in-arcs are scanned by their own lane, longer rows by the
+// whole warp 32 arcs at a time; every scan stops at the first parent found in
+// the frontier bitmap.
 __device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, uint32_t* fbn, uint32_t* qout,
                          uint32_t* cnt_n) {
   const DevAdj& a = p.g.in;
@@ -221,30 +282,49 @@ __device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, u
   const uint32_t words = (p.V + 31) >> 5;
   for (uint32_t w = gwarp(); w < words; w += nwarps()) {
     const uint32_t visw = p.vis[w];
-    if (visw == 0xFFFFFFFFu) continue;
+    if (visw == FULL) continue;
     const uint32_t v = w * 32 + lane;
-    bool found = false;
-    if (!((visw >> lane) & 1u)) {
-      uint64_t b, e;
+    const bool todo = !((visw >> lane) & 1u);
+    uint64_t b = 0, e = 0;
+    uint2 dr = make_uint2(0, 0);
+    if (todo) {
       vxb::base_range(a, v, b, e);
-      for (uint64_t j = b; j < e; ++j) {
-        const uint32_t x = a.col[j];
+      dr = a.drow[v];
+    }
+    const uint32_t nb = (uint32_t)(e - b), total = nb + dr.y;
+    bool found = false;
+    if (todo && total <= 32) {
+      for (uint32_t k = 0; k < total; ++k) {
+        const uint32_t x = k < nb ? a.col[b + k] : a.darena[dr.x + (k - nb)];
         if (!(x & kTomb) && test_bit(fbc, x)) {
           found = true;
           break;
         }
       }
-      if (!found) {
-        const uint2 dr = a.drow[v];
-        for (uint32_t j = dr.x; j < dr.x + dr.y; ++j) {
-          if (test_bit(fbc, a.darena[j])) {
-            found = true;
-            break;
-          }
+    }
+    uint32_t longm = __ballot_sync(FULL, todo && total > 32);
+    while (longm) {
+      const int l = __ffs(longm) - 1;
+      longm &= longm - 1;
+      const uint64_t bb = __shfl_sync(FULL, b, l);
+      const uint32_t nbl = __shfl_sync(FULL, nb, l), tot = __shfl_sync(FULL, total, l);
+      const uint32_t dx = __shfl_sync(FULL, dr.x, l);
+      bool hit_l = false;
+      for (uint32_t k0 = 0; k0 < tot; k0 += 32) {
+        const uint32_t k = k0 + lane;
+        bool hit = false;
+        if (k < tot) {
+          const uint32_t x = k < nbl ? a.col[bb + k] : a.darena[dx + (k - nbl)];
+          hit = !(x & kTomb) && test_bit(fbc, x);
+        }
+        if (__any_sync(FULL, hit)) {
+          hit_l = true;
+          break;
         }
       }
+      if (lane == l) found = hit_l;
     }
-    const uint32_t newly = __ballot_sync(0xFFFFFFFFu, found);
+    const uint32_t newly = __ballot_sync(FULL, found);
     if (found) p.dist[v] = level + 1;
     if (lane == 0 && newly) {
       p.vis[w] = visw | newly;
@@ -253,13 +333,6 @@ __device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, u
     const uint32_t slot = vxb::warp_append(found, cnt_n);
     if (found) qout[slot] = v;
   }
-}
-
-__device__ __forceinline__ void flush_degrees(TdCtx& t, unsigned long long* dst) {
-  if (!t.want_deg) return;
-  const unsigned long long sum = vxb::warp_sum(t.mloc);
-  if ((threadIdx.x & 31) == 0 && sum) atomicAdd(dst, sum);
-  t.mloc = 0;
 }
 
 // ------------------------------------------------------------ full BFS --
@@ -272,7 +345,7 @@ __device__ void full_bfs(const Params& p) {
   for (uint32_t i = gtid(); i < words; i += nthreads()) {
     // bits past V count as visited so bottom-up never scans them
     const uint32_t lo = i * 32;
-    p.vis[i] = (lo + 32 <= V) ? 0u : (0xFFFFFFFFu << (V - lo));
+    p.vis[i] = (lo + 32 <= V) ? 0u : (FULL << (V - lo));
     p.fb[0][i] = p.fb[1][i] = p.fb[2][i] = 0u;
   }
   if (gtid() == 0) {
@@ -282,7 +355,7 @@ __device__ void full_bfs(const Params& p) {
       c->lvl_m[k] = 0;
     }
   }
-  sync_grid(p);
+  if (!sync_grid(p)) return;
   if (p.source >= V) {
     if (gtid() == 0) {
       c->reachable = 0;
@@ -300,7 +373,7 @@ __device__ void full_bfs(const Params& p) {
     c->lvl_n[0] = 1;
     c->lvl_m[0] = degree_of(p.g.out, s);
   }
-  sync_grid(p);
+  if (!sync_grid(p)) return;
   unsigned long long m_visited = 0, reached = 0;
   bool bottom_up = false, left_bu = false;
   uint32_t prev_n = 0;
@@ -327,22 +400,26 @@ __device__ void full_bfs(const Params& p) {
       c->lvl_n[clr] = 0;
       c->lvl_m[clr] = 0;
       c->lvl_big[clr] = 0;
+      if (p.trace && level < kTraceLevels) {
+        p.trace[2 * level] = globaltimer();
+        p.trace[2 * level + 1] = (unsigned long long)n_f | ((unsigned long long)bottom_up << 63);
+      }
     }
     // clear the frontier bitmap of level-1 through its queue
     for (uint32_t i = gtid(); i < prev_n; i += nthreads()) p.fb[clr][p.q[clr][i] >> 5] = 0u;
     if (bottom_up) {
       bu_level(p, level, p.fb[cur], p.fb[nxt], p.q[nxt], &c->lvl_n[nxt]);
-      sync_grid(p);
+      if (!sync_grid(p)) return;
     } else {
-      TdCtx t{level, p.q[nxt], p.fb[nxt], &c->lvl_n[nxt], !left_bu, 0ull};
+      TdVisit t{&p, level, p.q[nxt], p.fb[nxt], &c->lvl_n[nxt], !left_bu, 0ull};
       td_level(p, t, p.q[cur], n_f, &c->lvl_big[cur]);
-      flush_degrees(t, &c->lvl_m[nxt]);
-      sync_grid(p);
+      t.flush(&c->lvl_m[nxt]);
+      if (!sync_grid(p)) return;
       const uint32_t nbig = ld_cg(&c->lvl_big[cur]);
       if (nbig) {
-        td_big_rows(p, t, nbig);
-        flush_degrees(t, &c->lvl_m[nxt]);
-        sync_grid(p);
+        grid_rows(p.g.out, p.big, nbig, t);
+        t.flush(&c->lvl_m[nxt]);
+        if (!sync_grid(p)) return;
       }
     }
     prev_n = n_f;
@@ -351,6 +428,10 @@ __device__ void full_bfs(const Params& p) {
     c->reachable = reached;
     c->levels = level;
     c->arcs = m_visited;
+    if (p.trace && level < kTraceLevels) {
+      p.trace[2 * level] = globaltimer();
+      p.trace[2 * level + 1] = 0;
+    }
   }
 }
 
@@ -374,47 +455,77 @@ __device__ bool is_final_deletion(const Params& p, uint32_t F, uint32_t u, uint3
   return lo < F && p.fu[lo] == u && p.fv[lo] == v && !(p.ff[lo] & kFAdd);
 }
 
-// shortest_parent_count (bfs.hpp:211-220) on the current adjacency.
-__device__ uint32_t support_of(const Params& p, uint32_t v) {
+// Does v (at distance d >= 1) keep a shortest parent in the pre-batch graph:
+// an in-neighbour x at distance d-1 that is not affected and whose arc (x, v)
+// is not deleted by the batch?  Whole warp, stops at the first such parent.
+// "v has none" is exactly the reference's lost >= support test
+// (bfs.hpp:229-240): lost counts every shortest parent that is deleted or
+// affected, each once, and support counts all of them.
+__device__ bool warp_has_surviving_parent(const Params& p, uint32_t v, uint32_t d, uint32_t F) {
   const DevAdj& a = p.g.in;
-  const uint32_t dv = p.dist[v];
-  uint32_t cnt = 0;
+  const int lane = threadIdx.x & 31;
   uint64_t b, e;
   vxb::base_range(a, v, b, e);
-  for (uint64_t j = b; j < e; ++j) {
-    const uint32_t x = a.col[j];
-    if (x & kTomb) continue;
-    if (x < p.dist_len && p.dist[x] != kUnreachable && p.dist[x] + 1 == dv) ++cnt;
-  }
   const uint2 dr = a.drow[v];
-  for (uint32_t j = dr.x; j < dr.x + dr.y; ++j) {
-    const uint32_t x = a.darena[j];
-    if (x < p.dist_len && p.dist[x] != kUnreachable && p.dist[x] + 1 == dv) ++cnt;
+  const uint64_t nb = e - b, total = nb + dr.y;
+  for (uint64_t k0 = 0; k0 < total; k0 += 32) {
+    const uint64_t k = k0 + lane;
+    bool ok = false;
+    if (k < total) {
+      uint32_t x;
+      bool valid = true;
+      if (k < nb) {
+        x = a.col[b + k];
+        valid = !(x & kTomb);
+      } else {
+        x = a.darena[dr.x + (uint32_t)(k - nb)];
+      }
+      ok = valid && x < p.dist_len && p.dist[x] + 1 == d && !test_bit(p.aff, x) && !is_final_deletion(p, F, x, v);
+    }
+    if (__any_sync(FULL, ok)) return true;
   }
-  return cnt;
+  return false;
 }
 
-__device__ void check_affected(const Params& p, uint32_t v) {
-  const uint32_t sup = support_of(p, v);
-  if (sup != 0 && p.lost[v] >= sup) {
-    atomicOr(&p.aff[v >> 5], 1u << (v & 31));
-    const uint32_t slot = atomicAdd(&p.c->a_n, 1u);
-    p.lst_a[slot] = v;
-  }
+__device__ __forceinline__ void mark_affected(const Params& p, uint32_t v) {
+  atomicOr(&p.aff[v >> 5], 1u << (v & 31));
+  const uint32_t slot = atomicAdd(&p.c->a_n, 1u);
+  p.lst_a[slot] = v;
 }
+
+// Children one level deeper of a newly affected vertex become touched.
+struct TouchChildren {
+  const Params* p;
+  uint32_t d;
+  uint32_t* plist;
+  uint32_t* pcount;
+  __device__ __forceinline__ void operator()(bool valid, uint32_t x, uint32_t) {
+    bool fresh = false;
+    if (valid && x < p->dist_len && p->dist[x] == d + 1) fresh = atomicOr(&p->lost[x], 1u) == 0u;
+    const uint32_t s1 = vxb::warp_append(fresh, pcount);
+    if (fresh) plist[s1] = x;
+    const uint32_t s2 = vxb::warp_append(fresh, &p->c->touched_n);
+    if (fresh) p->lst_t[s2] = x;
+  }
+};
 
 // --------------------------------------------------- pre-batch fixpoint --
 
+// compute_affected_prebatch (bfs.hpp:222-259) level by level: at distance d
+// the touched vertices (deletion candidates at d, children of vertices that
+// became affected at d-1) are affected iff no shortest parent survives; the
+// children of those at d+1 are touched next.  The fallback limit is checked
+// after every level (the affected count only grows).
 __device__ void repair_pre(const Params& p) {
   BfsCounters* c = p.c;
+  const int lane = threadIdx.x & 31;
   const uint32_t F = *p.F;
-  // deletion candidates: existing deleted arcs that are shortest-parent arcs
   for (uint32_t i = gtid(); i < F; i += nthreads()) {
     const uint8_t f = p.ff[i];
     if ((f & kFAdd) || !(f & kFCur)) continue;
     const uint32_t u = p.fu[i], v = p.fv[i];
     if (!is_sp(p, u, v)) continue;
-    if (atomicAdd(&p.lost[v], 1u) == 0u) {
+    if (atomicOr(&p.lost[v], 1u) == 0u) {
       const uint32_t slot = atomicAdd(&c->cand_n, 1u);
       p.lst_t[slot] = v;
     }
@@ -426,7 +537,7 @@ __device__ void repair_pre(const Params& p) {
     }
     c->seed_min = kUnreachable;
   }
-  sync_grid(p);
+  if (!sync_grid(p)) return;
   const uint32_t ncand = ld_cg(&c->cand_n);
   if (gtid() == 0) {
     c->candidates = ncand;
@@ -434,7 +545,7 @@ __device__ void repair_pre(const Params& p) {
   }
   if (ncand == 0) return;
   for (uint32_t i = gtid(); i < ncand; i += nthreads()) atomicMin(&c->seed_min, p.dist[p.lst_t[i]]);
-  sync_grid(p);
+  if (!sync_grid(p)) return;
   uint32_t d = ld_cg(&c->seed_min);
   uint32_t a_prev = 0;
   for (uint32_t it = 0;; ++it) {
@@ -448,47 +559,41 @@ __device__ void repair_pre(const Params& p) {
       c->list_n[k2] = 0;
       c->next_seed[k2] = kUnreachable;
     }
-    // level-d items: candidates at distance d, and children reached at d
-    for (uint32_t i = gtid(); i < ncand; i += nthreads()) {
-      const uint32_t v = p.lst_t[i];
-      const uint32_t dv = p.dist[v];
-      if (dv == d) check_affected(p, v);
-      else if (dv > d) atomicMin(&c->next_seed[k1], dv);
+    // candidates at distance d (32 per warp, each checked by the whole warp)
+    for (uint32_t base = gwarp() * 32; base < ncand; base += nwarps() * 32) {
+      const uint32_t i = base + lane;
+      const uint32_t v = i < ncand ? p.lst_t[i] : 0u;
+      const uint32_t dv = i < ncand ? p.dist[v] : kUnreachable;
+      if (dv != kUnreachable && dv > d) atomicMin(&c->next_seed[k1], dv);
+      uint32_t m = __ballot_sync(FULL, dv == d);
+      while (m) {
+        const int l = __ffs(m) - 1;
+        m &= m - 1;
+        const uint32_t vv = __shfl_sync(FULL, v, l);
+        if (!warp_has_surviving_parent(p, vv, d, F) && lane == 0) mark_affected(p, vv);
+      }
     }
-    for (uint32_t i = gtid(); i < np; i += nthreads()) check_affected(p, p.q[k][i]);
-    sync_grid(p);
+    // children touched at the previous level
+    for (uint32_t base = gwarp() * 32; base < np; base += nwarps() * 32) {
+      const uint32_t i = base + lane;
+      const uint32_t v = i < np ? p.q[k][i] : 0u;
+      uint32_t m = __ballot_sync(FULL, i < np);
+      while (m) {
+        const int l = __ffs(m) - 1;
+        m &= m - 1;
+        const uint32_t vv = __shfl_sync(FULL, v, l);
+        if (!warp_has_surviving_parent(p, vv, d, F) && lane == 0) mark_affected(p, vv);
+      }
+    }
+    if (!sync_grid(p)) return;
     const uint32_t a_tot = ld_cg(&c->a_n);
     if (a_tot > p.fallback_limit) {
       if (gtid() == 0) c->fallback = 1;
       break;
     }
-    // children of the vertices that became affected at level d
-    for (uint32_t i = a_prev + gtid(); i < a_tot; i += nthreads()) {
-      const uint32_t u = p.lst_a[i];
-      const DevAdj& a = p.g.out;
-      uint64_t b, e;
-      vxb::base_range(a, u, b, e);
-      const uint2 dr = a.drow[u];
-      const uint64_t nb = e - b;
-      for (uint64_t j = 0; j < nb + dr.y; ++j) {
-        uint32_t x;
-        if (j < nb) {
-          x = a.col[b + j];
-          if (x & kTomb) continue;
-        } else {
-          x = a.darena[dr.x + (j - nb)];
-        }
-        if (x >= p.dist_len || p.dist[x] != d + 1) continue;
-        if (is_final_deletion(p, F, u, x)) continue;
-        if (atomicAdd(&p.lost[x], 1u) == 0u) {
-          const uint32_t s1 = atomicAdd(&c->list_n[k1], 1u);
-          p.q[k1][s1] = x;
-          const uint32_t s2 = atomicAdd(&c->touched_n, 1u);
-          p.lst_t[s2] = x;
-        }
-      }
-    }
-    sync_grid(p);
+    TouchChildren tc{&p, d, p.q[k1], &c->list_n[k1]};
+    for (uint32_t i = a_prev + gwarp(); i < a_tot; i += nwarps()) warp_row(p.g.out, p.lst_a[i], tc);
+    if (!sync_grid(p)) return;
     a_prev = a_tot;
     const uint32_t nn = ld_cg(&c->list_n[k1]);
     const uint32_t ns = ld_cg(&c->next_seed[k1]);
@@ -526,11 +631,63 @@ __device__ __forceinline__ void lower_and_queue(const Params& p, uint32_t x, uin
   }
 }
 
+// Bucketed settle: relax affected out-neighbours of level-lvl vertices.
+struct SettleVisit {
+  const Params* p;
+  uint32_t lvl;
+  uint32_t* qn;
+  uint32_t* cnt;
+  long long* reach;
+  __device__ __forceinline__ void operator()(bool valid, uint32_t x, uint32_t) {
+    bool lowered = false;
+    if (valid && test_bit(p->aff, x)) {
+      const uint32_t cand = lvl + 1;
+      if (cand < ld_cg(&p->dist[x])) {
+        const uint32_t old = atomicMin(&p->dist[x], cand);
+        if (old > cand) {
+          lowered = true;
+          if (old == kUnreachable) ++*reach;
+        }
+      }
+    }
+    const uint32_t s = vxb::warp_append(lowered, cnt);
+    if (lowered) qn[s] = x;
+  }
+};
+
+// Decrease propagation: relax every out-neighbour of a queued vertex.
+struct PropVisit {
+  const Params* p;
+  uint32_t* inq_next;
+  uint32_t* qn;
+  uint32_t* cnt;
+  long long* reach;
+  __device__ __forceinline__ void operator()(bool valid, uint32_t x, uint32_t u) {
+    if (!valid) return;
+    const uint32_t du = ld_cg(&p->dist[u]);
+    if (du == kUnreachable) return;
+    lower_and_queue(*p, x, du + 1, inq_next, qn, cnt, *reach);
+  }
+};
+
+// Warp-uniform minimum of dist+1 over non-affected in-neighbours
+// (best_boundary_distance, bfs.hpp:261-269).
+struct BoundaryMin {
+  const Params* p;
+  uint32_t best;
+  __device__ __forceinline__ void operator()(bool valid, uint32_t x, uint32_t) {
+    if (!valid || x >= p->dist_len || test_bit(p->aff, x)) return;
+    const uint32_t dx = p->dist[x];
+    if (dx != kUnreachable && dx + 1 < best) best = dx + 1;
+  }
+};
+
 __device__ void repair_post(const Params& p) {
   BfsCounters* c = p.c;
+  const int lane = threadIdx.x & 31;
   if (ld_cg(&c->fallback)) {
     clear_workspace(p);
-    sync_grid(p);
+    if (!sync_grid(p)) return;
     full_bfs(p);
     if (gtid() == 0) c->full = 1;
     return;
@@ -551,39 +708,29 @@ __device__ void repair_post(const Params& p) {
         c->next_seed[k] = kUnreachable;
       }
     }
-    sync_grid(p);
-    // boundary seeds: best non-affected in-neighbour (bfs.hpp:261-269)
-    for (uint32_t i = gtid(); i < na; i += nthreads()) {
+    if (!sync_grid(p)) return;
+    // boundary seeds, one warp per affected vertex
+    for (uint32_t i = gwarp(); i < na; i += nwarps()) {
       const uint32_t v = p.lst_a[i];
-      const DevAdj& a = p.g.in;
-      uint32_t best = kUnreachable;
-      uint64_t b, e;
-      vxb::base_range(a, v, b, e);
-      const uint2 dr = a.drow[v];
-      const uint64_t nb = e - b;
-      for (uint64_t j = 0; j < nb + dr.y; ++j) {
-        uint32_t x;
-        if (j < nb) {
-          x = a.col[b + j];
-          if (x & kTomb) continue;
-        } else {
-          x = a.darena[dr.x + (j - nb)];
+      BoundaryMin bm{&p, kUnreachable};
+      warp_row(p.g.in, v, bm);
+      uint32_t best = bm.best;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(FULL, best, o));
+      if (lane == 0) {
+        p.tent[i] = best;
+        p.dist[v] = best;
+        if (best != kUnreachable) {
+          ++reach;
+          atomicMin(&c->seed_min, best);
         }
-        if (x >= p.dist_len || test_bit(p.aff, x)) continue;
-        const uint32_t dx = p.dist[x];
-        if (dx != kUnreachable && dx + 1 < best) best = dx + 1;
-      }
-      p.tent[i] = best;
-      p.dist[v] = best;
-      if (best != kUnreachable) {
-        ++reach;
-        atomicMin(&c->seed_min, best);
       }
     }
-    sync_grid(p);
+    if (!sync_grid(p)) return;
     // bucketed settle among affected vertices (unit-weight Dijkstra)
     uint32_t lvl = ld_cg(&c->seed_min);
     if (lvl != kUnreachable) {
+      const DevAdj& a = p.g.out;
       for (uint32_t it = 0;; ++it) {
         if (it > p.dist_len + 1) {
           if (gtid() == 0) atomicOr(&c->err, vxb::kErrLoopBound);
@@ -595,45 +742,32 @@ __device__ void repair_post(const Params& p) {
           c->list_n[k2] = 0;
           c->next_seed[k2] = kUnreachable;
         }
-        // seeds whose boundary distance is this level and still hold it
-        for (uint32_t i = gtid(); i < na + nr; i += nthreads()) {
-          uint32_t u;
+        SettleVisit sv{&p, lvl, p.q[k1], &c->list_n[k1], &reach};
+        // items: seeds whose boundary distance is lvl and still hold it, then
+        // the vertices relaxed to lvl at the previous level
+        for (uint32_t base = gwarp() * 32; base < na + nr; base += nwarps() * 32) {
+          const uint32_t i = base + lane;
+          bool act = false;
+          uint32_t u = 0;
           if (i < na) {
             const uint32_t t = p.tent[i];
             u = p.lst_a[i];
             const uint32_t du = ld_cg(&p.dist[u]);
-            if (t != lvl || du != lvl) {
-              if (t != kUnreachable && t > lvl && du == t) atomicMin(&c->next_seed[k1], t);
-              continue;
-            }
-          } else {
+            act = t == lvl && du == lvl;
+            if (!act && t != kUnreachable && t > lvl && du == t) atomicMin(&c->next_seed[k1], t);
+          } else if (i < na + nr) {
             u = p.q[k][i - na];
+            act = true;
           }
-          const DevAdj& a = p.g.out;
-          uint64_t b, e;
-          vxb::base_range(a, u, b, e);
-          const uint2 dr = a.drow[u];
-          const uint64_t nb = e - b;
-          for (uint64_t j = 0; j < nb + dr.y; ++j) {
-            uint32_t x;
-            if (j < nb) {
-              x = a.col[b + j];
-              if (x & kTomb) continue;
-            } else {
-              x = a.darena[dr.x + (j - nb)];
-            }
-            if (!test_bit(p.aff, x)) continue;
-            const uint32_t cand = lvl + 1;
-            if (cand >= ld_cg(&p.dist[x])) continue;
-            const uint32_t old = atomicMin(&p.dist[x], cand);
-            if (old > cand) {
-              if (old == kUnreachable) ++reach;
-              const uint32_t s = atomicAdd(&c->list_n[k1], 1u);
-              p.q[k1][s] = x;
-            }
+          uint64_t b = 0, e = 0;
+          uint2 dr = make_uint2(0, 0);
+          if (act) {
+            vxb::base_range(a, u, b, e);
+            dr = a.drow[u];
           }
+          expand_lanes(a, u, b, e, dr, sv);
         }
-        sync_grid(p);
+        if (!sync_grid(p)) return;
         const uint32_t nn = ld_cg(&c->list_n[k1]), ns = ld_cg(&c->next_seed[k1]);
         if (nn > 0) ++lvl;
         else if (ns != kUnreachable) lvl = ns;
@@ -647,7 +781,7 @@ __device__ void repair_post(const Params& p) {
   if (gtid() == 0) {
     for (int k = 0; k < 3; ++k) c->list_n[k] = 0;
   }
-  sync_grid(p);
+  if (!sync_grid(p)) return;
   for (uint32_t i = gtid(); i < na; i += nthreads()) {
     const uint32_t v = p.lst_a[i];
     const uint32_t dv = ld_cg(&p.dist[v]);
@@ -665,7 +799,8 @@ __device__ void repair_post(const Params& p) {
     if (du == kUnreachable) continue;
     lower_and_queue(p, v, du + 1, p.inq[0], p.q[0], &c->list_n[0], reach);
   }
-  sync_grid(p);
+  if (!sync_grid(p)) return;
+  const DevAdj& a = p.g.out;
   for (uint32_t r = 0;; ++r) {
     if (r > p.dist_len + 1) {
       if (gtid() == 0) atomicOr(&c->err, vxb::kErrLoopBound);
@@ -676,32 +811,24 @@ __device__ void repair_post(const Params& p) {
     if (n == 0) break;
     if (gtid() == 0) c->list_n[k2] = 0;
     uint32_t* inq_cur = p.inq[r & 1];
-    uint32_t* inq_nxt = p.inq[(r + 1) & 1];
-    for (uint32_t i = gtid(); i < n; i += nthreads()) {
-      const uint32_t u = p.q[k][i];
-      atomicAnd(&inq_cur[u >> 5], ~(1u << (u & 31)));
-      const uint32_t du = ld_cg(&p.dist[u]);
-      if (du == kUnreachable) continue;
-      const DevAdj& a = p.g.out;
-      uint64_t b, e;
-      vxb::base_range(a, u, b, e);
-      const uint2 dr = a.drow[u];
-      const uint64_t nb = e - b;
-      for (uint64_t j = 0; j < nb + dr.y; ++j) {
-        uint32_t x;
-        if (j < nb) {
-          x = a.col[b + j];
-          if (x & kTomb) continue;
-        } else {
-          x = a.darena[dr.x + (j - nb)];
-        }
-        lower_and_queue(p, x, du + 1, inq_nxt, p.q[k1], &c->list_n[k1], reach);
+    PropVisit pv{&p, p.inq[(r + 1) & 1], p.q[k1], &c->list_n[k1], &reach};
+    for (uint32_t base = gwarp() * 32; base < n; base += nwarps() * 32) {
+      const uint32_t i = base + lane;
+      const bool act = i < n;
+      const uint32_t u = act ? p.q[k][i] : 0u;
+      uint64_t b = 0, e = 0;
+      uint2 dr = make_uint2(0, 0);
+      if (act) {
+        atomicAnd(&inq_cur[u >> 5], ~(1u << (u & 31)));
+        vxb::base_range(a, u, b, e);
+        dr = a.drow[u];
       }
+      expand_lanes(a, u, b, e, dr, pv);
     }
-    sync_grid(p);
+    if (!sync_grid(p)) return;
   }
   reach = vxb::warp_sum(reach);
-  if ((threadIdx.x & 31) == 0) reach_add(p, reach);
+  if (lane == 0) reach_add(p, reach);
   clear_workspace(p);
 }
 
@@ -802,6 +929,7 @@ static Params make_params(Bfs* b, uint32_t V, uint32_t dist_len) {
   p.alpha = b->tune.alpha;
   p.beta = b->tune.beta;
   p.large_row = b->tune.large_row;
+  p.trace = b->trace;
   return p;
 }
 
@@ -829,6 +957,7 @@ int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac) {
   b->source = source;
   b->frac = frac;
   if (cudaMalloc(&b->ctr, sizeof(BfsCounters)) != cudaSuccess ||
+      cudaMalloc(&b->trace, 2 * (kTraceLevels + 1) * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMallocHost(&b->hctr, sizeof(BfsCounters)) != cudaSuccess) {
     set_error("BFS counter allocation failed");
     bfs_destroy(b);
@@ -851,6 +980,7 @@ void bfs_destroy(Bfs* b) {
                       b->lst_a, b->lst_t, b->old, b->tent, b->lost, b->aff, b->inq[0], b->inq[1]};
   for (uint32_t* p : ptrs) cudaFree(p);
   cudaFree(b->ctr);
+  cudaFree(b->trace);
   cudaFreeHost(b->hctr);
   delete b;
 }
@@ -924,4 +1054,15 @@ int bfs_reached_arcs(Bfs* b, unsigned long long* arcs) {
   return 0;
 }
 
+}  // namespace vxh
+
+namespace vxh {
+int bfs_level_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n) {
+  if (int rc = bfs_sync(b)) return rc;
+  const uint32_t levels = std::min<uint32_t>(b->hctr->levels, kTraceLevels - 1);
+  *n = 2 * ((size_t)levels + 1);
+  const size_t m = std::min(cap, *n);
+  if (out && m) VX_CUDA_TRY(cudaMemcpy(out, b->trace, m * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  return 0;
+}
 }  // namespace vxh

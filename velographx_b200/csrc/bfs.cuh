@@ -59,6 +59,7 @@ struct Bfs {
   uint32_t* inq[2] = {nullptr, nullptr};  // queued bitmaps of the decrease propagation
   BfsCounters* ctr = nullptr;
   BfsCounters* hctr = nullptr;
+  unsigned long long* trace = nullptr;  // per-level timestamps of the last full BFS
   BfsTuning tune;
   int grid = 0;
 };
@@ -70,5 +71,8 @@ int bfs_recompute(Bfs* b);
 int bfs_apply_staged(Bfs* b, size_t n, size_t vertex_bound);
 int bfs_sync(Bfs* b);  // copies counters to hctr (synchronises the stream)
 int bfs_reached_arcs(Bfs* b, unsigned long long* arcs);  // sum of degrees of reached vertices
+// Per-level trace of the last full BFS: pairs {globaltimer ns, n_f | bottom_up << 63}
+// for every level, then a closing timestamp.  Writes up to cap u64 values.
+int bfs_level_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n);
 
 }  // namespace vxh

@@ -241,6 +241,19 @@ PYBIND11_MODULE(_velographx, m) {
              detail::check(vx_bfs_reached_arcs(x.handle(), &a));
              return a;
            })
+      .def("level_trace",
+           [](IncrementalBFS& x) {
+             std::size_t n = 0;
+             detail::check(vx_bfs_level_trace(x.handle(), nullptr, 0, &n));
+             std::vector<std::uint64_t> t(n);
+             if (n) detail::check(vx_bfs_level_trace(x.handle(), t.data(), n, &n));
+             py::list out;
+             const std::size_t stamps = n / 2;  // levels + closing timestamp
+             for (std::size_t i = 0; i + 1 < stamps; ++i)
+               out.append(py::make_tuple(static_cast<double>(t[2 * (i + 1)] - t[2 * i]) * 1e-3,
+                                         t[2 * i + 1] & 0x7FFFFFFFFFFFFFFFull, (t[2 * i + 1] >> 63) != 0));
+             return out;
+           })
       .def("set_tuning", [](IncrementalBFS& x, float alpha, float beta, std::uint32_t large_row) {
         detail::check(vx_bfs_set_tuning(x.handle(), alpha, beta, large_row));
       }, py::arg("alpha"), py::arg("beta"), py::arg("large_row"));
