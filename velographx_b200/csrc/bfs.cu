@@ -226,6 +226,19 @@ struct TdVisit {
 __device__ void td_level(const Params& p, TdVisit& t, const uint32_t* qin, uint32_t n_f, uint32_t* cnt_big) {
   const DevAdj& a = p.g.out;
   const int lane = threadIdx.x & 31;
+  if (n_f <= nwarps()) {
+    // small frontier: one warp per vertex, so no warp walks several rows
+    for (uint32_t i = gwarp(); i < n_f; i += nwarps()) {
+      const uint32_t u = qin[i];
+      const bool big = degree_of(a, u) >= p.large_row;
+      if (big) {
+        if (lane == 0) p.big[atomicAdd(cnt_big, 1u)] = u;
+        continue;
+      }
+      warp_row(a, u, t);
+    }
+    return;
+  }
   for (uint32_t base = gwarp() * 32; base < n_f; base += nwarps() * 32) {
     const uint32_t i = base + lane;
     const bool act = i < n_f;
@@ -294,12 +307,16 @@ __device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, u
     const uint32_t nb = (uint32_t)(e - b), total = nb + dr.y;
     bool found = false;
     if (todo && total <= 32) {
-      for (uint32_t k = 0; k < total; ++k) {
-        const uint32_t x = k < nb ? a.col[b + k] : a.darena[dr.x + (k - nb)];
-        if (!(x & kTomb) && test_bit(fbc, x)) {
-          found = true;
-          break;
+      // four independent loads in flight per step
+      for (uint32_t k = 0; k < total && !found; k += 4) {
+        uint32_t x[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const uint32_t kk = k + j;
+          x[j] = kk >= total ? kTomb : (kk < nb ? a.col[b + kk] : a.darena[dr.x + (kk - nb)]);
         }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) found = found || (!(x[j] & kTomb) && test_bit(fbc, x[j]));
       }
     }
     uint32_t longm = __ballot_sync(FULL, todo && total > 32);
@@ -443,25 +460,13 @@ __device__ __forceinline__ bool is_sp(const Params& p, uint32_t u, uint32_t v) {
   return du != kUnreachable && dv != kUnreachable && du + 1 == dv;
 }
 
-// Is (u, v) a final deletion of the staged batch?  fu/fv sorted by (u, v).
-__device__ bool is_final_deletion(const Params& p, uint32_t F, uint32_t u, uint32_t v) {
-  uint32_t lo = 0, hi = F;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    const uint32_t mu = p.fu[mid], mv = p.fv[mid];
-    if (mu < u || (mu == u && mv < v)) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo < F && p.fu[lo] == u && p.fv[lo] == v && !(p.ff[lo] & kFAdd);
-}
-
-// Does v (at distance d >= 1) keep a shortest parent in the pre-batch graph:
-// an in-neighbour x at distance d-1 that is not affected and whose arc (x, v)
-// is not deleted by the batch?  Whole warp, stops at the first such parent.
+// Does v (at distance d >= 1) keep a shortest parent: an in-neighbour x at
+// distance d-1 that is not affected, in the pre-batch graph minus the batch's
+// deletions (already committed)?  Whole warp, stops at the first such parent.
 // "v has none" is exactly the reference's lost >= support test
 // (bfs.hpp:229-240): lost counts every shortest parent that is deleted or
 // affected, each once, and support counts all of them.
-__device__ bool warp_has_surviving_parent(const Params& p, uint32_t v, uint32_t d, uint32_t F) {
+__device__ bool warp_has_surviving_parent(const Params& p, uint32_t v, uint32_t d) {
   const DevAdj& a = p.g.in;
   const int lane = threadIdx.x & 31;
   uint64_t b, e;
@@ -480,7 +485,7 @@ __device__ bool warp_has_surviving_parent(const Params& p, uint32_t v, uint32_t 
       } else {
         x = a.darena[dr.x + (uint32_t)(k - nb)];
       }
-      ok = valid && x < p.dist_len && p.dist[x] + 1 == d && !test_bit(p.aff, x) && !is_final_deletion(p, F, x, v);
+      ok = valid && x < p.dist_len && p.dist[x] + 1 == d && !test_bit(p.aff, x);
     }
     if (__any_sync(FULL, ok)) return true;
   }
@@ -570,7 +575,7 @@ __device__ void repair_pre(const Params& p) {
         const int l = __ffs(m) - 1;
         m &= m - 1;
         const uint32_t vv = __shfl_sync(FULL, v, l);
-        if (!warp_has_surviving_parent(p, vv, d, F) && lane == 0) mark_affected(p, vv);
+        if (!warp_has_surviving_parent(p, vv, d) && lane == 0) mark_affected(p, vv);
       }
     }
     // children touched at the previous level
@@ -582,7 +587,7 @@ __device__ void repair_pre(const Params& p) {
         const int l = __ffs(m) - 1;
         m &= m - 1;
         const uint32_t vv = __shfl_sync(FULL, v, l);
-        if (!warp_has_surviving_parent(p, vv, d, F) && lane == 0) mark_affected(p, vv);
+        if (!warp_has_surviving_parent(p, vv, d) && lane == 0) mark_affected(p, vv);
       }
     }
     if (!sync_grid(p)) return;
@@ -832,7 +837,7 @@ __device__ void repair_post(const Params& p) {
   clear_workspace(p);
 }
 
-__global__ void __launch_bounds__(kThreads, 2) bfs_kernel(Params p, int mode) {
+__global__ void __launch_bounds__(kThreads, 3) bfs_kernel(Params p, int mode) {
   if (mode == kModeFull) full_bfs(p);
   else if (mode == kModePre) repair_pre(p);
   else repair_post(p);
@@ -1014,13 +1019,17 @@ int bfs_apply_staged(Bfs* b, size_t n, size_t vertex_bound) {
   // fallback limit: max(1, size_t(double(V) * fraction))  (bfs.hpp:225-226)
   unsigned long long lim = (unsigned long long)((double)V_pre * b->frac);
   if (lim < 1) lim = 1;
+  // The fixpoint reads the pre-batch graph without the batch's deletions
+  // (exactly the arcs the reference's support count and child propagation
+  // exclude), so removals are committed first and insertions after it.
+  if (int rc = graph_commit_removals(g)) return rc;
   {
     Params p = make_params(b, (uint32_t)V_pre, (uint32_t)len_pre);
     p.fallback_limit = lim;
     if (len_pre > 0)
       if (int rc = launch(b, p, kModePre)) return rc;
   }
-  if (int rc = graph_commit_batch(g)) return rc;
+  if (int rc = graph_commit_insertions(g)) return rc;
   if (b->dist_len < V_post) {
     VX_CUDA_TRY(cudaMemsetAsync(b->dist + b->dist_len, 0xFF, (V_post - b->dist_len) * 4, s));
     b->dist_len = V_post;
@@ -1043,7 +1052,7 @@ int bfs_sync(Bfs* b) {
 
 int bfs_reached_arcs(Bfs* b, unsigned long long* arcs) {
   cudaStream_t s = b->g->stream;
-  unsigned long long* d = reinterpret_cast<unsigned long long*>(&b->ctr->pad);
+  unsigned long long* d = &b->ctr->scratch64;
   VX_CUDA_TRY(cudaMemsetAsync(d, 0, 8, s));
   vxh::count_launch();
   reached_arcs_kernel<<<sm_count() * 8, 256, 0, s>>>(b->g->view().out, b->dist, (uint32_t)b->dist_len, d);

@@ -30,13 +30,13 @@ struct BfsCounters {
   uint32_t next_seed[3]; // smallest pending seed level (rotating)
   uint32_t seed_min;     // smallest seed level of the settle phase
   uint32_t bar[2];       // grid barrier {arrive, generation}
-  uint32_t pad[2];
+  unsigned long long scratch64;  // single-value readbacks
 };
 
 struct BfsTuning {
   float alpha = 14.0f;       // top-down -> bottom-up when m_f * alpha > m_u
   float beta = 24.0f;        // bottom-up -> top-down when n_f * beta < V (shrinking)
-  uint32_t large_row = 4096; // rows this long are expanded by the whole grid
+  uint32_t large_row = 1024; // rows this long are expanded by the whole grid
 };
 
 struct Bfs {

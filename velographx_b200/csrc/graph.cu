@@ -251,13 +251,16 @@ __global__ void count_valid_kernel(const uint64_t* keys, size_t m, uint32_t* fla
 
 // --------------------------------------------------------- batch commit --
 
+// mode 0: tombstone base arcs the batch deletes; mode 1: revive base arcs it re-adds.
 __global__ void tomb_kernel(DevAdj a, const uint32_t* fu, const uint8_t* ff, const uint64_t* fpos,
-                            const uint32_t* count, unsigned long long* tombs, unsigned long long* dirty_rows) {
+                            const uint32_t* count, int mode, unsigned long long* tombs,
+                            unsigned long long* dirty_rows) {
   const uint32_t F = *count;
   long long delta = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x) {
     const uint8_t f = ff[i];
     if (!(f & vxh::kFInBase) || !(f & vxh::kFChanged)) continue;
+    if (((f & vxh::kFAdd) != 0) != (mode == 1)) continue;
     const uint64_t p = fpos[i];
     const uint32_t u = fu[i];
     if (f & vxh::kFAdd) {
@@ -819,7 +822,7 @@ int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound) {
       if (int rc = reserve_arena(g, g->adj[d], m, &consolidate)) return rc;
   }
   if (int rc = graph_grow(g, std::max<size_t>(g->V, vertex_bound))) return rc;
-  VX_CUDA_TRY(cudaMemsetAsync(&g->ctr->final_arcs, 0, 6 * sizeof(uint32_t), s));
+  VX_CUDA_TRY(cudaMemsetAsync(&g->ctr->final_arcs, 0, 5 * sizeof(uint32_t), s));
   const int b = bits_for(std::max<size_t>(g->V, 2));
   if (n == 0) return 0;
   vxh::count_launch();
@@ -843,76 +846,90 @@ int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound) {
 }
 
 // Applies one canonical arc list (u, v, flags, base positions) to adjacency a.
+// Applies one half of a canonical arc list (u, v, flags, base positions) to
+// adjacency a: mode 0 the deletions (tombstones, delta removals), mode 1 the
+// insertions (revived tombstones, delta insertions).
 static int commit_list(Graph* g, Adjacency& a, int dir, uint32_t* fu, uint32_t* fv, uint8_t* ff, uint64_t* fpos,
-                       const uint32_t* count, size_t m) {
+                       const uint32_t* count, size_t m, int mode) {
   cudaStream_t s = g->stream;
   BatchBuffers& B = g->batch;
   GraphCounters* c = g->ctr;
   DevAdj da = devadj(a);
   vxh::count_launch();
-  tomb_kernel<<<grid_for(m), kBlock, 0, s>>>(da, fu, ff, fpos, count, &c->tombs[dir], &c->dirty_rows[dir]);
-  for (int mode = 0; mode < 2; ++mode) {
-    uint32_t* nlist = mode == 0 ? &c->rm_arcs : &c->ins_arcs;
-    uint32_t* nruns = mode == 0 ? &c->rm_runs : &c->ins_runs;
-    vxh::count_launch();
-    delta_flag_kernel<<<grid_for(m), kBlock, 0, s>>>(ff, count, m, mode, B.flag);
-    if (int rc = scan_count(g, B.flag, B.pos, m, nlist)) return rc;
-    vxh::count_launch();
-    compact_pairs_kernel<<<grid_for(m), kBlock, 0, s>>>(fu, fv, B.flag, B.pos, m, B.lu, B.lv);
-    vxh::count_launch();
-    run_flag_kernel<<<grid_for(m), kBlock, 0, s>>>(B.lu, nlist, m, B.flag);
-    if (int rc = scan_count(g, B.flag, B.pos, m, nruns)) return rc;
-    vxh::count_launch();
-    compact_index_kernel<<<grid_for(m), kBlock, 0, s>>>(B.flag, B.pos, m, B.runs);
-    const unsigned wg = grid_for(m * 32, kBlock);
-    vxh::count_launch();
-    if (mode == 0)
-      delta_remove_kernel<<<wg, kBlock, 0, s>>>(da, B.lu, B.lv, B.runs, nruns, nlist, &c->delta_live[dir],
-                                                &c->dirty_rows[dir]);
-    else
-      delta_insert_kernel<<<wg, kBlock, 0, s>>>(da, a.arena_cap, B.lu, B.lv, B.runs, nruns, nlist,
-                                                &c->arena_top[dir], &c->delta_live[dir], &c->dirty_rows[dir],
-                                                &c->err);
-    VX_CUDA_TRY(cudaGetLastError());
-  }
-  a.arena_bound += 8ull * m + 8;
+  tomb_kernel<<<grid_for(m), kBlock, 0, s>>>(da, fu, ff, fpos, count, mode, &c->tombs[dir], &c->dirty_rows[dir]);
+  uint32_t* nlist = mode == 0 ? &c->rm_arcs : &c->ins_arcs;
+  uint32_t* nruns = mode == 0 ? &c->rm_runs : &c->ins_runs;
+  vxh::count_launch();
+  delta_flag_kernel<<<grid_for(m), kBlock, 0, s>>>(ff, count, m, mode, B.flag);
+  if (int rc = scan_count(g, B.flag, B.pos, m, nlist)) return rc;
+  vxh::count_launch();
+  compact_pairs_kernel<<<grid_for(m), kBlock, 0, s>>>(fu, fv, B.flag, B.pos, m, B.lu, B.lv);
+  vxh::count_launch();
+  run_flag_kernel<<<grid_for(m), kBlock, 0, s>>>(B.lu, nlist, m, B.flag);
+  if (int rc = scan_count(g, B.flag, B.pos, m, nruns)) return rc;
+  vxh::count_launch();
+  compact_index_kernel<<<grid_for(m), kBlock, 0, s>>>(B.flag, B.pos, m, B.runs);
+  const unsigned wg = grid_for(m * 32, kBlock);
+  vxh::count_launch();
+  if (mode == 0)
+    delta_remove_kernel<<<wg, kBlock, 0, s>>>(da, B.lu, B.lv, B.runs, nruns, nlist, &c->delta_live[dir],
+                                              &c->dirty_rows[dir]);
+  else
+    delta_insert_kernel<<<wg, kBlock, 0, s>>>(da, a.arena_cap, B.lu, B.lv, B.runs, nruns, nlist,
+                                              &c->arena_top[dir], &c->delta_live[dir], &c->dirty_rows[dir],
+                                              &c->err);
+  VX_CUDA_TRY(cudaGetLastError());
+  if (mode == 1) a.arena_bound += 8ull * m + 8;
+  return 0;
+}
+
+// Reversed changed arcs (v, u) of a directed batch, sorted by (v, u) and
+// classified against the in-CSR (before either adjacency changes).
+static int prepare_reverse(Graph* g, size_t m) {
+  cudaStream_t s = g->stream;
+  BatchBuffers& B = g->batch;
+  const int b = bits_for(std::max<size_t>(g->V, 2));
+  vxh::count_launch();
+  reverse_keys_kernel<<<grid_for(m), kBlock, 0, s>>>(B.fu, B.fv, B.ff, &g->ctr->final_arcs, m, b, B.keys, B.vals);
+  bool in_alt = false;
+  if (int rc = radix_sort_u64(B.keys, B.keys_alt, B.vals, B.vals_alt, m, 2 * b, &in_alt, g->scratch, s)) return rc;
+  uint64_t* keys = in_alt ? B.keys_alt : B.keys;
+  uint32_t* vals = in_alt ? B.vals_alt : B.vals;
+  vxh::count_launch();
+  count_valid_kernel<<<grid_for(m), kBlock, 0, s>>>(keys, m, B.flag);
+  if (int rc = scan_count(g, B.flag, B.pos, m, &g->ctr->rev_arcs)) return rc;
+  vxh::count_launch();
+  compact_final_kernel<<<grid_for(m), kBlock, 0, s>>>(keys, vals, B.flag, B.pos, m, b, B.ru, B.rv, B.rf);
+  vxh::count_launch();
+  classify_kernel<<<grid_for(m), kBlock, 0, s>>>(devadj(g->adj[1]), B.ru, B.rv, B.rf, B.rpos, &g->ctr->rev_arcs);
+  VX_CUDA_TRY(cudaGetLastError());
+  return 0;
+}
+
+static int commit_half(Graph* g, int mode) {
+  const size_t n = g->batch_ops;
+  if (n == 0) return 0;
+  BatchBuffers& B = g->batch;
+  const size_t m = g->directed ? n : 2 * n;
+  if (mode == 0 && g->directed)
+    if (int rc = prepare_reverse(g, m)) return rc;
+  if (int rc = commit_list(g, g->adj[0], 0, B.fu, B.fv, B.ff, B.fpos, &g->ctr->final_arcs, m, mode)) return rc;
+  if (g->directed)
+    if (int rc = commit_list(g, g->adj[1], 1, B.ru, B.rv, B.rf, B.rpos, &g->ctr->rev_arcs, m, mode)) return rc;
+  return 0;
+}
+
+int graph_commit_removals(Graph* g) { return commit_half(g, 0); }
+
+int graph_commit_insertions(Graph* g) {
+  if (int rc = commit_half(g, 1)) return rc;
+  if (g->batch_ops) ++g->version;
   return 0;
 }
 
 int graph_commit_batch(Graph* g) {
-  const size_t n = g->batch_ops;
-  if (n == 0) return 0;
-  cudaStream_t s = g->stream;
-  BatchBuffers& B = g->batch;
-  const size_t m = g->directed ? n : 2 * n;
-  if (g->directed) {
-    // reversed changed arcs, sorted by (v, u), classified against the in-CSR
-    const int b = bits_for(std::max<size_t>(g->V, 2));
-    vxh::count_launch();
-    reverse_keys_kernel<<<grid_for(m), kBlock, 0, s>>>(B.fu, B.fv, B.ff, &g->ctr->final_arcs, m, b, B.keys,
-                                                       B.vals);
-    bool in_alt = false;
-    if (int rc = radix_sort_u64(B.keys, B.keys_alt, B.vals, B.vals_alt, m, 2 * b, &in_alt, g->scratch, s))
-      return rc;
-    uint64_t* keys = in_alt ? B.keys_alt : B.keys;
-    uint32_t* vals = in_alt ? B.vals_alt : B.vals;
-    vxh::count_launch();
-    count_valid_kernel<<<grid_for(m), kBlock, 0, s>>>(keys, m, B.flag);
-    uint32_t* rcount = &g->ctr->pad;
-    if (int rc = scan_count(g, B.flag, B.pos, m, rcount)) return rc;
-    vxh::count_launch();
-    compact_final_kernel<<<grid_for(m), kBlock, 0, s>>>(keys, vals, B.flag, B.pos, m, b, B.ru, B.rv, B.rf);
-    vxh::count_launch();
-    classify_kernel<<<grid_for(m), kBlock, 0, s>>>(devadj(g->adj[1]), B.ru, B.rv, B.rf, B.rpos, rcount);
-    VX_CUDA_TRY(cudaGetLastError());
-    // out-adjacency first (the in-list was derived from its pre-batch flags)
-    if (int rc = commit_list(g, g->adj[0], 0, B.fu, B.fv, B.ff, B.fpos, &g->ctr->final_arcs, m)) return rc;
-    if (int rc = commit_list(g, g->adj[1], 1, B.ru, B.rv, B.rf, B.rpos, rcount, m)) return rc;
-  } else {
-    if (int rc = commit_list(g, g->adj[0], 0, B.fu, B.fv, B.ff, B.fpos, &g->ctr->final_arcs, m)) return rc;
-  }
-  ++g->version;
-  return 0;
+  if (int rc = graph_commit_removals(g)) return rc;
+  return graph_commit_insertions(g);
 }
 
 int graph_consolidate(Graph* g) {
@@ -963,7 +980,7 @@ int graph_consolidate(Graph* g) {
 int graph_maybe_compact(Graph* g, double threshold, int* compacted) {
   *compacted = 0;
   cudaStream_t s = g->stream;
-  uint32_t* flag = reinterpret_cast<uint32_t*>(&g->ctr->pad);
+  uint32_t* flag = &g->ctr->scratch32;
   VX_CUDA_TRY(cudaMemsetAsync(flag, 0, 4, s));
   for (int d = 0; d < (g->directed ? 2 : 1); ++d) {
     vxh::count_launch();
@@ -1013,7 +1030,7 @@ int graph_row(Graph* g, int dir, uint32_t u, uint32_t* host_out, size_t cap, siz
 int graph_has_edge(Graph* g, uint32_t u, uint32_t v, int* out) {
   *out = 0;
   if (u >= g->V) return 0;
-  uint32_t* r = reinterpret_cast<uint32_t*>(&g->ctr->pad);
+  uint32_t* r = &g->ctr->scratch32;
   vxh::count_launch();
   has_edge_kernel<<<1, 1, 0, g->stream>>>(devadj(g->adj[0]), u, v, r);
   VX_CUDA_TRY(cudaMemcpyAsync(g->pinned_scalar, r, 4, cudaMemcpyDeviceToHost, g->stream));

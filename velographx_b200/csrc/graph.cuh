@@ -23,7 +23,8 @@ struct GraphCounters {
   uint32_t rm_runs, ins_runs;        // row runs among them
   uint32_t err;                      // vxb::kErr* bits
   uint32_t max_vertex_plus1;         // max(src,dst)+1 over non-self-loop ops
-  uint32_t pad;
+  uint32_t rev_arcs;                 // reversed changed arcs (directed graphs)
+  uint32_t scratch32;                // single-value readbacks (has_edge, maybe_compact)
 };
 
 struct Adjacency {
@@ -101,8 +102,11 @@ int graph_bulk_load(Graph* g, const uint32_t* d_uv, size_t n_edges);
 // Stage a batch already in g->batch.{src,dst,add}: canonicalise + classify on
 // the pre-batch graph.  vertex_bound bounds every non-self-loop id + 1.
 int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound);
-// Apply the staged batch to the device structure (after any pre-batch reads).
+// Apply the staged batch to the device structure (after any pre-batch reads):
+// removals first (tombstones, delta removals), then insertions.
 int graph_commit_batch(Graph* g);
+int graph_commit_removals(Graph* g);
+int graph_commit_insertions(Graph* g);
 int graph_consolidate(Graph* g);
 // maybe_compact(threshold) (dynamic_graph.hpp:620-631, 764-789): consolidates when
 // any dirty row's overlay density reaches the threshold; *compacted = 1 then.

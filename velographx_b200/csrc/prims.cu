@@ -156,85 +156,103 @@ __device__ __forceinline__ uint32_t digit_of(uint64_t k, int shift) {
   return (uint32_t)(k >> shift) & 0xFFu;
 }
 
-// Ranks one round of BLOCK items (one per thread, position order = thread
-// order).  `run[d]` holds the count of digit d in earlier rounds of the tile
-// and is advanced here.  Returns the rank of the thread's item among items of
-// its digit (earlier rounds + earlier threads).  Items with valid == false
-// still take part (they carry the largest digit and come last in order).
-template <int BLOCK>
-__device__ uint32_t rank_round(uint32_t d, uint32_t* warp_cnt /*[BLOCK/32][256]*/, uint32_t* run) {
+// Stable block-wide digit ranking with warp-private histograms.
+//
+// Warp w owns the ITEMS*32 consecutive tile positions starting at
+// w*ITEMS*32; round r of the warp holds positions w*ITEMS*32 + r*32 + lane.
+// Each warp ranks its own items in position order (match_any peers + a
+// private 256-bin histogram, no block barrier), then one pass over the
+// histograms gives every warp its per-digit offset.  The returned rank of an
+// item is its position among equal digits of the tile (earlier warps, earlier
+// rounds, lower lanes first), and digit_total[d] the tile's count of digit d.
+template <int BLOCK, int ITEMS>
+__device__ void rank_tile(const uint32_t (&d)[ITEMS], uint32_t (&rank)[ITEMS], uint32_t* warp_hist /*[W][256]*/,
+                          uint32_t* digit_total /*[256]*/) {
   constexpr int W = BLOCK / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  __syncthreads();  // previous round's readers of warp_cnt are done
-  for (int i = threadIdx.x; i < W * kDigits; i += BLOCK) warp_cnt[i] = 0;
-  __syncthreads();
-  const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-  const uint32_t lane_rank = __popc(peers & vxb::lanemask_lt());
-  if (lane == __ffs(peers) - 1) warp_cnt[warp * kDigits + d] = __popc(peers);
-  __syncthreads();
-  for (int dd = threadIdx.x; dd < kDigits; dd += BLOCK) {
-    uint32_t s = run[dd];
-    for (int w = 0; w < W; ++w) {
-      const uint32_t c = warp_cnt[w * kDigits + dd];
-      warp_cnt[w * kDigits + dd] = s;
-      s += c;
-    }
-    run[dd] = s;
+  uint32_t* h = warp_hist + warp * kDigits;
+  for (int i = lane; i < kDigits; i += 32) h[i] = 0;
+  __syncwarp();
+#pragma unroll
+  for (int r = 0; r < ITEMS; ++r) {
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d[r]);
+    const uint32_t base = h[d[r]];
+    __syncwarp();
+    if (lane == __ffs(peers) - 1) h[d[r]] = base + __popc(peers);
+    __syncwarp();
+    rank[r] = base + __popc(peers & vxb::lanemask_lt());
   }
   __syncthreads();
-  return warp_cnt[warp * kDigits + d] + lane_rank;
+  for (int dd = threadIdx.x; dd < kDigits; dd += BLOCK) {
+    uint32_t s = 0;
+#pragma unroll 4
+    for (int w = 0; w < W; ++w) {
+      const uint32_t c = warp_hist[w * kDigits + dd];
+      warp_hist[w * kDigits + dd] = s;
+      s += c;
+    }
+    digit_total[dd] = s;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < ITEMS; ++r) rank[r] += h[d[r]];
 }
 
 // Whole sort inside one CTA.  Shared layout: keys[kSmallN] u64, vals[kSmallN]
-// u32, warp_cnt[32*256], run[256], digit_base[256].
+// u32, warp_hist[32*256], digit_total[256], digit_base[256].
 __global__ void __launch_bounds__(kSmallBlock) small_sort_kernel(uint64_t* keys, uint32_t* vals, size_t n,
                                                                   int passes) {
   extern __shared__ __align__(16) unsigned char smem[];
   uint64_t* sk = reinterpret_cast<uint64_t*>(smem);
   uint32_t* sv = reinterpret_cast<uint32_t*>(sk + kSmallN);
-  uint32_t* warp_cnt = sv + kSmallN;
-  uint32_t* run = warp_cnt + (kSmallBlock / 32) * kDigits;
-  uint32_t* dbase = run + kDigits;
+  uint32_t* warp_hist = sv + kSmallN;
+  uint32_t* total = warp_hist + (kSmallBlock / 32) * kDigits;
+  uint32_t* dbase = total + kDigits;
   for (size_t i = threadIdx.x; i < kSmallN; i += kSmallBlock) {
     sk[i] = i < n ? keys[i] : ~0ull;
     if (vals) sv[i] = i < n ? vals[i] : 0u;
   }
   __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int pos0 = warp * kSmallItems * 32 + lane;
   for (int p = 0; p < passes; ++p) {
     const int shift = p * 8;
     uint64_t k[kSmallItems];
-    uint32_t v[kSmallItems];
-    uint32_t d[kSmallItems];
-    for (int i = threadIdx.x; i < kDigits; i += kSmallBlock) {
-      run[i] = 0;
-      dbase[i] = 0;
-    }
-    __syncthreads();
+    uint32_t v[kSmallItems], d[kSmallItems], rank[kSmallItems];
 #pragma unroll
     for (int r = 0; r < kSmallItems; ++r) {
-      const int idx = r * kSmallBlock + threadIdx.x;
-      k[r] = sk[idx];
-      v[r] = vals ? sv[idx] : 0u;
+      k[r] = sk[pos0 + r * 32];
+      v[r] = vals ? sv[pos0 + r * 32] : 0u;
       d[r] = digit_of(k[r], shift);
-      atomicAdd(&dbase[d[r]], 1u);
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t s = 0;
-      for (int i = 0; i < kDigits; ++i) {
-        const uint32_t c = dbase[i];
-        dbase[i] = s;
-        s += c;
+    rank_tile<kSmallBlock, kSmallItems>(d, rank, warp_hist, total);
+    if (threadIdx.x < 32) {
+      // exclusive scan of the 256 digit totals by one warp (8 per lane)
+      uint32_t loc[8], run = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        loc[j] = total[threadIdx.x * 8 + j];
+        run += loc[j];
+      }
+      uint32_t incl = run;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (threadIdx.x >= o) incl += y;
+      }
+      uint32_t ex = incl - run;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        dbase[threadIdx.x * 8 + j] = ex;
+        ex += loc[j];
       }
     }
     __syncthreads();
-    uint32_t rank[kSmallItems];
-#pragma unroll
-    for (int r = 0; r < kSmallItems; ++r) rank[r] = dbase[d[r]] + rank_round<kSmallBlock>(d[r], warp_cnt, run);
 #pragma unroll
     for (int r = 0; r < kSmallItems; ++r) {
-      sk[rank[r]] = k[r];
-      if (vals) sv[rank[r]] = v[r];
+      const uint32_t dst = dbase[d[r]] + rank[r];
+      sk[dst] = k[r];
+      if (vals) sv[dst] = v[r];
     }
     __syncthreads();
   }
@@ -246,6 +264,7 @@ __global__ void __launch_bounds__(kSmallBlock) small_sort_kernel(uint64_t* keys,
 
 constexpr size_t kSmallSmem =
     kSmallN * 8 + kSmallN * 4 + (kSmallBlock / 32) * kDigits * 4 + kDigits * 4 * 2;
+static_assert(kSmallSmem <= 227 * 1024, "small sort exceeds shared memory");
 
 __global__ void __launch_bounds__(kBigBlock) radix_hist_kernel(const uint64_t* keys, size_t n, int shift,
                                                                uint32_t* hist, uint32_t nblk) {
@@ -266,26 +285,29 @@ __global__ void __launch_bounds__(kBigBlock) radix_scatter_kernel(const uint64_t
                                                                   uint64_t* keys_out, uint32_t* vals_out,
                                                                   size_t n, int shift,
                                                                   const uint32_t* offsets, uint32_t nblk) {
-  __shared__ uint32_t warp_cnt[(kBigBlock / 32) * kDigits];
-  __shared__ uint32_t run[kDigits];
+  __shared__ uint32_t warp_hist[(kBigBlock / 32) * kDigits];
+  __shared__ uint32_t total[kDigits];
   __shared__ uint32_t gbase[kDigits];
-  for (int i = threadIdx.x; i < kDigits; i += kBigBlock) {
-    run[i] = 0;
-    gbase[i] = offsets[(size_t)i * nblk + blockIdx.x];
-  }
-  __syncthreads();
-  const size_t base = (size_t)blockIdx.x * kBigTile;
+  for (int i = threadIdx.x; i < kDigits; i += kBigBlock) gbase[i] = offsets[(size_t)i * nblk + blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const size_t pos0 = (size_t)blockIdx.x * kBigTile + warp * kBigItems * 32 + lane;
+  uint64_t k[kBigItems];
+  uint32_t v[kBigItems], d[kBigItems], rank[kBigItems];
+#pragma unroll
   for (int r = 0; r < kBigItems; ++r) {
-    const size_t idx = base + (size_t)r * kBigBlock + threadIdx.x;
+    const size_t idx = pos0 + r * 32;
     const bool valid = idx < n;
-    const uint64_t k = valid ? keys[idx] : ~0ull;
-    const uint32_t v = (valid && vals) ? vals[idx] : 0u;
-    const uint32_t d = valid ? digit_of(k, shift) : 255u;
-    const uint32_t rk = rank_round<kBigBlock>(d, warp_cnt, run);
-    if (valid) {
-      const uint32_t dst = gbase[d] + rk;
-      keys_out[dst] = k;
-      if (vals) vals_out[dst] = v;
+    k[r] = valid ? keys[idx] : ~0ull;
+    v[r] = (valid && vals) ? vals[idx] : 0u;
+    d[r] = valid ? digit_of(k[r], shift) : 255u;
+  }
+  rank_tile<kBigBlock, kBigItems>(d, rank, warp_hist, total);
+#pragma unroll
+  for (int r = 0; r < kBigItems; ++r) {
+    if (pos0 + r * 32 < n) {
+      const uint32_t dst = gbase[d[r]] + rank[r];
+      keys_out[dst] = k[r];
+      if (vals) vals_out[dst] = v[r];
     }
   }
 }
