@@ -217,3 +217,27 @@ def test_capi_direct_calls():
     assert n.value == 4 and out.tolist() == [0, 1, 2, 3]
     lib.vx_bfs_destroy(b)
     lib.vx_graph_destroy(g)
+
+
+@pytest.mark.parametrize("directed", [False, True])
+def test_large_batches_use_the_multipass_path(directed):
+    """Batches above one cluster's capacity (~90k arcs) take the multi-kernel
+    sort path; results must be the same."""
+    from velographx_b200 import workloads as w
+
+    V = 1 << 15
+    e = w.rmat_edges(15, seed=31)
+    og = OracleGraph(V, directed, "port")
+    og.bulk_load_edges(e)
+    ob = OracleBFS(og, 0, 0.35)
+    g = vx.Graph(V, directed)
+    g.bulk_load_edges(e)
+    b = vx.IncrementalBFS(g, 0, 0.35)
+    st = w.mixed_stream(e, V, [100_000, 3, 60_000], 0.6, seed=32)
+    for i in range(st.batches):
+        s, d, a = st.batch(i)
+        ob.apply(s, d, a)
+        b.apply_arrays(s, d, a)
+        assert np.array_equal(b.distances_array(), ob.distances()), i
+        assert b.reachable_count == ob.reachable_count
+        assert g.edge_count_directed() == og.edge_count_directed()

@@ -189,6 +189,49 @@ __device__ __forceinline__ uint64_t globaltimer() {
   return t;
 }
 
+// Block-aggregated frontier queue: warps reserve slots in shared memory
+// (shared atomics); the block flushes with one global atomic per phase.  Warps
+// that find the buffer full append straight to the global queue.
+constexpr uint32_t kBlockQueueCap = 2048;
+struct BlockQueue {
+  uint32_t cnt;
+  uint32_t gbase;
+  uint32_t items[kBlockQueueCap];
+};
+
+__device__ __forceinline__ void bq_push(BlockQueue& bq, bool pred, uint32_t v, uint32_t* gcnt, uint32_t* gq) {
+  const uint32_t mask = __ballot_sync(FULL, pred);
+  if (!mask) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  const uint32_t n = __popc(mask);
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(&bq.cnt, n);
+  base = __shfl_sync(FULL, base, leader);
+  const uint32_t r = __popc(mask & vxb::lanemask_lt());
+  const uint32_t spill = base + n > kBlockQueueCap ? base + n - max(base, kBlockQueueCap) : 0u;
+  uint32_t gb = 0;
+  if (spill && lane == leader) gb = atomicAdd(gcnt, spill);
+  gb = __shfl_sync(FULL, gb, leader);
+  if (pred) {
+    const uint32_t slot = base + r;
+    if (slot < kBlockQueueCap) bq.items[slot] = v;
+    else gq[gb + (slot - max(base, kBlockQueueCap))] = v;
+  }
+}
+
+// Block-uniform: moves the buffered entries to the global queue.
+__device__ __forceinline__ void bq_flush(BlockQueue& bq, uint32_t* gcnt, uint32_t* gq) {
+  __syncthreads();
+  const uint32_t n = min(bq.cnt, kBlockQueueCap);
+  if (threadIdx.x == 0) bq.gbase = n ? atomicAdd(gcnt, n) : 0u;
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) gq[bq.gbase + i] = bq.items[i];
+  __syncthreads();
+  if (threadIdx.x == 0) bq.cnt = 0;
+  __syncthreads();
+}
+
 // ------------------------------------------------------------ top-down --
 
 struct TdVisit {
@@ -199,6 +242,7 @@ struct TdVisit {
   uint32_t* cnt_n;
   bool want_deg;
   unsigned long long mloc;
+  BlockQueue* bq;
   // Claim x for the next level (warp-uniform).
   __device__ __forceinline__ void operator()(bool valid, uint32_t x, uint32_t) {
     bool claim = false;
@@ -212,8 +256,7 @@ struct TdVisit {
       atomicOr(&fbn[x >> 5], bit);
       if (want_deg) mloc += degree_of(p->g.out, x);
     }
-    const uint32_t slot = vxb::warp_append(claim, cnt_n);
-    if (claim) qout[slot] = x;
+    bq_push(*bq, claim, x, cnt_n, qout);
   }
   __device__ __forceinline__ void flush(unsigned long long* dst) {
     if (!want_deg) return;
@@ -289,7 +332,7 @@ __device__ void grid_rows(const DevAdj& a, const uint32_t* rows, uint32_t n, F& 
 // whole warp 32 arcs at a time; every scan stops at the first parent found in
 // the frontier bitmap.
 __device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, uint32_t* fbn, uint32_t* qout,
-                         uint32_t* cnt_n) {
+                         uint32_t* cnt_n, BlockQueue& bq) {
   const DevAdj& a = p.g.in;
   const int lane = threadIdx.x & 31;
   const uint32_t words = (p.V + 31) >> 5;
@@ -347,15 +390,17 @@ __device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, u
       p.vis[w] = visw | newly;
       fbn[w] = newly;
     }
-    const uint32_t slot = vxb::warp_append(found, cnt_n);
-    if (found) qout[slot] = v;
+    bq_push(bq, found, v, cnt_n, qout);
   }
+  bq_flush(bq, cnt_n, qout);
 }
 
 // ------------------------------------------------------------ full BFS --
 
 __device__ void full_bfs(const Params& p) {
+  __shared__ BlockQueue bq;
   BfsCounters* c = p.c;
+  if (threadIdx.x == 0) bq.cnt = 0;
   const uint32_t V = p.V;
   const uint32_t words = (V + 31) >> 5;
   for (uint32_t i = gtid(); i < V; i += nthreads()) p.dist[i] = kUnreachable;
@@ -425,17 +470,19 @@ __device__ void full_bfs(const Params& p) {
     // clear the frontier bitmap of level-1 through its queue
     for (uint32_t i = gtid(); i < prev_n; i += nthreads()) p.fb[clr][p.q[clr][i] >> 5] = 0u;
     if (bottom_up) {
-      bu_level(p, level, p.fb[cur], p.fb[nxt], p.q[nxt], &c->lvl_n[nxt]);
+      bu_level(p, level, p.fb[cur], p.fb[nxt], p.q[nxt], &c->lvl_n[nxt], bq);
       if (!sync_grid(p)) return;
     } else {
-      TdVisit t{&p, level, p.q[nxt], p.fb[nxt], &c->lvl_n[nxt], !left_bu, 0ull};
+      TdVisit t{&p, level, p.q[nxt], p.fb[nxt], &c->lvl_n[nxt], !left_bu, 0ull, &bq};
       td_level(p, t, p.q[cur], n_f, &c->lvl_big[cur]);
       t.flush(&c->lvl_m[nxt]);
+      bq_flush(bq, &c->lvl_n[nxt], p.q[nxt]);
       if (!sync_grid(p)) return;
       const uint32_t nbig = ld_cg(&c->lvl_big[cur]);
       if (nbig) {
         grid_rows(p.g.out, p.big, nbig, t);
         t.flush(&c->lvl_m[nxt]);
+        bq_flush(bq, &c->lvl_n[nxt], p.q[nxt]);
         if (!sync_grid(p)) return;
       }
     }
@@ -552,6 +599,12 @@ __device__ void repair_pre(const Params& p) {
   for (uint32_t i = gtid(); i < ncand; i += nthreads()) atomicMin(&c->seed_min, p.dist[p.lst_t[i]]);
   if (!sync_grid(p)) return;
   uint32_t d = ld_cg(&c->seed_min);
+  // level-d work list: candidates at d (and later the children touched at d)
+  for (uint32_t i = gtid(); i < ncand; i += nthreads()) {
+    const uint32_t v = p.lst_t[i];
+    if (p.dist[v] == d) p.q[0][atomicAdd(&c->list_n[0], 1u)] = v;
+  }
+  if (!sync_grid(p)) return;
   uint32_t a_prev = 0;
   for (uint32_t it = 0;; ++it) {
     if (it > p.dist_len + 1) {
@@ -564,31 +617,10 @@ __device__ void repair_pre(const Params& p) {
       c->list_n[k2] = 0;
       c->next_seed[k2] = kUnreachable;
     }
-    // candidates at distance d (32 per warp, each checked by the whole warp)
-    for (uint32_t base = gwarp() * 32; base < ncand; base += nwarps() * 32) {
-      const uint32_t i = base + lane;
-      const uint32_t v = i < ncand ? p.lst_t[i] : 0u;
-      const uint32_t dv = i < ncand ? p.dist[v] : kUnreachable;
-      if (dv != kUnreachable && dv > d) atomicMin(&c->next_seed[k1], dv);
-      uint32_t m = __ballot_sync(FULL, dv == d);
-      while (m) {
-        const int l = __ffs(m) - 1;
-        m &= m - 1;
-        const uint32_t vv = __shfl_sync(FULL, v, l);
-        if (!warp_has_surviving_parent(p, vv, d) && lane == 0) mark_affected(p, vv);
-      }
-    }
-    // children touched at the previous level
-    for (uint32_t base = gwarp() * 32; base < np; base += nwarps() * 32) {
-      const uint32_t i = base + lane;
-      const uint32_t v = i < np ? p.q[k][i] : 0u;
-      uint32_t m = __ballot_sync(FULL, i < np);
-      while (m) {
-        const int l = __ffs(m) - 1;
-        m &= m - 1;
-        const uint32_t vv = __shfl_sync(FULL, v, l);
-        if (!warp_has_surviving_parent(p, vv, d) && lane == 0) mark_affected(p, vv);
-      }
+    // every touched vertex at distance d: one warp each
+    for (uint32_t i = gwarp(); i < np; i += nwarps()) {
+      const uint32_t v = p.q[k][i];
+      if (!warp_has_surviving_parent(p, v, d) && lane == 0) mark_affected(p, v);
     }
     if (!sync_grid(p)) return;
     const uint32_t a_tot = ld_cg(&c->a_n);
@@ -596,15 +628,31 @@ __device__ void repair_pre(const Params& p) {
       if (gtid() == 0) c->fallback = 1;
       break;
     }
+    // next level's list: children of the vertices affected at d, candidates
+    // at d+1; the nearest deeper candidate level for a jump
     TouchChildren tc{&p, d, p.q[k1], &c->list_n[k1]};
     for (uint32_t i = a_prev + gwarp(); i < a_tot; i += nwarps()) warp_row(p.g.out, p.lst_a[i], tc);
+    for (uint32_t i = gtid(); i < ncand; i += nthreads()) {
+      const uint32_t v = p.lst_t[i];
+      const uint32_t dv = p.dist[v];
+      if (dv == d + 1) p.q[k1][atomicAdd(&c->list_n[k1], 1u)] = v;
+      else if (dv != kUnreachable && dv > d + 1) atomicMin(&c->next_seed[k1], dv);
+    }
     if (!sync_grid(p)) return;
     a_prev = a_tot;
     const uint32_t nn = ld_cg(&c->list_n[k1]);
+    if (nn > 0) {
+      ++d;
+      continue;
+    }
     const uint32_t ns = ld_cg(&c->next_seed[k1]);
-    if (nn > 0) ++d;
-    else if (ns != kUnreachable) d = ns;
-    else break;
+    if (ns == kUnreachable) break;
+    d = ns;  // no touched vertex at d+1: jump to the next candidate level
+    for (uint32_t i = gtid(); i < ncand; i += nthreads()) {
+      const uint32_t v = p.lst_t[i];
+      if (p.dist[v] == d) p.q[k1][atomicAdd(&c->list_n[k1], 1u)] = v;
+    }
+    if (!sync_grid(p)) return;
   }
   if (gtid() == 0) c->affected = ld_cg(&c->a_n);
 }

@@ -825,6 +825,9 @@ int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound) {
   VX_CUDA_TRY(cudaMemsetAsync(&g->ctr->final_arcs, 0, 5 * sizeof(uint32_t), s));
   const int b = bits_for(std::max<size_t>(g->V, 2));
   if (n == 0) return 0;
+  bool done = false;
+  if (int rc = canon_cluster(g, n, b, (uint32_t)g->V, &done)) return rc;
+  if (done) return 0;
   vxh::count_launch();
   expand_ops_kernel<<<grid_for(n), kBlock, 0, s>>>(B.src, B.dst, B.add, n, g->directed, b, (uint32_t)g->V,
                                                     B.keys, B.vals, g->ctr);

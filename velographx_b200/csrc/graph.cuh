@@ -108,6 +108,11 @@ int graph_commit_batch(Graph* g);
 int graph_commit_removals(Graph* g);
 int graph_commit_insertions(Graph* g);
 int graph_consolidate(Graph* g);
+// One-launch canonicalisation of the staged batch in a thread-block cluster
+// (sort, last-op-wins dedupe, compaction, classification); *done = false when
+// the batch exceeds one cluster's capacity.
+int canon_cluster(Graph* g, size_t n, int b, uint32_t bound, bool* done);
+size_t canon_cluster_capacity();
 // maybe_compact(threshold) (dynamic_graph.hpp:620-631, 764-789): consolidates when
 // any dirty row's overlay density reaches the threshold; *compacted = 1 then.
 int graph_maybe_compact(Graph* g, double threshold, int* compacted);
