@@ -647,6 +647,9 @@ __device__ void repair_pre(const Params& p) {
     }
     const uint32_t ns = ld_cg(&c->next_seed[k1]);
     if (ns == kUnreachable) break;
+    // every block must have read list_n[k1] == 0 before it is refilled, or a
+    // late block would see the refilled count and take the other branch
+    if (!sync_grid(p)) return;
     d = ns;  // no touched vertex at d+1: jump to the next candidate level
     for (uint32_t i = gtid(); i < ncand; i += nthreads()) {
       const uint32_t v = p.lst_t[i];
