@@ -185,11 +185,39 @@ def run_b200(args, rank, world, local):
     cs = torch.cuda.ExternalStream(g.stream)
     A = g.edge_count_directed()
 
+    # ---- autotune the direction switch (alpha, beta) on a few roots, untimed ----
+    def time_bfs(b):
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s0.record(cs)
+        b.recompute()
+        s1.record(cs)
+        s1.synchronize()
+        return s0.elapsed_time(s1)
+
+    tune_roots = roots[: min(4, len(roots))].tolist()
+    best, tuning = None, []
+    for alpha in (4.0, 14.0, 40.0, 120.0):
+        for beta in (8.0, 24.0, 96.0):
+            ts = []
+            for r in tune_roots:
+                b = vx.IncrementalBFS(g, int(r))
+                b.set_tuning(alpha, beta, 1024)
+                b.recompute()
+                ts.append(time_bfs(b))
+                del b
+            t = float(np.median(ts))
+            tuning.append((alpha, beta, round(t, 4)))
+            if best is None or t < best[2]:
+                best = (alpha, beta, t)
+    alpha, beta = best[0], best[1]
+
     # ---- direction-optimising full BFS from the roots (GTEPS, roofline) ----
     bfs_ms, arcs, levels = [], [], []
     trace = None
     for r in roots.tolist():
         b = vx.IncrementalBFS(g, int(r))
+        b.set_tuning(alpha, beta, 1024)
         b.recompute()  # warm
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -212,6 +240,7 @@ def run_b200(args, rank, world, local):
     # ---- update stream, device-resident batches (value) ----
     root = int(roots[0])
     b = vx.IncrementalBFS(g, root)
+    b.set_tuning(alpha, beta, 1024)
     ops = args.batch_ops
     dsrc = torch.from_numpy(stream.src.view(np.int32)).cuda()
     ddst = torch.from_numpy(stream.dst.view(np.int32)).cuda()
@@ -312,7 +341,8 @@ def run_b200(args, rank, world, local):
         },
         "bfs": {"roots": int(len(roots)), "gteps": gteps, "ms_mean": float(bfs_ms.mean()),
                 "ms_median": float(np.median(bfs_ms)), "levels_median": float(np.median(levels)),
-                "arcs": int(A), "level_trace_root0_us_nf_dir": trace},
+                "arcs": int(A), "level_trace_root0_us_nf_dir": trace,
+                "autotune": {"alpha": alpha, "beta": beta, "sweep_alpha_beta_ms": tuning}},
         "repair_last": {"affected": st["last_affected_vertices"], "candidates": st["last_deletion_candidates"],
                         "full": st["last_used_full_recompute"]},
         "clocks": clocks.summary(),

@@ -63,6 +63,7 @@ struct Params {
   uint32_t large_row;
   uint32_t nblocks;
   unsigned long long* trace;  // optional per-level {time, n_f | bottom-up << 63}
+  uint32_t* bar;              // grid barrier words
 };
 
 constexpr uint32_t kTraceLevels = 256;
@@ -77,7 +78,7 @@ __device__ __forceinline__ uint32_t nwarps() { return nthreads() >> 5; }
 // Grid barrier; returns false once any block recorded a device error (a
 // barrier that gave up waiting, a loop bound), so every persistent loop ends.
 __device__ __forceinline__ bool sync_grid(const Params& p) {
-  vxb::grid_barrier(p.c->bar, p.nblocks, &p.c->err);
+  vxb::grid_barrier(p.bar, p.nblocks, &p.c->err);
   return __ldcg(&p.c->err) == 0u;
 }
 
@@ -303,6 +304,96 @@ __device__ void td_level(const Params& p, TdVisit& t, const uint32_t* qin, uint3
   }
 }
 
+// Top-down expansion of a small frontier (n_f <= kLbMax) as one flat edge
+// space: every block stages the frontier's row ranges and their degree prefix
+// in shared memory, then each warp takes 32 consecutive edges per step and
+// finds their owners by binary search -- the same number of edges per warp
+// however skewed the rows are (a 30-vertex frontier of hubs included).
+constexpr uint32_t kLbMax = 1024;
+struct LbStage {
+  uint32_t pref[kLbMax + 1];
+  uint64_t base[kLbMax];
+  uint32_t blen[kLbMax];
+  uint32_t dx[kLbMax];
+};
+
+__device__ void td_level_lb(const Params& p, TdVisit& t, const uint32_t* qin, uint32_t n_f, LbStage& st) {
+  const DevAdj& a = p.g.out;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // stage: two frontier entries per thread (blockDim 512 covers kLbMax)
+  uint32_t len[2], sum = 0;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t i = threadIdx.x * 2 + h;
+    len[h] = 0;
+    if (i < n_f) {
+      const uint32_t u = qin[i];
+      uint64_t b, e;
+      vxb::base_range(a, u, b, e);
+      const uint2 dr = a.drow[u];
+      st.base[i] = b;
+      st.blen[i] = (uint32_t)(e - b);
+      st.dx[i] = dr.x;
+      len[h] = (uint32_t)(e - b) + dr.y;
+    }
+    sum += len[h];
+  }
+  uint32_t incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += y;
+  }
+  __shared__ uint32_t wsum[kThreads / 32];
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t w = lane < kThreads / 32 ? wsum[lane] : 0u;
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (lane < kThreads / 32) wsum[lane] = wi - w;
+  }
+  __syncthreads();
+  uint32_t ex = wsum[warp] + incl - sum;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t i = threadIdx.x * 2 + h;
+    if (i < n_f) st.pref[i] = ex;
+    ex += len[h];
+  }
+  if (threadIdx.x * 2 + 1 == n_f - 1 || (threadIdx.x * 2 == n_f - 1)) st.pref[n_f] = ex;
+  __syncthreads();
+  const uint32_t M = st.pref[n_f];
+  for (uint32_t e0 = gwarp() * 32; e0 < M; e0 += nwarps() * 32) {
+    const uint32_t e = e0 + lane;
+    bool valid = false;
+    uint32_t x = 0;
+    if (e < M) {
+      uint32_t lo = 0, hi = n_f;  // last i with pref[i] <= e
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (st.pref[mid] <= e) lo = mid;
+        else hi = mid;
+      }
+      const uint32_t j = e - st.pref[lo];
+      if (j < st.blen[lo]) {
+        x = a.col[st.base[lo] + j];
+        valid = !(x & kTomb);
+        x &= kIdMask;
+      } else {
+        x = a.darena[st.dx[lo] + (j - st.blen[lo])];
+        valid = true;
+      }
+    }
+    t(valid, x, 0u);
+  }
+  __syncthreads();  // st is reused by the next level
+}
+
 // Rows of at least large_row arcs: every warp of the grid takes a slice.
 template <class F>
 __device__ void grid_rows(const DevAdj& a, const uint32_t* rows, uint32_t n, F& f) {
@@ -399,6 +490,7 @@ __device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, u
 
 __device__ void full_bfs(const Params& p) {
   __shared__ BlockQueue bq;
+  __shared__ LbStage lbst;
   BfsCounters* c = p.c;
   if (threadIdx.x == 0) bq.cnt = 0;
   const uint32_t V = p.V;
@@ -474,7 +566,8 @@ __device__ void full_bfs(const Params& p) {
       if (!sync_grid(p)) return;
     } else {
       TdVisit t{&p, level, p.q[nxt], p.fb[nxt], &c->lvl_n[nxt], !left_bu, 0ull, &bq};
-      td_level(p, t, p.q[cur], n_f, &c->lvl_big[cur]);
+      if (n_f <= kLbMax) td_level_lb(p, t, p.q[cur], n_f, lbst);
+      else td_level(p, t, p.q[cur], n_f, &c->lvl_big[cur]);
       t.flush(&c->lvl_m[nxt]);
       bq_flush(bq, &c->lvl_n[nxt], p.q[nxt]);
       if (!sync_grid(p)) return;
@@ -986,6 +1079,7 @@ static Params make_params(Bfs* b, uint32_t V, uint32_t dist_len) {
   p.beta = b->tune.beta;
   p.large_row = b->tune.large_row;
   p.trace = b->trace;
+  p.bar = b->barrier;
   return p;
 }
 
@@ -1014,12 +1108,14 @@ int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac) {
   b->frac = frac;
   if (cudaMalloc(&b->ctr, sizeof(BfsCounters)) != cudaSuccess ||
       cudaMalloc(&b->trace, 2 * (kTraceLevels + 1) * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&b->barrier, vxb::kBarrierWords * sizeof(uint32_t)) != cudaSuccess ||
       cudaMallocHost(&b->hctr, sizeof(BfsCounters)) != cudaSuccess) {
     set_error("BFS counter allocation failed");
     bfs_destroy(b);
     return -4;
   }
   cudaMemsetAsync(b->ctr, 0, sizeof(BfsCounters), g->stream);
+  cudaMemsetAsync(b->barrier, 0, vxb::kBarrierWords * sizeof(uint32_t), g->stream);
   memset(b->hctr, 0, sizeof(BfsCounters));
   if (int rc = bfs_recompute(b)) {
     bfs_destroy(b);
@@ -1037,6 +1133,7 @@ void bfs_destroy(Bfs* b) {
   for (uint32_t* p : ptrs) cudaFree(p);
   cudaFree(b->ctr);
   cudaFree(b->trace);
+  cudaFree(b->barrier);
   cudaFreeHost(b->hctr);
   delete b;
 }

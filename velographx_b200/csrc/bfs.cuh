@@ -29,7 +29,6 @@ struct BfsCounters {
   uint32_t list_n[3];    // rotating frontier lists of the repair loops
   uint32_t next_seed[3]; // smallest pending seed level (rotating)
   uint32_t seed_min;     // smallest seed level of the settle phase
-  uint32_t bar[2];       // grid barrier {arrive, generation}
   unsigned long long scratch64;  // single-value readbacks
 };
 
@@ -60,6 +59,7 @@ struct Bfs {
   BfsCounters* ctr = nullptr;
   BfsCounters* hctr = nullptr;
   unsigned long long* trace = nullptr;  // per-level timestamps of the last full BFS
+  uint32_t* barrier = nullptr;          // grid barrier words (vxb::kBarrierWords)
   BfsTuning tune;
   int grid = 0;
 };

@@ -12,8 +12,8 @@
 // totals through distributed shared memory, and scatters every key straight
 // into the shared memory of the CTA that owns its destination.  The epilogue
 // keeps the last key of every run, compacts them across the cluster and
-// classifies each canonical arc against the pre-batch graph (base position,
-// tombstone, delta membership) -- the work of seven separate launches.
+// hands the canonical arcs to the (wide) classification kernel -- the work of
+// six separate launches.
 #include <cooperative_groups.h>
 
 #include "graph.cuh"
@@ -93,8 +93,8 @@ __device__ void scan256(uint32_t* v) {
 
 __global__ void __launch_bounds__(kThreads, 1)
     canon_cluster_kernel(const uint32_t* src, const uint32_t* dst, const uint8_t* add, uint32_t n, int directed,
-                         int b, int sh, uint32_t bound, int passes, vxb::DevAdj a, uint32_t* fu, uint32_t* fv,
-                         uint8_t* ff, uint64_t* fpos, GraphCounters* ctr) {
+                         int b, int sh, uint32_t bound, int passes, uint32_t* fu, uint32_t* fv, uint8_t* ff,
+                         GraphCounters* ctr) {
   cg::cluster_group cluster = cg::this_cluster();
   const uint32_t C = cluster.num_blocks();
   const uint32_t r = cluster.block_rank();
@@ -226,24 +226,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (!keep[j]) continue;
     const uint64_t key = A[j0 + j];
     const uint32_t u = (uint32_t)(key >> (b + sh)), v = (uint32_t)((key >> sh) & vmask);
-    // classify against the pre-batch graph
-    uint8_t f = (uint8_t)(key & 1ull);
-    uint64_t bb, ee;
-    vxb::base_range(a, u, bb, ee);
-    const uint64_t pp = vxb::lower_bound_masked(a.col, bb, ee, v);
-    bool cur;
-    if (pp < ee && (a.col[pp] & vxb::kIdMask) == v) {
-      f |= kFInBase;
-      cur = !(a.col[pp] & vxb::kTomb);
-      fpos[out] = pp;
-    } else {
-      const uint2 dr = a.drow[u];
-      const uint32_t q = vxb::lower_bound_u32(a.darena, dr.x, dr.x + dr.y, v);
-      cur = q < dr.x + dr.y && a.darena[q] == v;
-      fpos[out] = ~0ull;
-    }
-    if (cur) f |= kFCur;
-    if (cur != ((f & kFAdd) != 0)) f |= kFChanged;
+    const uint8_t f = (uint8_t)(key & 1ull);
     fu[out] = u;
     fv[out] = v;
     ff[out] = f;
@@ -286,19 +269,9 @@ int canon_cluster(Graph* g, size_t n, int b, uint32_t bound, bool* done) {
   cfg.numAttrs = 1;
   const int passes = (2 * b + 7) / 8;
   BatchBuffers& B = g->batch;
-  Adjacency& ad = g->adj[0];
-  vxb::DevAdj da;
-  da.off = ad.off;
-  da.col = ad.col;
-  da.Vb = ad.Vb;
-  da.drow = ad.drow;
-  da.dcap = ad.dcap;
-  da.darena = ad.darena;
-  da.tcnt = ad.tcnt;
-  da.dirty = ad.dirty;
   count_launch();
   VX_CUDA_TRY(cudaLaunchKernelEx(&cfg, canon_cluster_kernel, B.src, B.dst, B.add, (uint32_t)n, (int)g->directed, b,
-                                 sh, bound, passes, da, B.fu, B.fv, B.ff, B.fpos, g->ctr));
+                                 sh, bound, passes, B.fu, B.fv, B.ff, g->ctr));
   return 0;
 }
 

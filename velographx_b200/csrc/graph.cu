@@ -827,7 +827,13 @@ int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound) {
   if (n == 0) return 0;
   bool done = false;
   if (int rc = canon_cluster(g, n, b, (uint32_t)g->V, &done)) return rc;
-  if (done) return 0;
+  if (done) {
+    vxh::count_launch();
+    classify_kernel<<<grid_for(m), kBlock, 0, s>>>(devadj(g->adj[0]), B.fu, B.fv, B.ff, B.fpos,
+                                                    &g->ctr->final_arcs);
+    VX_CUDA_TRY(cudaGetLastError());
+    return 0;
+  }
   vxh::count_launch();
   expand_ops_kernel<<<grid_for(n), kBlock, 0, s>>>(B.src, B.dst, B.add, n, g->directed, b, (uint32_t)g->V,
                                                     B.keys, B.vals, g->ctr);

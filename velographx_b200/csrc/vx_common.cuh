@@ -118,23 +118,40 @@ __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t 
   return lo;
 }
 
-// Grid-wide barrier for cooperative (co-resident) launches.  The wait is
-// bounded: after ~2^22 polls with back-off the block records
-// kErrBarrierTimeout in *err and proceeds, so a broken launch ends instead of
-// hanging the device.  `bar` = {arrive count, generation}, zeroed at setup.
+// Grid-wide barrier for cooperative (co-resident) launches, two levels deep:
+// blocks arrive on one of kBarrierGroups counters (each on its own 128-byte
+// line), the last arrival of a group arrives on the top counter, and the last
+// group releases everyone by bumping the generation word.  bar layout (u32):
+// [0] generation, [32 * (1 + g)] group g, [32 * (1 + kBarrierGroups)] top;
+// kBarrierWords words, zeroed at setup.  The wait is bounded: after
+// kBarrierSpinLimit polls a block records kErrBarrierTimeout in *err and
+// proceeds, so a broken launch ends instead of hanging the device.
+constexpr uint32_t kBarrierGroups = 16;
+constexpr uint32_t kBarrierWords = 32 * (kBarrierGroups + 2);
 constexpr uint32_t kBarrierSpinLimit = 1u << 22;
 
 __device__ __forceinline__ void grid_barrier(uint32_t* bar, uint32_t nblocks, uint32_t* err) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile uint32_t* vgen = bar + 1;
+    volatile uint32_t* vgen = bar;
     const uint32_t gen = *vgen;
     __threadfence();
-    const uint32_t arrived = atomicAdd(bar, 1u);
-    if (arrived == nblocks - 1) {
-      atomicExch(bar, 0u);
+    const uint32_t g = blockIdx.x % kBarrierGroups;
+    const uint32_t gsize = nblocks / kBarrierGroups + (g < nblocks % kBarrierGroups ? 1u : 0u);
+    const uint32_t ngroups = nblocks < kBarrierGroups ? nblocks : kBarrierGroups;
+    uint32_t* gc = bar + 32 * (1 + g);
+    uint32_t* top = bar + 32 * (1 + kBarrierGroups);
+    bool release = false;
+    if (atomicAdd(gc, 1u) == gsize - 1) {
+      atomicExch(gc, 0u);
+      if (atomicAdd(top, 1u) == ngroups - 1) {
+        atomicExch(top, 0u);
+        release = true;
+      }
+    }
+    if (release) {
       __threadfence();
-      atomicAdd(bar + 1, 1u);
+      atomicAdd(bar, 1u);
     } else {
       uint32_t spins = 0;
       while (*vgen == gen) {
@@ -142,7 +159,7 @@ __device__ __forceinline__ void grid_barrier(uint32_t* bar, uint32_t nblocks, ui
           atomicOr(err, kErrBarrierTimeout);
           break;
         }
-        __nanosleep(spins < 64 ? 20 : 200);
+        if (spins > 64) __nanosleep(spins < 1024 ? 32 : 256);
       }
     }
     __threadfence();
