@@ -50,6 +50,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=20.0, help="bound of the CPU-baseline sample")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--seed", type=int, default=22)
+    p.add_argument("--alpha", type=float, default=None, help="fix the direction switch (skips the autotune sweep)")
+    p.add_argument("--beta", type=float, default=None)
     return p.parse_args()
 
 
@@ -197,8 +199,12 @@ def run_b200(args, rank, world, local):
 
     tune_roots = roots[: min(4, len(roots))].tolist()
     best, tuning = None, []
-    for alpha in (4.0, 14.0, 40.0, 120.0):
-        for beta in (8.0, 24.0, 96.0):
+    alphas = (4.0, 14.0, 40.0, 120.0) if args.alpha is None else (args.alpha,)
+    betas = (8.0, 24.0, 96.0) if args.beta is None else (args.beta,)
+    if args.alpha is not None and args.beta is not None:
+        alphas, betas, best = (), (), (args.alpha, args.beta, 0.0)
+    for alpha in alphas:
+        for beta in betas:
             ts = []
             for r in tune_roots:
                 b = vx.IncrementalBFS(g, int(r))

@@ -418,10 +418,12 @@ __device__ void grid_rows(const DevAdj& a, const uint32_t* rows, uint32_t n, F& 
 
 // ----------------------------------------------------------- bottom-up --
 
-// One warp per 32 unvisited-candidate vertices (a visited-bitmap word).  Rows
-// of at most 32 in-arcs are scanned by their own lane, longer rows by the
-// whole warp 32 arcs at a time; every scan stops at the first parent found in
-// the frontier bitmap.
+constexpr uint32_t kBuHead = 8;  // arcs a lane scans itself before the warp helps
+
+// One warp per 32 unvisited-candidate vertices (a visited-bitmap word).  Each
+// lane scans the first kBuHead in-arcs of its row; the remainder of longer
+// rows is scanned by the whole warp 32 arcs at a time; every scan stops at the
+// first parent found in the frontier bitmap.
 __device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, uint32_t* fbn, uint32_t* qout,
                          uint32_t* cnt_n, BlockQueue& bq) {
   const DevAdj& a = p.g.in;
@@ -440,20 +442,22 @@ __device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, u
     }
     const uint32_t nb = (uint32_t)(e - b), total = nb + dr.y;
     bool found = false;
-    if (todo && total <= 32) {
-      // four independent loads in flight per step
-      for (uint32_t k = 0; k < total && !found; k += 4) {
-        uint32_t x[4];
+    // every lane first scans the head of its own row (rows are sorted, and in
+    // skewed graphs the hubs that fill the frontier sit at small ids), four
+    // independent loads in flight per step
+    const uint32_t head = todo ? min(total, kBuHead) : 0u;
+    for (uint32_t k = 0; k < head && !found; k += 4) {
+      uint32_t x[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const uint32_t kk = k + j;
-          x[j] = kk >= total ? kTomb : (kk < nb ? a.col[b + kk] : a.darena[dr.x + (kk - nb)]);
-        }
-#pragma unroll
-        for (int j = 0; j < 4; ++j) found = found || (!(x[j] & kTomb) && test_bit(fbc, x[j]));
+      for (int j = 0; j < 4; ++j) {
+        const uint32_t kk = k + j;
+        x[j] = kk >= head ? kTomb : (kk < nb ? a.col[b + kk] : a.darena[dr.x + (kk - nb)]);
       }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) found = found || (!(x[j] & kTomb) && test_bit(fbc, x[j]));
     }
-    uint32_t longm = __ballot_sync(FULL, todo && total > 32);
+    // the rest of the longer rows: whole warp, 32 arcs per step, early exit
+    uint32_t longm = __ballot_sync(FULL, todo && !found && total > head);
     while (longm) {
       const int l = __ffs(longm) - 1;
       longm &= longm - 1;
@@ -461,7 +465,7 @@ __device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, u
       const uint32_t nbl = __shfl_sync(FULL, nb, l), tot = __shfl_sync(FULL, total, l);
       const uint32_t dx = __shfl_sync(FULL, dr.x, l);
       bool hit_l = false;
-      for (uint32_t k0 = 0; k0 < tot; k0 += 32) {
+      for (uint32_t k0 = kBuHead; k0 < tot; k0 += 32) {
         const uint32_t k = k0 + lane;
         bool hit = false;
         if (k < tot) {

@@ -313,6 +313,84 @@ __global__ void compact_index_kernel(const uint32_t* flag, const uint32_t* pos, 
     if (flag[i]) out[pos[i]] = (uint32_t)i;
 }
 
+// One CTA builds a delta work list and its row runs (batches of at most
+// kListMax canonical arcs): selected arcs are compacted in order with a block
+// scan, then every entry whose row differs from its predecessor starts a run.
+// Replaces the flag / scan / compact / run-flag / scan / compact launches.
+constexpr int kListThreads = 1024;
+constexpr int kListItems = 32;
+constexpr size_t kListMax = (size_t)kListThreads * kListItems;
+
+__device__ uint32_t block_scan_1024(uint32_t v, uint32_t* wsum, uint32_t* total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t incl = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  __syncthreads();
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t w = wsum[lane];
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    wsum[lane] = wi - w;
+    if (lane == 31) *total = wi;
+  }
+  __syncthreads();
+  return wsum[warp] + incl - v;
+}
+
+__global__ void __launch_bounds__(kListThreads) build_list_kernel(const uint32_t* fu, const uint32_t* fv,
+                                                                   const uint8_t* ff, const uint32_t* count,
+                                                                   int mode, uint32_t* lu, uint32_t* lv,
+                                                                   uint32_t* runs, uint32_t* nlist,
+                                                                   uint32_t* nruns) {
+  __shared__ uint32_t wsum[32];
+  __shared__ uint32_t total;
+  const uint32_t F = *count;
+  const uint32_t base = threadIdx.x * kListItems;
+  uint32_t bits = 0, cnt = 0;
+  for (int j = 0; j < kListItems; ++j) {
+    const uint32_t i = base + j;
+    if (i >= F) break;
+    const uint8_t f = ff[i];
+    const bool sel = !(f & kFInBase) && (f & kFChanged) && (((f & kFAdd) != 0) == (mode == 1));
+    bits |= (uint32_t)sel << j;
+    cnt += sel;
+  }
+  uint32_t pos = block_scan_1024(cnt, wsum, &total);
+  const uint32_t n = total;
+  for (int j = 0; j < kListItems; ++j) {
+    if ((bits >> j) & 1u) {
+      lu[pos] = fu[base + j];
+      lv[pos] = fv[base + j];
+      ++pos;
+    }
+  }
+  if (threadIdx.x == 0) *nlist = n;
+  __syncthreads();  // the compacted list is visible to the whole block
+  bits = 0;
+  cnt = 0;
+  for (int j = 0; j < kListItems; ++j) {
+    const uint32_t k = base + j;
+    if (k >= n) break;
+    const bool st = k == 0 || lu[k] != lu[k - 1];
+    bits |= (uint32_t)st << j;
+    cnt += st;
+  }
+  pos = block_scan_1024(cnt, wsum, &total);
+  for (int j = 0; j < kListItems; ++j)
+    if ((bits >> j) & 1u) runs[pos++] = base + j;
+  if (threadIdx.x == 0) *nruns = total;
+}
+
 // One warp per row run: drop the run's arcs from the row's sorted delta list
 // (forward in-place compaction: every kept entry moves to a lower index).
 __global__ void delta_remove_kernel(DevAdj a, const uint32_t* lu, const uint32_t* lv, const uint32_t* runs,
@@ -868,16 +946,21 @@ static int commit_list(Graph* g, Adjacency& a, int dir, uint32_t* fu, uint32_t* 
   tomb_kernel<<<grid_for(m), kBlock, 0, s>>>(da, fu, ff, fpos, count, mode, &c->tombs[dir], &c->dirty_rows[dir]);
   uint32_t* nlist = mode == 0 ? &c->rm_arcs : &c->ins_arcs;
   uint32_t* nruns = mode == 0 ? &c->rm_runs : &c->ins_runs;
-  vxh::count_launch();
-  delta_flag_kernel<<<grid_for(m), kBlock, 0, s>>>(ff, count, m, mode, B.flag);
-  if (int rc = scan_count(g, B.flag, B.pos, m, nlist)) return rc;
-  vxh::count_launch();
-  compact_pairs_kernel<<<grid_for(m), kBlock, 0, s>>>(fu, fv, B.flag, B.pos, m, B.lu, B.lv);
-  vxh::count_launch();
-  run_flag_kernel<<<grid_for(m), kBlock, 0, s>>>(B.lu, nlist, m, B.flag);
-  if (int rc = scan_count(g, B.flag, B.pos, m, nruns)) return rc;
-  vxh::count_launch();
-  compact_index_kernel<<<grid_for(m), kBlock, 0, s>>>(B.flag, B.pos, m, B.runs);
+  if (m <= kListMax) {
+    vxh::count_launch();
+    build_list_kernel<<<1, kListThreads, 0, s>>>(fu, fv, ff, count, mode, B.lu, B.lv, B.runs, nlist, nruns);
+  } else {
+    vxh::count_launch();
+    delta_flag_kernel<<<grid_for(m), kBlock, 0, s>>>(ff, count, m, mode, B.flag);
+    if (int rc = scan_count(g, B.flag, B.pos, m, nlist)) return rc;
+    vxh::count_launch();
+    compact_pairs_kernel<<<grid_for(m), kBlock, 0, s>>>(fu, fv, B.flag, B.pos, m, B.lu, B.lv);
+    vxh::count_launch();
+    run_flag_kernel<<<grid_for(m), kBlock, 0, s>>>(B.lu, nlist, m, B.flag);
+    if (int rc = scan_count(g, B.flag, B.pos, m, nruns)) return rc;
+    vxh::count_launch();
+    compact_index_kernel<<<grid_for(m), kBlock, 0, s>>>(B.flag, B.pos, m, B.runs);
+  }
   const unsigned wg = grid_for(m * 32, kBlock);
   vxh::count_launch();
   if (mode == 0)
