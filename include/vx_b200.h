@@ -126,6 +126,28 @@ int vx_bfs_level_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
  * No reference counterpart: the reference BFS is top-down only. */
 int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row);
 
+/* ---- Multi-root BFS (up to 256 roots, one launch) ----------------------
+ * For every root r, row r of the result equals BasicIncrementalBFS(g,
+ * roots[r]).distances() (bfs.hpp:100-120); the reference's multicore harness
+ * benchmarks/thread_scaling_bfs.cpp:78-108 computes the same with one thread
+ * per root.  Distances are laid out root-major: dist[r * V + v]. */
+typedef struct vx_mrbfs vx_mrbfs;
+int vx_mrbfs_create(vx_graph* g, const uint32_t* roots, size_t k, vx_mrbfs** out);
+int vx_mrbfs_destroy(vx_mrbfs* m);
+/* Enqueues the traversal on the graph's stream (asynchronous). */
+int vx_mrbfs_run(vx_mrbfs* m);
+/* Waits, then copies min(cap, k*V) distances; *n = k*V. */
+int vx_mrbfs_distances(vx_mrbfs* m, uint32_t* host_out, size_t cap, size_t* n);
+int vx_mrbfs_distances_device(vx_mrbfs* m, const uint32_t** d_dist, size_t* n);
+/* Sum over roots of the out-degrees of reached vertices (for TEPS), and the
+ * level count of the last run. */
+int vx_mrbfs_reached_arcs(vx_mrbfs* m, uint64_t* out);
+int vx_mrbfs_levels(vx_mrbfs* m, uint32_t* out);
+/* Pull (bottom-up) when the frontier holds more than frac * V vertices. */
+int vx_mrbfs_set_pull_fraction(vx_mrbfs* m, float frac);
+/* One-shot form: create, run, copy k*V distances into out (cap entries). */
+int vx_multiroot_bfs(vx_graph* g, const uint32_t* roots, size_t k, uint32_t* out, size_t cap);
+
 #ifdef __cplusplus
 }
 #endif

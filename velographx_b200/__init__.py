@@ -19,6 +19,7 @@ try:
     from ._velographx import (  # noqa: F401
         Graph,
         IncrementalBFS,
+        MultiRootBFS,
         UpdateBatch,
         from_arrow_columns,
         from_arrow_table,
@@ -47,6 +48,7 @@ def capi() -> _ctypes.CDLL:
 __all__ = [
     "Graph",
     "IncrementalBFS",
+    "MultiRootBFS",
     "UpdateBatch",
     "from_numpy_edges",
     "from_scipy_csr",

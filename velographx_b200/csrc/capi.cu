@@ -9,6 +9,7 @@
 #include "../../include/vx_b200.h"
 #include "bfs.cuh"
 #include "graph.cuh"
+#include "mrbfs.cuh"
 
 namespace vxh {
 
@@ -32,6 +33,9 @@ struct vx_graph {
 struct vx_bfs {
   vxh::Bfs* b;
   vx_graph* owner;
+};
+struct vx_mrbfs {
+  vxh::MrBfs* m;
 };
 
 namespace {
@@ -313,6 +317,74 @@ int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row) {
   b->b->tune.beta = beta;
   b->b->tune.large_row = large_row;
   return VX_OK;
+}
+
+int vx_mrbfs_create(vx_graph* g, const uint32_t* roots, size_t k, vx_mrbfs** out) {
+  if (!g || !roots || !out) return fail(VX_ERR_INVALID, "null argument");
+  vxh::MrBfs* m = nullptr;
+  if (int rc = vxh::mrbfs_create(&m, g->g, roots, k)) return rc;
+  *out = new vx_mrbfs{m};
+  return VX_OK;
+}
+
+int vx_mrbfs_destroy(vx_mrbfs* m) {
+  if (!m) return VX_OK;
+  vxh::mrbfs_destroy(m->m);
+  delete m;
+  return VX_OK;
+}
+
+int vx_mrbfs_run(vx_mrbfs* m) {
+  if (!m) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::mrbfs_run(m->m);
+}
+
+int vx_mrbfs_distances(vx_mrbfs* m, uint32_t* host_out, size_t cap, size_t* n) {
+  if (!m || !n) return fail(VX_ERR_INVALID, "null argument");
+  vxh::MrBfs* x = m->m;
+  *n = x->K * x->V;
+  if (int rc = vxh::mrbfs_sync(x)) return rc;
+  const size_t c = std::min(cap, *n);
+  if (host_out && c) VX_CUDA_TRY(cudaMemcpy(host_out, x->dist, c * 4, cudaMemcpyDeviceToHost));
+  return VX_OK;
+}
+
+int vx_mrbfs_distances_device(vx_mrbfs* m, const uint32_t** d_dist, size_t* n) {
+  if (!m || !d_dist || !n) return fail(VX_ERR_INVALID, "null argument");
+  *d_dist = m->m->dist;
+  *n = m->m->K * m->m->V;
+  return VX_OK;
+}
+
+int vx_mrbfs_reached_arcs(vx_mrbfs* m, uint64_t* out) {
+  if (!m || !out) return fail(VX_ERR_INVALID, "null argument");
+  unsigned long long a = 0;
+  if (int rc = vxh::mrbfs_reached_arcs(m->m, &a)) return rc;
+  *out = a;
+  return VX_OK;
+}
+
+int vx_mrbfs_levels(vx_mrbfs* m, uint32_t* out) {
+  if (!m || !out) return fail(VX_ERR_INVALID, "null argument");
+  if (int rc = vxh::mrbfs_sync(m->m)) return rc;
+  *out = m->m->hctr->levels;
+  return VX_OK;
+}
+
+int vx_mrbfs_set_pull_fraction(vx_mrbfs* m, float frac) {
+  if (!m || !(frac > 0.f)) return fail(VX_ERR_INVALID, "invalid pull fraction");
+  m->m->pull_frac = frac;
+  return VX_OK;
+}
+
+int vx_multiroot_bfs(vx_graph* g, const uint32_t* roots, size_t k, uint32_t* out, size_t cap) {
+  vx_mrbfs* m = nullptr;
+  if (int rc = vx_mrbfs_create(g, roots, k, &m)) return rc;
+  size_t n = 0;
+  int rc = vx_mrbfs_run(m);
+  if (!rc) rc = vx_mrbfs_distances(m, out, cap, &n);
+  vx_mrbfs_destroy(m);
+  return rc;
 }
 
 }  // extern "C"

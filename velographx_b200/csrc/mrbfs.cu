@@ -1,0 +1,345 @@
+// Multi-root BFS: up to 256 independent BFS traversals in one persistent
+// cooperative launch, bit-parallel over the roots.
+//
+// Every vertex carries W = ceil(K/32) words of "reached by root r" bits and
+// rotating frontier words; a level expands all roots at once, so each row is
+// read once per level instead of once per root.  Sparse levels push the
+// frontier words of the queued vertices along their rows (atomicOr into the
+// next-level words of the heads, heads queued once through a touched bitmap);
+// dense levels pull: every vertex not yet reached by all roots ORs the
+// frontier words of its in-neighbours and stops as soon as every root has
+// reached it.  Distances are written as dist[r * V + v]; for every root they
+// equal BasicIncrementalBFS::recompute (include/velographx/incremental/bfs.hpp:100-120)
+// from that root, and the reference's multicore harness
+// (benchmarks/thread_scaling_bfs.cpp:78-108) runs the same roots one thread each.
+#include <algorithm>
+#include <cstring>
+
+#include "frontier.cuh"
+#include "graph.cuh"
+#include "mrbfs.cuh"
+
+namespace vxh {
+
+namespace {
+
+using namespace frontier;
+
+constexpr int kThreads = 512;
+
+struct MrParams {
+  vxb::DevGraph g;
+  uint32_t V, K, W;
+  const uint32_t* roots;
+  uint32_t* vis;     // [V][W]
+  uint32_t* frn[3];  // [V][W] rotating frontier words
+  uint32_t* nxt;     // [V][W] pushed words of the level being built
+  uint32_t* touched; // bitmap
+  uint32_t* q[3];    // rotating frontier queues
+  uint32_t* tl;      // touched list of a push level
+  uint32_t* dist;    // [K][V]
+  MrCounters* c;
+  uint32_t* bar;
+  uint32_t nblocks;
+  float pull_frac;   // pull when the frontier holds more than V * pull_frac vertices
+};
+
+__device__ __forceinline__ bool mr_sync(const MrParams& p) {
+  vxb::grid_barrier(p.bar, p.nblocks, &p.c->err);
+  return __ldcg(&p.c->err) == 0u;
+}
+
+__device__ __forceinline__ uint32_t word_mask(const MrParams& p, uint32_t w) {
+  const uint32_t rem = p.K - 32 * w;
+  return rem >= 32 ? 0xFFFFFFFFu : ((1u << rem) - 1u);
+}
+
+// Record newly reached roots of v at distance lvl; returns whether any.
+__device__ __forceinline__ void write_dists(const MrParams& p, uint32_t v, uint32_t w, uint32_t bits, uint32_t lvl) {
+  while (bits) {
+    const uint32_t b = __ffs(bits) - 1;
+    bits &= bits - 1;
+    p.dist[(size_t)(32 * w + b) * p.V + v] = lvl;
+  }
+}
+
+// Push: the warp walks the row of frontier vertex u with u's frontier words
+// in registers.  W (words per vertex) is a compile-time constant so the
+// per-vertex word arrays stay in registers.
+template <uint32_t W>
+struct PushVisit {
+  const MrParams* p;
+  uint32_t fw[W];
+  uint32_t* tcount;
+  __device__ __forceinline__ void operator()(bool valid, uint32_t x, uint32_t) {
+    bool fresh = false;
+    if (valid) {
+      bool any = false;
+#pragma unroll
+      for (uint32_t w = 0; w < W; ++w) {
+        const uint32_t m = fw[w] & ~p->vis[(size_t)x * W + w];
+        if (m) {
+          atomicOr(&p->nxt[(size_t)x * W + w], m);
+          any = true;
+        }
+      }
+      if (any) {
+        const uint32_t bit = 1u << (x & 31);
+        fresh = !(atomicOr(&p->touched[x >> 5], bit) & bit);
+      }
+    }
+    const uint32_t s = vxb::warp_append(fresh, tcount);
+    if (fresh) p->tl[s] = x;
+  }
+};
+
+template <uint32_t W>
+__global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
+  MrCounters* c = p.c;
+  // roots (queued once per distinct vertex)
+  for (uint32_t r = gtid(); r < p.K; r += nthreads()) {
+    const uint32_t v = p.roots[r];
+    if (v >= p.V) continue;
+    atomicOr(&p.vis[(size_t)v * W + r / 32], 1u << (r & 31));
+    atomicOr(&p.frn[0][(size_t)v * W + r / 32], 1u << (r & 31));
+    p.dist[(size_t)r * p.V + v] = 0;
+    const uint32_t bit = 1u << (v & 31);
+    if (!(atomicOr(&p.touched[v >> 5], bit) & bit)) p.q[0][atomicAdd(&c->qn[0], 1u)] = v;
+  }
+  if (!mr_sync(p)) return;
+  for (uint32_t i = gtid(); i < __ldcg(&c->qn[0]); i += nthreads()) p.touched[p.q[0][i] >> 5] = 0u;
+  if (!mr_sync(p)) return;
+  uint32_t prev_n = 0;
+  uint32_t level = 0;
+  for (;; ++level) {
+    if (level > p.V + 1) {
+      if (gtid() == 0) atomicOr(&c->err, vxb::kErrLoopBound);
+      break;
+    }
+    const int cur = level % 3, nx = (level + 1) % 3, clr = (level + 2) % 3;
+    const uint32_t n_f = __ldcg(&c->qn[cur]);
+    if (n_f == 0) break;
+    if (gtid() == 0) {
+      c->qn[clr] = 0;
+      c->tn = 0;
+    }
+    // frontier words of level-1 are no longer read: clear them for reuse
+    for (uint32_t i = gtid(); i < prev_n * W; i += nthreads()) p.frn[clr][(size_t)p.q[clr][i / W] * W + i % W] = 0u;
+    const uint32_t* fc = p.frn[cur];
+    uint32_t* fn = p.frn[nx];
+    if ((float)n_f > p.pull_frac * (float)p.V) {
+      // pull: every vertex not reached by all roots ORs its in-neighbours'
+      // frontier words, stopping once all roots reached it
+      const DevAdj& a = p.g.in;
+      for (uint32_t v = gtid(); v < p.V; v += nthreads()) {
+        uint32_t vis[W], acc[W];
+        bool full = true;
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w) {
+          vis[w] = p.vis[(size_t)v * W + w];
+          acc[w] = 0;
+          full = full && vis[w] == word_mask(p, w);
+        }
+        if (full) continue;
+        uint64_t b, e;
+        vxb::base_range(a, v, b, e);
+        const uint2 dr = a.drow[v];
+        const uint64_t nb = e - b;
+        for (uint64_t j = 0; j < nb + dr.y && !full; ++j) {
+          uint32_t x;
+          if (j < nb) {
+            x = a.col[b + j];
+            if (x & kTomb) continue;
+          } else {
+            x = a.darena[dr.x + (uint32_t)(j - nb)];
+          }
+          full = true;
+#pragma unroll
+          for (uint32_t w = 0; w < W; ++w) {
+            acc[w] |= fc[(size_t)x * W + w] & ~vis[w];
+            full = full && (vis[w] | acc[w]) == word_mask(p, w);
+          }
+        }
+        bool any = false;
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w) {
+          if (!acc[w]) continue;
+          any = true;
+          p.vis[(size_t)v * W + w] = vis[w] | acc[w];
+          fn[(size_t)v * W + w] = acc[w];
+          write_dists(p, v, w, acc[w], level + 1);
+        }
+        if (any) p.q[nx][atomicAdd(&c->qn[nx], 1u)] = v;
+      }
+      if (!mr_sync(p)) return;
+    } else {
+      // push along the rows of the queued frontier vertices, one warp each
+      const DevAdj& a = p.g.out;
+      PushVisit<W> pv{&p, {}, &c->tn};
+      for (uint32_t i = gwarp(); i < n_f; i += nwarps()) {
+        const uint32_t u = p.q[cur][i];
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w) pv.fw[w] = fc[(size_t)u * W + w];
+        warp_row(a, u, pv);
+      }
+      if (!mr_sync(p)) return;
+      const uint32_t nt = __ldcg(&c->tn);
+      for (uint32_t i = gtid(); i < nt; i += nthreads()) {
+        const uint32_t x = p.tl[i];
+        bool any = false;
+        for (uint32_t w = 0; w < W; ++w) {
+          const size_t o = (size_t)x * W + w;
+          const uint32_t m = p.nxt[o] & ~p.vis[o];
+          p.nxt[o] = 0u;
+          if (!m) continue;
+          any = true;
+          p.vis[o] |= m;
+          fn[o] = m;
+          write_dists(p, x, w, m, level + 1);
+        }
+        p.touched[x >> 5] = 0u;
+        if (any) p.q[nx][atomicAdd(&c->qn[nx], 1u)] = x;
+      }
+      if (!mr_sync(p)) return;
+    }
+    prev_n = n_f;
+  }
+  if (gtid() == 0) c->levels = level;
+}
+
+__global__ void mr_arcs_kernel(vxb::DevAdj a, const uint32_t* dist, uint32_t V, uint32_t K,
+                               unsigned long long* out) {
+  unsigned long long s = 0;
+  const size_t total = (size_t)V * K;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+    if (dist[i] == kUnreachable) continue;
+    const uint32_t v = (uint32_t)(i % V);
+    uint64_t b, e;
+    vxb::base_range(a, v, b, e);
+    s += (e - b) - a.tcnt[v] + a.drow[v].y;
+  }
+  s = vxb::warp_sum(s);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, s);
+}
+
+}  // namespace
+
+int mrbfs_create(MrBfs** out, Graph* g, const uint32_t* host_roots, size_t k) {
+  if (k == 0 || k > kMaxRoots) {
+    set_error("multi-root BFS takes 1..%u roots", kMaxRoots);
+    return -1;
+  }
+  MrBfs* m = new MrBfs();
+  m->g = g;
+  m->K = k;
+  const size_t words = (k + 31) / 32;
+  m->W = words <= 1 ? 1 : words <= 2 ? 2 : words <= 4 ? 4 : 8;  // kernel instantiations
+  const size_t V = std::max<size_t>(g->V, 1);
+  m->V = V;
+  const size_t vw = V * m->W;
+  bool ok = cudaMalloc(&m->roots, k * 4) == cudaSuccess && cudaMalloc(&m->vis, vw * 4) == cudaSuccess &&
+            cudaMalloc(&m->nxt, vw * 4) == cudaSuccess && cudaMalloc(&m->touched, ((V + 31) / 32) * 4) == cudaSuccess &&
+            cudaMalloc(&m->tl, V * 4) == cudaSuccess && cudaMalloc(&m->dist, V * k * 4) == cudaSuccess &&
+            cudaMalloc(&m->ctr, sizeof(MrCounters)) == cudaSuccess &&
+            cudaMalloc(&m->barrier, vxb::kBarrierWords * 4) == cudaSuccess &&
+            cudaMallocHost(&m->hctr, sizeof(MrCounters)) == cudaSuccess;
+  for (int i = 0; i < 3 && ok; ++i)
+    ok = cudaMalloc(&m->frn[i], vw * 4) == cudaSuccess && cudaMalloc(&m->q[i], V * 4) == cudaSuccess;
+  if (!ok) {
+    set_error("multi-root BFS allocation failed (%zu roots, %zu vertices)", k, V);
+    mrbfs_destroy(m);
+    return -4;
+  }
+  cudaMemcpyAsync(m->roots, host_roots, k * 4, cudaMemcpyHostToDevice, g->stream);
+  cudaMemsetAsync(m->barrier, 0, vxb::kBarrierWords * 4, g->stream);
+  cudaMemsetAsync(m->touched, 0, ((V + 31) / 32) * 4, g->stream);
+  *out = m;
+  return 0;
+}
+
+void mrbfs_destroy(MrBfs* m) {
+  if (!m) return;
+  if (m->g && m->g->stream) cudaStreamSynchronize(m->g->stream);
+  void* ptrs[] = {m->roots, m->vis, m->nxt, m->touched, m->tl, m->dist, m->ctr, m->barrier,
+                  m->frn[0], m->frn[1], m->frn[2], m->q[0], m->q[1], m->q[2]};
+  for (void* p : ptrs) cudaFree(p);
+  cudaFreeHost(m->hctr);
+  delete m;
+}
+
+int mrbfs_run(MrBfs* m) {
+  Graph* g = m->g;
+  cudaStream_t s = g->stream;
+  if (g->V != m->V) {
+    set_error("graph vertex count changed since the multi-root BFS was created");
+    return -1;
+  }
+  const size_t vw = m->V * m->W;
+  VX_CUDA_TRY(cudaMemsetAsync(m->vis, 0, vw * 4, s));
+  VX_CUDA_TRY(cudaMemsetAsync(m->nxt, 0, vw * 4, s));
+  for (int i = 0; i < 3; ++i) VX_CUDA_TRY(cudaMemsetAsync(m->frn[i], 0, vw * 4, s));
+  VX_CUDA_TRY(cudaMemsetAsync(m->dist, 0xFF, m->V * m->K * 4, s));
+  VX_CUDA_TRY(cudaMemsetAsync(m->ctr, 0, sizeof(MrCounters), s));
+  const void* kern = m->W <= 1 ? (const void*)mrbfs_kernel<1>
+                     : m->W <= 2 ? (const void*)mrbfs_kernel<2>
+                     : m->W <= 4 ? (const void*)mrbfs_kernel<4>
+                                 : (const void*)mrbfs_kernel<8>;
+  if (!m->grid) {
+    int per_sm = 0;
+    VX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, 0));
+    if (per_sm < 1) {
+      set_error("multi-root BFS kernel cannot be resident on an SM");
+      return -3;
+    }
+    m->grid = per_sm * sm_count();
+  }
+  MrParams p;
+  memset(&p, 0, sizeof(p));
+  p.g = g->view();
+  p.V = (uint32_t)m->V;
+  p.K = (uint32_t)m->K;
+  p.W = (uint32_t)m->W;
+  p.roots = m->roots;
+  p.vis = m->vis;
+  for (int i = 0; i < 3; ++i) {
+    p.frn[i] = m->frn[i];
+    p.q[i] = m->q[i];
+  }
+  p.nxt = m->nxt;
+  p.touched = m->touched;
+  p.tl = m->tl;
+  p.dist = m->dist;
+  p.c = m->ctr;
+  p.bar = m->barrier;
+  p.nblocks = (uint32_t)m->grid;
+  p.pull_frac = m->pull_frac;
+  void* args[] = {&p};
+  count_launch();
+  VX_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(m->grid), dim3(kThreads), args, 0, s));
+  return 0;
+}
+
+int mrbfs_sync(MrBfs* m) {
+  cudaStream_t s = m->g->stream;
+  VX_CUDA_TRY(cudaMemcpyAsync(m->hctr, m->ctr, sizeof(MrCounters), cudaMemcpyDeviceToHost, s));
+  VX_CUDA_TRY(cudaStreamSynchronize(s));
+  if (m->hctr->err) {
+    set_error("multi-root BFS device error word 0x%x", m->hctr->err);
+    return -5;
+  }
+  return 0;
+}
+
+int mrbfs_reached_arcs(MrBfs* m, unsigned long long* out) {
+  cudaStream_t s = m->g->stream;
+  unsigned long long* d = &m->ctr->arcs;
+  VX_CUDA_TRY(cudaMemsetAsync(d, 0, 8, s));
+  count_launch();
+  mr_arcs_kernel<<<sm_count() * 8, 256, 0, s>>>(m->g->view().out, m->dist, (uint32_t)m->V, (uint32_t)m->K, d);
+  VX_CUDA_TRY(cudaGetLastError());
+  if (int rc = mrbfs_sync(m)) return rc;
+  *out = m->hctr->arcs;
+  return 0;
+}
+
+}  // namespace vxh

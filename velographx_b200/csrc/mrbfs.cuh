@@ -1,0 +1,45 @@
+// Multi-root BFS state (bit-parallel traversal of up to kMaxRoots roots).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "graph.cuh"
+
+namespace vxh {
+
+constexpr uint32_t kMaxRoots = 256;
+
+struct MrCounters {
+  uint32_t qn[3];   // rotating frontier queue lengths
+  uint32_t tn;      // touched heads of a push level
+  uint32_t levels;
+  uint32_t err;
+  unsigned long long arcs;  // reached-arc total (mrbfs_reached_arcs)
+};
+
+struct MrBfs {
+  Graph* g = nullptr;
+  size_t K = 0, W = 0, V = 0;
+  uint32_t* roots = nullptr;
+  uint32_t* vis = nullptr;
+  uint32_t* frn[3] = {nullptr, nullptr, nullptr};
+  uint32_t* nxt = nullptr;
+  uint32_t* touched = nullptr;
+  uint32_t* q[3] = {nullptr, nullptr, nullptr};
+  uint32_t* tl = nullptr;
+  uint32_t* dist = nullptr;  // [K][V]
+  MrCounters* ctr = nullptr;
+  MrCounters* hctr = nullptr;
+  uint32_t* barrier = nullptr;
+  float pull_frac = 0.02f;
+  int grid = 0;
+};
+
+int mrbfs_create(MrBfs** out, Graph* g, const uint32_t* host_roots, size_t k);
+void mrbfs_destroy(MrBfs* m);
+int mrbfs_run(MrBfs* m);   // enqueues the traversal on the graph's stream
+int mrbfs_sync(MrBfs* m);  // waits and checks the device error word
+int mrbfs_reached_arcs(MrBfs* m, unsigned long long* out);
+
+}  // namespace vxh

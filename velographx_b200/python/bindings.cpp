@@ -103,6 +103,18 @@ DynamicGraph graph_from_arrow_table(const py::object& table, const std::string& 
   return graph_from_arrow_columns(table.attr("column")(src_name), table.attr("column")(dst_name), directed);
 }
 
+// Owns one multi-root BFS handle (vx_mrbfs_*).
+struct MultiRoot {
+  vx_mrbfs* h = nullptr;
+  std::size_t k = 0;
+  MultiRoot(DynamicGraph& g, const u32_array& roots) : k(static_cast<std::size_t>(roots.size())) {
+    detail::check(vx_mrbfs_create(g.handle(), roots.data(), k, &h));
+  }
+  ~MultiRoot() { vx_mrbfs_destroy(h); }
+  MultiRoot(const MultiRoot&) = delete;
+  MultiRoot& operator=(const MultiRoot&) = delete;
+};
+
 struct Arrays {
   u32_array src, dst;
   u8_array add;
@@ -257,6 +269,36 @@ PYBIND11_MODULE(_velographx, m) {
       .def("set_tuning", [](IncrementalBFS& x, float alpha, float beta, std::uint32_t large_row) {
         detail::check(vx_bfs_set_tuning(x.handle(), alpha, beta, large_row));
       }, py::arg("alpha"), py::arg("beta"), py::arg("large_row"));
+
+  py::class_<MultiRoot>(m, "MultiRootBFS")
+      .def(py::init<DynamicGraph&, const u32_array&>(), py::arg("graph"), py::arg("roots"), py::keep_alive<1, 2>())
+      .def("run", [](MultiRoot& r) { detail::check(vx_mrbfs_run(r.h)); })
+      .def("set_pull_fraction", [](MultiRoot& r, float f) { detail::check(vx_mrbfs_set_pull_fraction(r.h, f)); })
+      .def("distances_array",
+           [](MultiRoot& r) {
+             std::size_t n = 0;
+             const std::uint32_t* d = nullptr;
+             detail::check(vx_mrbfs_distances_device(r.h, &d, &n));
+             const auto V = static_cast<py::ssize_t>(n / r.k);
+             py::array_t<std::uint32_t> out({static_cast<py::ssize_t>(r.k), V});
+             auto* ptr = out.mutable_data();
+             {
+               py::gil_scoped_release release;
+               detail::check(vx_mrbfs_distances(r.h, ptr, n, &n));
+             }
+             return out;
+           })
+      .def("reached_arcs",
+           [](MultiRoot& r) {
+             std::uint64_t a = 0;
+             detail::check(vx_mrbfs_reached_arcs(r.h, &a));
+             return a;
+           })
+      .def_property_readonly("levels", [](MultiRoot& r) {
+        std::uint32_t l = 0;
+        detail::check(vx_mrbfs_levels(r.h, &l));
+        return l;
+      });
 
   m.def("from_numpy_edges", &graph_from_numpy_edges, py::arg("edges"), py::arg("directed") = false);
   m.def("from_scipy_csr", &graph_from_scipy_csr, py::arg("csr"), py::arg("directed") = false);
