@@ -66,6 +66,15 @@ def workload(args):
     return V, edges, roots, stream
 
 
+def vx_roots(roots, k, V, edges, args):
+    """k seeded non-isolated roots (the first len(roots) are the single-root ones)."""
+    from velographx_b200 import workloads as w
+
+    if k <= len(roots):
+        return roots[:k]
+    return w.non_isolated_roots(edges, V, k, seed=args.seed + 1)
+
+
 def config_dict(args, V):
     return {
         "workload": f"rmat{args.scale}-undirected-ef{args.edge_factor}-incremental-bfs-{args.batch_ops}-op-batches",
@@ -243,6 +252,23 @@ def run_b200(args, rank, world, local):
     b_full = 4.0 * arcs + 8.0 * (V + 1) + 4.0 * V
     achieved = float((b_full / (bfs_ms * 1e-3)).mean() / 1e9)
 
+    # ---- multi-root BFS: 64 and 256 roots in one bit-parallel launch ----
+    multiroot = {}
+    for k in (64, 256):
+        rr = vx_roots(roots, k, V, edges, args)
+        mr = vx.MultiRootBFS(g, rr)
+        mr.run()  # warm
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s0.record(cs)
+        mr.run()
+        s1.record(cs)
+        s1.synchronize()
+        ms = s0.elapsed_time(s1)
+        marcs = mr.reached_arcs()
+        multiroot[str(k)] = {"ms": ms, "gteps": marcs / 2 / (ms * 1e-3) / 1e9, "levels": mr.levels}
+        del mr
+
     # ---- update stream, device-resident batches (value) ----
     root = int(roots[0])
     b = vx.IncrementalBFS(g, root)
@@ -349,6 +375,7 @@ def run_b200(args, rank, world, local):
                 "ms_median": float(np.median(bfs_ms)), "levels_median": float(np.median(levels)),
                 "arcs": int(A), "level_trace_root0_us_nf_dir": trace,
                 "autotune": {"alpha": alpha, "beta": beta, "sweep_alpha_beta_ms": tuning}},
+        "multiroot_bfs": multiroot,
         "repair_last": {"affected": st["last_affected_vertices"], "candidates": st["last_deletion_candidates"],
                         "full": st["last_used_full_recompute"]},
         "clocks": clocks.summary(),

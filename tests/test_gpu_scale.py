@@ -6,6 +6,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+from oracle import OracleBFS, OracleGraph
 from oracle import load as load_oracle
 from velographx_b200 import workloads as w
 
@@ -23,10 +24,15 @@ def simple_arcs(edges, directed):
     return (k >> 32).astype(np.uint32), (k & 0xFFFFFFFF).astype(np.uint32)
 
 
-def oracle_bfs(edges, V, root, directed):
+def oracle_csr(edges, V, directed):
     u, v = simple_arcs(edges, directed)
     off = np.zeros(V + 1, np.uint64)
     np.cumsum(np.bincount(u, minlength=V), out=off[1:])
+    return off, v
+
+
+def oracle_bfs(edges, V, root, directed, csr=None):
+    off, v = csr if csr is not None else oracle_csr(edges, V, directed)
     lib = load_oracle("port")
     dist = np.empty(V, np.uint32)
     rc = lib.dll.vxo_csr_bfs(off.ctypes.data_as(C.POINTER(C.c_uint64)), v.ctypes.data_as(C.POINTER(C.c_uint32)),
@@ -111,3 +117,50 @@ def test_rmat22_config2_repair_equals_recompute():
         got = b.distances_array()
         assert np.array_equal(got, fresh.distances_array()), f"batch {i}"
         assert b.reachable_count == fresh.reachable_count == int(np.count_nonzero(got != U))
+
+
+@pytest.mark.parametrize("scale,directed,k", [(14, False, 256), (13, True, 33), (12, False, 1)])
+def test_multiroot_matches_single_root(scale, directed, k):
+    """Every row of the bit-parallel multi-root BFS equals the oracle's BFS from
+    that root; roots may repeat or lie outside the graph (all unreachable)."""
+    V = 1 << scale
+    e = w.rmat_edges(scale, seed=40 + scale)
+    g = vx.Graph(V, directed)
+    g.bulk_load_edges(e)
+    rng = np.random.default_rng(scale)
+    roots = rng.integers(0, V, size=k).astype(np.uint32)
+    if k > 2:
+        roots[1] = roots[0]
+        roots[2] = V + 5
+    m = vx.MultiRootBFS(g, roots)
+    m.run()
+    got = m.distances_array()
+    assert got.shape == (k, V)
+    csr = oracle_csr(e, V, directed)
+    for r in range(k):
+        if roots[r] >= V:
+            assert np.all(got[r] == U)
+            continue
+        exp = oracle_bfs(e, V, int(roots[r]), directed, csr)
+        assert np.array_equal(got[r], exp), f"root index {r}"
+
+
+def test_multiroot_on_updated_graph():
+    """Tombstoned base arcs and delta rows are traversed like the logical graph."""
+    V = 1 << 12
+    e = w.rmat_edges(12, seed=77)
+    g = vx.Graph(V, False)
+    g.bulk_load_edges(e)
+    st = w.mixed_stream(e, V, [3000, 3000], 0.5, seed=78)
+    og = OracleGraph(V, False, "port")
+    og.bulk_load_edges(e)
+    for i in range(st.batches):
+        g.apply_arrays(*st.batch(i))
+        og.apply(*st.batch(i))
+    roots = np.arange(0, 64, dtype=np.uint32) * 37
+    m = vx.MultiRootBFS(g, roots)
+    m.run()
+    got = m.distances_array()
+    for r, root in enumerate(roots.tolist()):
+        ob = OracleBFS(og, root)
+        assert np.array_equal(got[r], ob.distances()), r

@@ -25,17 +25,23 @@ namespace vxh {
 namespace {
 
 constexpr int kThreads = 1024;
-constexpr int kItems = 11;
-constexpr int kTile = kThreads * kItems;  // keys per CTA
 constexpr int kDigits = 256;
 constexpr int kMaxCluster = 8;
-constexpr size_t kSmem = 2ull * kTile * 8 + (kThreads / 32) * kDigits * 4 + 3 * kDigits * 4 + 64 * 4;
-static_assert(kSmem <= 227 * 1024, "cluster tile exceeds shared memory");
+// Two tile shapes: 4 keys per thread spreads mid-size batches over more SMs,
+// 11 keys per thread holds the largest batch one cluster can take.
+template <int ITEMS>
+struct Tile {
+  static constexpr int kItems = ITEMS;
+  static constexpr int kTile = kThreads * ITEMS;
+  static constexpr size_t kSmem = 2ull * kTile * 8 + (kThreads / 32) * kDigits * 4 + 3 * kDigits * 4 + 64 * 4;
+  static_assert(kSmem <= 227 * 1024, "cluster tile exceeds shared memory");
+};
 
 __device__ __forceinline__ uint32_t lanemask_lt() { return vxb::lanemask_lt(); }
 
 // Stable rank of the CTA's keys by one digit (warp w owns positions
 // [w*kItems*32, (w+1)*kItems*32); see prims.cu for the same scheme).
+template <int kItems>
 __device__ void rank_keys(const uint32_t (&d)[kItems], uint32_t (&rank)[kItems], uint32_t* warp_hist,
                           uint32_t* total) {
   constexpr int W = kThreads / 32;
@@ -91,10 +97,13 @@ __device__ void scan256(uint32_t* v) {
   }
 }
 
+template <int ITEMS>
 __global__ void __launch_bounds__(kThreads, 1)
     canon_cluster_kernel(const uint32_t* src, const uint32_t* dst, const uint8_t* add, uint32_t n, int directed,
                          int b, int sh, uint32_t bound, int passes, uint32_t* fu, uint32_t* fv, uint8_t* ff,
                          GraphCounters* ctr) {
+  constexpr int kItems = Tile<ITEMS>::kItems;
+  constexpr int kTile = Tile<ITEMS>::kTile;
   cg::cluster_group cluster = cg::this_cluster();
   const uint32_t C = cluster.num_blocks();
   const uint32_t r = cluster.block_rank();
@@ -149,7 +158,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       k[j] = A[pos0 + 32 * j];
       d[j] = (uint32_t)(k[j] >> shift) & 0xFFu;
     }
-    rank_keys(d, rank, warp_hist, total);
+    rank_keys<kItems>(d, rank, warp_hist, total);
     cluster.sync();  // every CTA's digit totals are final
     if (threadIdx.x < kDigits) {
       const uint32_t dd = threadIdx.x;
@@ -237,28 +246,22 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 }  // namespace
 
-size_t canon_cluster_capacity() { return (size_t)kMaxCluster * kTile; }
+size_t canon_cluster_capacity() { return (size_t)kMaxCluster * Tile<11>::kTile; }
 
-// Canonicalises the staged batch when it fits one cluster (*done = true);
-// returns a negative status on a launch error.
-int canon_cluster(Graph* g, size_t n, int b, uint32_t bound, bool* done) {
-  *done = false;
-  const size_t m = g->directed ? n : 2 * n;
-  int sbits = 1;
-  while (sbits < 32 && ((size_t)1 << sbits) < n) ++sbits;
-  const int sh = sbits + 1;
-  if (m == 0 || m > canon_cluster_capacity() || 2 * b + sh > 64) return 0;
-  *done = true;
+template <int ITEMS>
+static int launch_canon(Graph* g, size_t n, size_t m, int b, int sh, uint32_t bound) {
+  using T = Tile<ITEMS>;
   static bool attr = false;
   if (!attr) {
-    VX_CUDA_TRY(cudaFuncSetAttribute(canon_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem));
+    VX_CUDA_TRY(cudaFuncSetAttribute(canon_cluster_kernel<ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)T::kSmem));
     attr = true;
   }
-  const unsigned C = (unsigned)((m + kTile - 1) / kTile);
+  const unsigned C = (unsigned)((m + T::kTile - 1) / T::kTile);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(C);
   cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = kSmem;
+  cfg.dynamicSmemBytes = T::kSmem;
   cfg.stream = g->stream;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeClusterDimension;
@@ -270,9 +273,23 @@ int canon_cluster(Graph* g, size_t n, int b, uint32_t bound, bool* done) {
   const int passes = (2 * b + 7) / 8;
   BatchBuffers& B = g->batch;
   count_launch();
-  VX_CUDA_TRY(cudaLaunchKernelEx(&cfg, canon_cluster_kernel, B.src, B.dst, B.add, (uint32_t)n, (int)g->directed, b,
-                                 sh, bound, passes, B.fu, B.fv, B.ff, g->ctr));
+  VX_CUDA_TRY(cudaLaunchKernelEx(&cfg, canon_cluster_kernel<ITEMS>, B.src, B.dst, B.add, (uint32_t)n,
+                                 (int)g->directed, b, sh, bound, passes, B.fu, B.fv, B.ff, g->ctr));
   return 0;
+}
+
+// Canonicalises the staged batch when it fits one cluster (*done = true);
+// returns a negative status on a launch error.
+int canon_cluster(Graph* g, size_t n, int b, uint32_t bound, bool* done) {
+  *done = false;
+  const size_t m = g->directed ? n : 2 * n;
+  int sbits = 1;
+  while (sbits < 32 && ((size_t)1 << sbits) < n) ++sbits;
+  const int sh = sbits + 1;
+  if (m == 0 || m > canon_cluster_capacity() || 2 * b + sh > 64) return 0;
+  *done = true;
+  if (m <= (size_t)kMaxCluster * Tile<4>::kTile) return launch_canon<4>(g, n, m, b, sh, bound);
+  return launch_canon<11>(g, n, m, b, sh, bound);
 }
 
 }  // namespace vxh

@@ -321,16 +321,12 @@ constexpr int kListThreads = 1024;
 constexpr int kListItems = 32;
 constexpr size_t kListMax = (size_t)kListThreads * kListItems;
 
-__device__ uint32_t block_scan_1024(uint32_t v, uint32_t* wsum, uint32_t* total) {
+// Exclusive scan of the 32 per-warp counts of a 1024-thread block; every
+// thread gets its warp's base, *total the block sum.
+__device__ uint32_t warp_bases_1024(uint32_t warp_count, uint32_t* wsum, uint32_t* total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint32_t incl = v;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-    if (lane >= o) incl += y;
-  }
   __syncthreads();
-  if (lane == 31) wsum[warp] = incl;
+  if (lane == 0) wsum[warp] = warp_count;
   __syncthreads();
   if (warp == 0) {
     const uint32_t w = wsum[lane];
@@ -344,9 +340,11 @@ __device__ uint32_t block_scan_1024(uint32_t v, uint32_t* wsum, uint32_t* total)
     if (lane == 31) *total = wi;
   }
   __syncthreads();
-  return wsum[warp] + incl - v;
+  return wsum[warp];
 }
 
+// Warp w owns items [w * 1024, (w + 1) * 1024) and reads them in 32 coalesced
+// rounds; ballots give each selected item its position inside the warp.
 __global__ void __launch_bounds__(kListThreads) build_list_kernel(const uint32_t* fu, const uint32_t* fv,
                                                                    const uint8_t* ff, const uint32_t* count,
                                                                    int mode, uint32_t* lu, uint32_t* lv,
@@ -354,40 +352,42 @@ __global__ void __launch_bounds__(kListThreads) build_list_kernel(const uint32_t
                                                                    uint32_t* nruns) {
   __shared__ uint32_t wsum[32];
   __shared__ uint32_t total;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t F = *count;
-  const uint32_t base = threadIdx.x * kListItems;
-  uint32_t bits = 0, cnt = 0;
-  for (int j = 0; j < kListItems; ++j) {
-    const uint32_t i = base + j;
-    if (i >= F) break;
+  const uint32_t w0 = (uint32_t)warp * 32 * kListItems;
+  auto selected = [&](uint32_t i) {
+    if (i >= F) return false;
     const uint8_t f = ff[i];
-    const bool sel = !(f & kFInBase) && (f & kFChanged) && (((f & kFAdd) != 0) == (mode == 1));
-    bits |= (uint32_t)sel << j;
-    cnt += sel;
-  }
-  uint32_t pos = block_scan_1024(cnt, wsum, &total);
+    return !(f & kFInBase) && (f & kFChanged) && (((f & kFAdd) != 0) == (mode == 1));
+  };
+  uint32_t cnt = 0;
+  for (int r = 0; r < kListItems; ++r) cnt += __popc(__ballot_sync(0xFFFFFFFFu, selected(w0 + r * 32 + lane)));
+  uint32_t pos = warp_bases_1024(cnt, wsum, &total);
   const uint32_t n = total;
-  for (int j = 0; j < kListItems; ++j) {
-    if ((bits >> j) & 1u) {
-      lu[pos] = fu[base + j];
-      lv[pos] = fv[base + j];
-      ++pos;
+  for (int r = 0; r < kListItems; ++r) {
+    const uint32_t i = w0 + r * 32 + lane;
+    const bool sel = selected(i);
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, sel);
+    if (sel) {
+      const uint32_t o = pos + __popc(m & vxb::lanemask_lt());
+      lu[o] = fu[i];
+      lv[o] = fv[i];
     }
+    pos += __popc(m);
   }
   if (threadIdx.x == 0) *nlist = n;
   __syncthreads();  // the compacted list is visible to the whole block
-  bits = 0;
+  auto starts = [&](uint32_t k) { return k < n && (k == 0 || lu[k] != lu[k - 1]); };
   cnt = 0;
-  for (int j = 0; j < kListItems; ++j) {
-    const uint32_t k = base + j;
-    if (k >= n) break;
-    const bool st = k == 0 || lu[k] != lu[k - 1];
-    bits |= (uint32_t)st << j;
-    cnt += st;
+  for (int r = 0; r < kListItems; ++r) cnt += __popc(__ballot_sync(0xFFFFFFFFu, starts(w0 + r * 32 + lane)));
+  pos = warp_bases_1024(cnt, wsum, &total);
+  for (int r = 0; r < kListItems; ++r) {
+    const uint32_t k = w0 + r * 32 + lane;
+    const bool st = starts(k);
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, st);
+    if (st) runs[pos + __popc(m & vxb::lanemask_lt())] = k;
+    pos += __popc(m);
   }
-  pos = block_scan_1024(cnt, wsum, &total);
-  for (int j = 0; j < kListItems; ++j)
-    if ((bits >> j) & 1u) runs[pos++] = base + j;
   if (threadIdx.x == 0) *nruns = total;
 }
 
