@@ -148,6 +148,44 @@ int vx_mrbfs_set_pull_fraction(vx_mrbfs* m, float frac);
 /* One-shot form: create, run, copy k*V distances into out (cap entries). */
 int vx_multiroot_bfs(vx_graph* g, const uint32_t* roots, size_t k, uint32_t* out, size_t cap);
 
+/* ---- Repair-vs-recompute selector -----------------------------------------
+ * The reference chooses between IncrementalBFS::apply and graph.apply +
+ * recompute in its benchmark harnesses (benchmarks/publication_policy_bfs.cpp:
+ * 163-235).  Here: 16 batch features computed on the device, a 16-64-64-2 fp32
+ * MLP (5,378 parameters) trained and evaluated by the library's own kernels,
+ * and the reference's adaptive heuristic as the fallback. */
+#define VX_SEL_FEATURES 16
+#define VX_SEL_PARAMS 5378
+typedef struct vx_selector vx_selector;
+typedef struct vx_heuristic vx_heuristic;
+
+/* Stage a host batch (canonicalise + classify, no mutation) and compute its
+ * features; then run exactly one of vx_bfs_run_repair (IncrementalBFS::apply,
+ * bfs.hpp:29-98) or vx_bfs_run_full (graph apply + recompute). */
+int vx_bfs_stage(vx_bfs* b, const uint32_t* src, const uint32_t* dst, const uint8_t* add, size_t n);
+int vx_bfs_staged_features(vx_bfs* b, float prev_affected_fraction, float* out16);
+int vx_bfs_run_repair(vx_bfs* b);
+int vx_bfs_run_full(vx_bfs* b);
+
+int vx_selector_create(uint64_t seed, vx_selector** out);
+int vx_selector_destroy(vx_selector* s);
+/* Adam on standardised log-time targets: X n x 16, Y n x 2 (repair, full). */
+int vx_selector_train(vx_selector* s, const float* X, const float* Y, size_t n, uint32_t epochs, uint32_t batch,
+                      float lr, uint32_t seed, float* final_loss);
+/* Mean-squared-error gradient of one minibatch (n <= 64) -> grad[5378]. */
+int vx_selector_gradients(vx_selector* s, const float* X, const float* Y, size_t n, float* grad, float* loss);
+int vx_selector_predict(vx_selector* s, const float* X, size_t n, float* Y);
+int vx_selector_set_params(vx_selector* s, const float* params);
+int vx_selector_get_params(vx_selector* s, float* params);
+
+/* The reference's adaptive selector (publication_policy_bfs.cpp:163-235, EMA
+ * updates :285-320), used as the fallback and as the baseline of regret. */
+int vx_heuristic_create(size_t vertices, double initial_reachable_fraction, double initial_full_us,
+                        vx_heuristic** out);
+int vx_heuristic_destroy(vx_heuristic* h);
+int vx_heuristic_decide(vx_heuristic* h, double update_fraction, double shallow_fraction, int* choose_full);
+int vx_heuristic_observe(vx_heuristic* h, int observed_full, double execution_us, double affected_fraction);
+
 #ifdef __cplusplus
 }
 #endif

@@ -959,6 +959,7 @@ int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac) {
   if (cudaMalloc(&b->ctr, sizeof(BfsCounters)) != cudaSuccess ||
       cudaMalloc(&b->trace, 2 * (kTraceLevels + 1) * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&b->barrier, vxb::kBarrierWords * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&b->features, 64 * sizeof(float)) != cudaSuccess ||
       cudaMallocHost(&b->hctr, sizeof(BfsCounters)) != cudaSuccess) {
     set_error("BFS counter allocation failed");
     bfs_destroy(b);
@@ -984,6 +985,7 @@ void bfs_destroy(Bfs* b) {
   cudaFree(b->ctr);
   cudaFree(b->trace);
   cudaFree(b->barrier);
+  cudaFree(b->features);
   cudaFreeHost(b->hctr);
   delete b;
 }
@@ -1002,18 +1004,26 @@ int bfs_recompute(Bfs* b) {
   return launch(b, p, kModeFull);
 }
 
-int bfs_apply_staged(Bfs* b, size_t n, size_t vertex_bound) {
+int bfs_stage(Bfs* b, size_t n, size_t vertex_bound) {
   Graph* g = b->g;
   cudaStream_t s = g->stream;
   // last_* counters reset on every apply (bfs.hpp:30-33)
   VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->candidates, 0, 4 * sizeof(uint32_t), s));
+  b->staged_ops = n;
+  b->staged_V_pre = g->V;
+  b->staged_len_pre = b->dist_len;
   if (n == 0) return 0;
-  const size_t V_pre = g->V;
-  const size_t len_pre = b->dist_len;
   VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->cand_n, 0, 3 * sizeof(uint32_t), s));
   if (int rc = graph_stage_batch(g, n, vertex_bound)) return rc;
+  return ensure_capacity(b, std::max<size_t>(g->V, 1));
+}
+
+int bfs_repair_staged(Bfs* b) {
+  Graph* g = b->g;
+  cudaStream_t s = g->stream;
+  if (b->staged_ops == 0) return 0;
+  const size_t V_pre = b->staged_V_pre, len_pre = b->staged_len_pre;
   const size_t V_post = g->V;
-  if (int rc = ensure_capacity(b, std::max<size_t>(V_post, 1))) return rc;
   // fallback limit: max(1, size_t(double(V) * fraction))  (bfs.hpp:225-226)
   unsigned long long lim = (unsigned long long)((double)V_pre * b->frac);
   if (lim < 1) lim = 1;
@@ -1032,9 +1042,22 @@ int bfs_apply_staged(Bfs* b, size_t n, size_t vertex_bound) {
     VX_CUDA_TRY(cudaMemsetAsync(b->dist + b->dist_len, 0xFF, (V_post - b->dist_len) * 4, s));
     b->dist_len = V_post;
   }
+  b->staged_ops = 0;
   Params p = make_params(b, (uint32_t)V_post, (uint32_t)b->dist_len);
   p.fallback_limit = lim;
   return launch(b, p, kModePost);
+}
+
+int bfs_full_staged(Bfs* b) {
+  if (b->staged_ops == 0) return 0;
+  if (int rc = graph_commit_batch(b->g)) return rc;
+  b->staged_ops = 0;
+  return bfs_recompute(b);
+}
+
+int bfs_apply_staged(Bfs* b, size_t n, size_t vertex_bound) {
+  if (int rc = bfs_stage(b, n, vertex_bound)) return rc;
+  return bfs_repair_staged(b);
 }
 
 int bfs_sync(Bfs* b) {

@@ -60,6 +60,8 @@ struct Bfs {
   BfsCounters* hctr = nullptr;
   unsigned long long* trace = nullptr;  // per-level timestamps of the last full BFS
   uint32_t* barrier = nullptr;          // grid barrier words (vxb::kBarrierWords)
+  float* features = nullptr;            // selector features of the staged batch
+  size_t staged_ops = 0, staged_V_pre = 0, staged_len_pre = 0;  // batch staged by bfs_stage
   BfsTuning tune;
   int grid = 0;
 };
@@ -67,8 +69,14 @@ struct Bfs {
 int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac);
 void bfs_destroy(Bfs* b);
 int bfs_recompute(Bfs* b);
-// Incremental apply of the batch staged in b->g->batch (ops already on device).
+// Incremental apply of the batch in b->g->batch (ops already on device):
+// bfs_stage (canonicalise + classify on the pre-batch graph) followed by
+// bfs_repair_staged (the reference's apply) or bfs_full_staged (graph apply +
+// recompute, the explicit full arm of the reference's selector harness).
 int bfs_apply_staged(Bfs* b, size_t n, size_t vertex_bound);
+int bfs_stage(Bfs* b, size_t n, size_t vertex_bound);
+int bfs_repair_staged(Bfs* b);
+int bfs_full_staged(Bfs* b);
 int bfs_sync(Bfs* b);  // copies counters to hctr (synchronises the stream)
 int bfs_reached_arcs(Bfs* b, unsigned long long* arcs);  // sum of degrees of reached vertices
 // Per-level trace of the last full BFS: pairs {globaltimer ns, n_f | bottom_up << 63}

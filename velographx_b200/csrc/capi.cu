@@ -10,6 +10,7 @@
 #include "bfs.cuh"
 #include "graph.cuh"
 #include "mrbfs.cuh"
+#include "selector.cuh"
 
 namespace vxh {
 
@@ -36,6 +37,12 @@ struct vx_bfs {
 };
 struct vx_mrbfs {
   vxh::MrBfs* m;
+};
+struct vx_selector {
+  vxh::Selector* s;
+};
+struct vx_heuristic {
+  vxh::HeuristicState h;
 };
 
 namespace {
@@ -385,6 +392,115 @@ int vx_multiroot_bfs(vx_graph* g, const uint32_t* roots, size_t k, uint32_t* out
   if (!rc) rc = vx_mrbfs_distances(m, out, cap, &n);
   vx_mrbfs_destroy(m);
   return rc;
+}
+
+int vx_bfs_stage(vx_bfs* b, const uint32_t* src, const uint32_t* dst, const uint8_t* add, size_t n) {
+  if (!b || (n && (!src || !dst || !add))) return fail(VX_ERR_INVALID, "null argument");
+  vxh::Graph* g = b->b->g;
+  size_t v_after = g->V;
+  if (n)
+    if (int rc = upload_batch(g, src, dst, add, n, &v_after)) return rc;
+  return vxh::bfs_stage(b->b, n, v_after);
+}
+
+int vx_bfs_staged_features(vx_bfs* b, float prev_affected_fraction, float* out16) {
+  if (!b || !out16) return fail(VX_ERR_INVALID, "null argument");
+  vxh::Bfs* x = b->b;
+  vxh::Graph* g = x->g;
+  if (int rc = vxh::bfs_sync(x)) return rc;
+  if (int rc = vxh::graph_sync_counters(g)) return rc;
+  vxh::SelInputs in;
+  in.ops = x->staged_ops;
+  in.edges = vxh::graph_edge_count_directed(g);
+  in.vertices = (uint32_t)g->V;
+  in.levels = x->hctr->levels;
+  in.reachable_fraction = (float)((double)x->hctr->reachable / (double)std::max<size_t>(1, g->V));
+  in.prev_affected_fraction = prev_affected_fraction;
+  if (x->staged_ops == 0) {
+    for (int i = 0; i < vxh::kSelFeatures; ++i) out16[i] = 0.f;
+    return VX_OK;
+  }
+  return vxh::batch_features(x, x->staged_ops, in, out16);
+}
+
+int vx_bfs_run_repair(vx_bfs* b) {
+  if (!b) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::bfs_repair_staged(b->b);
+}
+
+int vx_bfs_run_full(vx_bfs* b) {
+  if (!b) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::bfs_full_staged(b->b);
+}
+
+int vx_selector_create(uint64_t seed, vx_selector** out) {
+  if (!out) return fail(VX_ERR_INVALID, "null argument");
+  vxh::Selector* s = nullptr;
+  if (int rc = vxh::selector_create(&s, seed)) return rc;
+  *out = new vx_selector{s};
+  return VX_OK;
+}
+
+int vx_selector_destroy(vx_selector* s) {
+  if (!s) return VX_OK;
+  vxh::selector_destroy(s->s);
+  delete s;
+  return VX_OK;
+}
+
+int vx_selector_train(vx_selector* s, const float* X, const float* Y, size_t n, uint32_t epochs, uint32_t batch,
+                      float lr, uint32_t seed, float* final_loss) {
+  if (!s || !X || !Y) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::selector_train(s->s, X, Y, n, epochs, batch, lr, seed, final_loss);
+}
+
+int vx_selector_gradients(vx_selector* s, const float* X, const float* Y, size_t n, float* grad, float* loss) {
+  if (!s || !X || !Y || !grad) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::selector_gradients(s->s, X, Y, n, grad, loss);
+}
+
+int vx_selector_predict(vx_selector* s, const float* X, size_t n, float* Y) {
+  if (!s || (n && (!X || !Y))) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::selector_predict(s->s, X, n, Y);
+}
+
+int vx_selector_set_params(vx_selector* s, const float* params) {
+  if (!s || !params) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::selector_set_params(s->s, params);
+}
+
+int vx_selector_get_params(vx_selector* s, float* params) {
+  if (!s || !params) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::selector_get_params(s->s, params);
+}
+
+int vx_heuristic_create(size_t vertices, double initial_reachable_fraction, double initial_full_us,
+                        vx_heuristic** out) {
+  if (!out) return fail(VX_ERR_INVALID, "null argument");
+  vx_heuristic* h = new vx_heuristic();
+  h->h.large_scale = vertices >= 200000;  // publication_policy_bfs.cpp:94
+  h->h.initial_reachable_fraction = initial_reachable_fraction;
+  h->h.ema_full_us = initial_full_us;
+  h->h.have_full = true;
+  *out = h;
+  return VX_OK;
+}
+
+int vx_heuristic_destroy(vx_heuristic* h) {
+  delete h;
+  return VX_OK;
+}
+
+int vx_heuristic_decide(vx_heuristic* h, double update_fraction, double shallow_fraction, int* choose_full) {
+  if (!h || !choose_full) return fail(VX_ERR_INVALID, "null argument");
+  *choose_full = vxh::heuristic_decide(h->h, update_fraction, shallow_fraction) ? 1 : 0;
+  return VX_OK;
+}
+
+int vx_heuristic_observe(vx_heuristic* h, int observed_full, double execution_us, double affected_fraction) {
+  if (!h) return fail(VX_ERR_INVALID, "null argument");
+  vxh::heuristic_observe(h->h, observed_full != 0, execution_us, affected_fraction);
+  return VX_OK;
 }
 
 }  // extern "C"

@@ -150,6 +150,7 @@ PYBIND11_MODULE(_velographx, m) {
       .def("compact", &DynamicGraph::compact)
       // extras beyond the reference module
       .def_property_readonly("directed", &DynamicGraph::directed)
+      .def_property_readonly("handle", [](DynamicGraph& g) { return reinterpret_cast<std::uintptr_t>(g.handle()); })
       .def("in_neighbors", &DynamicGraph::in_neighbors)
       .def("has_edge", &DynamicGraph::has_edge)
       .def("edge_count_directed", &DynamicGraph::edge_count_directed)
@@ -199,6 +200,8 @@ PYBIND11_MODULE(_velographx, m) {
       .def("recompute", &IncrementalBFS::recompute)
       .def_property_readonly_static("unreachable", [](py::object) { return IncrementalBFS::unreachable; })
       // extras
+      .def_property_readonly("handle", [](IncrementalBFS& x) { return reinterpret_cast<std::uintptr_t>(x.handle()); })
+      .def("mark_stale", [](IncrementalBFS& x) { x.mark_stale(); })
       .def_property_readonly("reachable_count", &IncrementalBFS::reachable_count)
       .def_property_readonly("last_deletion_candidates", &IncrementalBFS::last_deletion_candidates)
       .def_property_readonly("last_affected_vertices", &IncrementalBFS::last_affected_vertices)
