@@ -148,6 +148,24 @@ int vx_mrbfs_set_pull_fraction(vx_mrbfs* m, float frac);
 /* One-shot form: create, run, copy k*V distances into out (cap entries). */
 int vx_multiroot_bfs(vx_graph* g, const uint32_t* roots, size_t k, uint32_t* out, size_t cap);
 
+/* ---- Allocation-free full BFS ---------------------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (their device memory is owned by another allocator, or they must not block
+ * on the driver's allocator once running): the same direction-optimising BFS
+ * as vx_bfs_recompute, on a CSR the caller holds in device memory (out- and
+ * in-rows; pass the same arrays twice for an undirected graph; column ids
+ * below 2^31), writing `vertices` distances to d_dist.  All other working
+ * memory is one file-scope device array (~6.3 MB per GPU that loads the
+ * library, held until exit), so at most 262,144 vertices (larger counts
+ * return VX_ERR_RANGE).  Calls share that array: calls that overlap on the
+ * GPU race, so issue them one at a time per device.  The first call on a
+ * device looks up the array's address on that device; make it before any
+ * stream capture.  Runs on `stream` (a cudaStream_t, 0 for the legacy
+ * stream), waits for completion, and returns the reachable count. */
+int vx_bfs_csr_static(const uint64_t* d_out_offsets, const uint32_t* d_out_cols, const uint64_t* d_in_offsets,
+                      const uint32_t* d_in_cols, uint32_t vertices, uint64_t arcs, uint32_t source, uint32_t* d_dist,
+                      void* stream, uint64_t* reachable);
+
 /* ---- Repair-vs-recompute selector -----------------------------------------
  * The reference chooses between IncrementalBFS::apply and graph.apply +
  * recompute in its benchmark harnesses (benchmarks/publication_policy_bfs.cpp:

@@ -1096,3 +1096,141 @@ int bfs_level_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n) {
   return 0;
 }
 }  // namespace vxh
+
+// ------------------------------------------------ allocation-free full BFS --
+//
+// Some callers cannot call cudaMalloc: a host framework that owns the whole
+// device memory through its own pool (and forbids raw driver allocations),
+// or a latency-critical serving loop that must never block on the driver's
+// allocator after start-up.  vx_bfs_csr_static serves them: it runs the same
+// direction-optimising BFS kernel as recompute() on a CSR the caller already
+// holds in device memory, writing distances into the caller's buffer, and
+// keeps every other buffer (visited and frontier bitmaps, frontier queues,
+// counters, barrier words, the empty delta-row table) in one file-scope
+// device array.  It allocates nothing.
+//
+// Limits and sharing: at most kStaticMaxVertices vertices; every GPU that
+// loads this library holds the array (about 6.3 MB) until the process exits;
+// all calls share it and it keeps the last call's contents, so calls that
+// overlap on the GPU (different streams, different threads) race -- issue
+// them one at a time per device.  The first call on a device looks up the
+// array's device address for that device; make that first call before any
+// stream capture.
+namespace vxh {
+namespace {
+
+constexpr uint32_t kStaticMaxVertices = 1u << 18;  // 262,144
+constexpr uint32_t kStaticWords = kStaticMaxVertices / 32 + 1;
+
+struct StaticBfsScratch {
+  uint32_t vis[kStaticWords];
+  uint32_t fb[3][kStaticWords];
+  uint32_t q[3][kStaticMaxVertices];
+  uint32_t big[kStaticMaxVertices];
+  uint2 drow[kStaticMaxVertices];  // kept all-zero: a plain CSR has no delta rows
+  BfsCounters ctr;
+  uint32_t bar[vxb::kBarrierWords];
+};
+
+}  // namespace
+}  // namespace vxh
+
+static __device__ __align__(256) unsigned char vx_static_bfs_scratch[sizeof(vxh::StaticBfsScratch)];
+
+namespace {
+constexpr int kStaticMaxDevices = 64;
+void* g_static_scratch_addr[kStaticMaxDevices];  // device address of the array, per device
+}  // namespace
+
+extern "C" int vx_bfs_csr_static(const uint64_t* d_out_offsets, const uint32_t* d_out_cols,
+                                 const uint64_t* d_in_offsets, const uint32_t* d_in_cols, uint32_t vertices,
+                                 uint64_t arcs, uint32_t source, uint32_t* d_dist, void* stream,
+                                 uint64_t* reachable) {
+  using vxh::StaticBfsScratch;
+  if (!d_out_offsets || !d_out_cols || !d_in_offsets || !d_in_cols || !d_dist) {
+    vxh::set_error("vx_bfs_csr_static: null argument");
+    return -1;
+  }
+  if (vertices == 0 || vertices > vxh::kStaticMaxVertices) {
+    vxh::set_error("vx_bfs_csr_static: %u vertices; the static scratch holds 1..%u", vertices,
+                   vxh::kStaticMaxVertices);
+    return -2;
+  }
+  int dev = 0;
+  VX_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kStaticMaxDevices) {
+    vxh::set_error("vx_bfs_csr_static: device %d beyond the supported %d", dev, kStaticMaxDevices);
+    return -2;
+  }
+  if (!g_static_scratch_addr[dev]) {
+    // one-time set-up on this device (the device is current here)
+    void* ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, vx_static_bfs_scratch);
+    if (e != cudaSuccess || !ptr) {
+      vxh::set_error("vx_bfs_csr_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+      return -3;
+    }
+    g_static_scratch_addr[dev] = ptr;
+  }
+  StaticBfsScratch* sc = static_cast<StaticBfsScratch*>(g_static_scratch_addr[dev]);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // what must start at zero: counters, barrier words, the delta-row table
+  VX_CUDA_TRY(cudaMemsetAsync(&sc->ctr, 0, sizeof(vxh::BfsCounters), s));
+  VX_CUDA_TRY(cudaMemsetAsync(sc->bar, 0, sizeof(sc->bar), s));
+  VX_CUDA_TRY(cudaMemsetAsync(sc->drow, 0, (size_t)vertices * sizeof(uint2), s));
+  vxh::Params p;
+  memset(&p, 0, sizeof(p));
+  auto adj = [&](const uint64_t* off, const uint32_t* col) {
+    vxb::DevAdj a;
+    memset(&a, 0, sizeof(a));
+    a.off = off;
+    a.col = const_cast<uint32_t*>(col);
+    a.Vb = vertices;
+    a.drow = sc->drow;
+    return a;
+  };
+  p.g.out = adj(d_out_offsets, d_out_cols);
+  p.g.in = adj(d_in_offsets, d_in_cols);
+  p.g.V = vertices;
+  p.g.directed = d_in_offsets != d_out_offsets || d_in_cols != d_out_cols;
+  p.V = vertices;
+  p.dist_len = vertices;
+  p.source = source;
+  p.dist = d_dist;
+  p.vis = sc->vis;
+  for (int k = 0; k < 3; ++k) {
+    p.fb[k] = sc->fb[k];
+    p.q[k] = sc->q[k];
+  }
+  p.big = sc->big;
+  p.c = &sc->ctr;
+  p.total_arcs = arcs;
+  p.alpha = 14.0f;
+  p.beta = 24.0f;
+  p.large_row = 1024;
+  p.bar = sc->bar;
+  int per_sm = 0, sms = 0;
+  VX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vxh::bfs_kernel, vxh::kThreads, 0));
+  VX_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (per_sm < 1) {
+    vxh::set_error("vx_bfs_csr_static: BFS kernel cannot be resident on an SM");
+    return -3;
+  }
+  p.nblocks = (uint32_t)(per_sm * sms);
+  int mode = vxh::kModeFull;
+  void* args[] = {&p, &mode};
+  vxh::count_launch();
+  VX_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)vxh::bfs_kernel, dim3(p.nblocks), dim3(vxh::kThreads), args,
+                                          0, s));
+  uint32_t err = 0;
+  unsigned long long reach = 0;
+  VX_CUDA_TRY(cudaMemcpyAsync(&err, &sc->ctr.err, sizeof(err), cudaMemcpyDeviceToHost, s));
+  VX_CUDA_TRY(cudaMemcpyAsync(&reach, &sc->ctr.reachable, sizeof(reach), cudaMemcpyDeviceToHost, s));
+  VX_CUDA_TRY(cudaStreamSynchronize(s));
+  if (err) {
+    vxh::set_error("vx_bfs_csr_static: device error word 0x%x", err);
+    return -5;
+  }
+  if (reachable) *reachable = reach;
+  return 0;
+}
