@@ -1,0 +1,176 @@
+"""GPU: the repair-vs-recompute selector.
+
+* the MLP gradient kernel against the fp64 oracle (oracle/selector_ref.py);
+* the inference kernel against the fp64 forward pass;
+* the training kernel fits a smooth synthetic target;
+* the 16 batch features computed on the device against a numpy restatement
+  of their definitions on the first batch after a bulk load;
+* a reduced regime study: both arms on two replicas give bit-identical
+  distances, and the trained network's held-out regret is at or below the
+  heuristic's.
+"""
+import numpy as np
+import pytest
+
+from oracle import selector_ref as ref
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import velographx_b200 as vx  # noqa: E402
+from velographx_b200 import selector as sel  # noqa: E402
+from velographx_b200 import workloads as w  # noqa: E402
+
+# fp32 accumulation over at most 64 samples x 64 hidden units
+GRAD_RTOL = 2e-4
+
+
+@pytest.mark.parametrize("B", [1, 7, 64])
+def test_gradient_kernel_matches_fp64_oracle(B):
+    rng = np.random.default_rng(B)
+    m = sel.MLPSelector(seed=3)
+    P = m.params.astype(np.float64)
+    P[ref.O_B1:ref.O_W2] = rng.normal(0, 0.1, ref.H)
+    P[ref.O_B2:ref.O_W3] = rng.normal(0, 0.1, ref.H)
+    m.params = P.astype(np.float32)
+    P = m.params.astype(np.float64)
+    X = rng.normal(0, 1, (B, ref.IN)).astype(np.float32)
+    Y = rng.normal(0, 1, (B, ref.OUT)).astype(np.float32)
+    g, loss = m.gradients(X, Y)
+    loss_ref, g_ref = ref.loss_and_grad(P, X, Y)
+    assert loss == pytest.approx(loss_ref, rel=1e-4)
+    scale = np.abs(g_ref).max()
+    assert np.abs(g - g_ref).max() <= GRAD_RTOL * scale
+
+
+def test_inference_kernel_matches_fp64_forward():
+    rng = np.random.default_rng(5)
+    m = sel.MLPSelector(seed=9)
+    X = rng.normal(0, 1, (5000, ref.IN)).astype(np.float32)
+    Y = m.predict_log(X)
+    Yr = ref.forward(m.params.astype(np.float64), X)
+    assert np.abs(Y - Yr).max() <= 1e-4 * max(1.0, np.abs(Yr).max())
+
+
+def test_training_kernel_fits_a_smooth_target():
+    rng = np.random.default_rng(6)
+    X = rng.uniform(0, 1, (2000, ref.IN)).astype(np.float32)
+    t_rep = np.exp(1.0 + 3.0 * X[:, 0] + X[:, 1] * X[:, 2])
+    t_full = np.exp(2.5 + 0.5 * X[:, 3])
+    m = sel.MLPSelector(seed=1)
+    logs = np.log(np.stack([t_rep, t_full], 1))
+    m.mean, m.std = float(logs.mean()), float(logs.std())
+    before = float(np.mean((m.predict_log(X) - (logs - m.mean) / m.std) ** 2))
+    loss = m.fit(X, t_rep, t_full, epochs=60, batch=32, lr=3e-3)
+    after = float(np.mean((m.predict_log(X) - (logs - m.mean) / m.std) ** 2))
+    assert np.isfinite(loss) and after < 0.05 * before and after < 0.02
+    full, ok = m.choose_full(X)
+    assert ok.all() and np.mean(full == (t_full <= t_rep)) > 0.95
+
+
+def test_training_rejects_bad_arguments():
+    m = sel.MLPSelector()
+    X = np.zeros((4, ref.IN), np.float32)
+    with pytest.raises(RuntimeError):
+        m.fit(X, np.ones(4), np.ones(4), batch=65)
+    with pytest.raises(RuntimeError):
+        m.gradients(np.zeros((65, ref.IN), np.float32), np.zeros((65, 2), np.float32))
+
+
+def numpy_features(edges, V, src, dst, add, dist, levels, reach_frac, prev_aff, arcs_before):
+    """The 16 features of the first batch after a bulk load (undirected)."""
+    e = edges[edges[:, 0] != edges[:, 1]].astype(np.int64)
+    present = set(map(tuple, np.concatenate([e, e[:, ::-1]]).tolist()))
+    deg = np.zeros(V, np.int64)
+    for u, v in present:
+        deg[u] += 1
+    last = {}
+    for i, (u, v, a) in enumerate(zip(src.tolist(), dst.tolist(), add.tolist())):
+        if u == v:
+            continue
+        last[(u, v)] = a
+        last[(v, u)] = a
+    U = 0xFFFFFFFF
+    depth = float(levels + 1)
+    s = np.zeros(8)
+    mxdeg, mxd, mnd = 0.0, 0.0, 1e30
+    for (u, v), a in last.items():
+        du = int(dist[u]) if u < len(dist) else U
+        dv = int(dist[v]) if v < len(dist) else U
+        lg = np.log2(1.0 + (deg[v] if v < V else 0))
+        s[7] += lg
+        mxdeg = max(mxdeg, lg)
+        if not a:
+            s[0] += 1
+            if (u, v) in present:
+                s[1] += 1
+                if du != U and dv != U and du + 1 == dv:
+                    s[2] += 1
+                    s[3] += dv <= 3
+                    s[4] += dv / depth
+                    s[5] += lg
+                    mnd = min(mnd, dv / depth)
+                    mxd = max(mxd, dv / depth)
+        elif du != U:
+            s[6] += 1.0 if dv == U else (0.5 if du + 1 < dv else 0.0)
+    F = max(1, len(last))
+    trees = max(1.0, s[2])
+    ops = len(src)
+    return np.array([
+        np.log1p(ops) / 16, np.log1p(1000 * ops / max(1, arcs_before)) / 10, s[0] / F, s[1] / F, s[2] / F,
+        s[3] / F, s[4] / trees if s[2] else 0, mnd if s[2] else 1, mxd, s[6] / F, s[5] / trees / 32 if s[2] else 0,
+        mxdeg / 32, s[7] / F / 32, reach_frac, prev_aff, np.log2(1 + V) / 32], np.float64)
+
+
+@pytest.mark.parametrize("ops,seed", [(40, 1), (3000, 2)])
+def test_device_features_match_numpy(ops, seed):
+    import ctypes as C
+
+    V = 1 << 12
+    edges = w.rmat_edges(12, 8, seed=seed)
+    g = vx.Graph(V, False)
+    g.bulk_load_edges(edges)
+    root = w.max_degree_root(edges, V)
+    b = vx.IncrementalBFS(g, root, 2.0)
+    dist = b.distances_array()
+    st = b.stats()
+    arcs = g.edge_count_directed()
+    stream = w.mixed_stream(edges, V, [ops], 0.5, seed=seed)
+    s, d, a = (np.ascontiguousarray(x) for x in stream.batch(0))
+    lib = sel._lib()
+    f16 = np.zeros(16, np.float32)
+    assert lib.vx_bfs_stage(C.c_void_p(b.handle), s.ctypes.data_as(sel._u32p), d.ctypes.data_as(sel._u32p),
+                            a.ctypes.data_as(sel._u8p), len(s)) == 0
+    assert lib.vx_bfs_staged_features(C.c_void_p(b.handle), 0.125, f16.ctypes.data_as(sel._f32p)) == 0
+    want = numpy_features(edges, V, s, d, a, dist, st["levels"], st["reachable_count"] / V, 0.125, arcs)
+    assert np.allclose(f16, want, rtol=1e-4, atol=1e-5), np.c_[f16, want]
+    assert lib.vx_bfs_run_repair(C.c_void_p(b.handle)) == 0
+    b.mark_stale()
+    g2 = vx.Graph(V, False)
+    g2.bulk_load_edges(edges)
+    g2.apply_arrays(s, d, a)
+    assert np.array_equal(b.distances_array(), vx.IncrementalBFS(g2, root).distances_array())
+
+
+def test_reduced_regime_study():
+    V = 1 << 14
+    edges = w.rmat_edges(14, 16, seed=21)
+    root = w.max_degree_root(edges, V)
+    sizes = np.tile([10, 300, 3000, 30000], 12)
+    rd = sel.collect("rmat14", edges, V, root, sizes, 0.75, seed=4)
+    assert rd.exact
+    assert np.all(rd.t_repair > 0) and np.all(rd.t_full > 0)
+    assert np.all(np.isfinite(rd.features))
+    rep = sel.evaluate([rd], train_fraction=0.3, epochs=200)
+    for arm in ("mlp", "heuristic"):
+        r = rep[arm]
+        assert 0 <= r["wrong_arm_rate"] <= 1
+        assert r["equal_regime_mean_regret"] >= 0 and np.isfinite(r["max_regret"])
+    assert rep["mlp"]["fallbacks"] == 0
+    # what the trained network gains over the heuristic on held-out batches
+    # (timing noise gets a 1% slack)
+    assert rep["mlp"]["equal_regime_mean_regret"] <= rep["heuristic"]["equal_regime_mean_regret"] + 0.01, rep
+    print(rep)

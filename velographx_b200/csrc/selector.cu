@@ -369,7 +369,7 @@ static int upload(const void* host, size_t bytes, void** dev) {
     set_error("selector staging allocation failed");
     return -4;
   }
-  if (bytes) VX_CUDA_TRY(cudaMemcpy(*dev, host, bytes, cudaMemcpyHostToDevice));
+  if (bytes && host) VX_CUDA_TRY(cudaMemcpy(*dev, host, bytes, cudaMemcpyHostToDevice));
   return 0;
 }
 

@@ -1,0 +1,416 @@
+"""Repair-vs-recompute selection on the GPU.
+
+The reference chooses, per update batch, between ``IncrementalBFS.apply``
+(repair) and ``graph.apply`` + ``recompute`` (full) in its benchmark harnesses
+(benchmarks/publication_policy_bfs.cpp:46-335) with a hand-tuned heuristic;
+regret is measured offline against the per-batch oracle
+min(t_repair, t_full), full winning ties (tools/summarize_publication_policy.py:66,72).
+
+Here:
+
+* ``collect`` runs a regime's stream on two graph replicas in lockstep -- one
+  executes the repair arm, the other the full arm -- so every batch carries
+  its 16 device-computed features and both arms' GPU times (CUDA events on the
+  graph's stream), and the two replicas' distances are compared bit for bit;
+* ``MLPSelector`` trains the 16-64-64-2 network with the library's own
+  kernels (vx_selector_train) on standardised log times and predicts both arms;
+* ``Heuristic`` is the reference's adaptive selector, restated in the library
+  (vx_heuristic_*), used as fallback and baseline;
+* ``evaluate`` replays the held-out batches through both selectors and
+  reports regret and wrong-arm rates.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import IncrementalBFS, Graph, capi
+from . import workloads as w
+
+N_FEATURES = 16
+N_PARAMS = 5378
+
+_f32p = C.POINTER(C.c_float)
+_u32p = C.POINTER(C.c_uint32)
+_u8p = C.POINTER(C.c_uint8)
+
+
+def _lib():
+    lib = capi()
+    sig = {
+        "vx_bfs_stage": (C.c_int, [C.c_void_p, _u32p, _u32p, _u8p, C.c_size_t]),
+        "vx_bfs_staged_features": (C.c_int, [C.c_void_p, C.c_float, _f32p]),
+        "vx_bfs_run_repair": (C.c_int, [C.c_void_p]),
+        "vx_bfs_run_full": (C.c_int, [C.c_void_p]),
+        "vx_selector_create": (C.c_int, [C.c_uint64, C.POINTER(C.c_void_p)]),
+        "vx_selector_destroy": (C.c_int, [C.c_void_p]),
+        "vx_selector_train": (C.c_int, [C.c_void_p, _f32p, _f32p, C.c_size_t, C.c_uint32, C.c_uint32, C.c_float,
+                                        C.c_uint32, _f32p]),
+        "vx_selector_gradients": (C.c_int, [C.c_void_p, _f32p, _f32p, C.c_size_t, _f32p, _f32p]),
+        "vx_selector_predict": (C.c_int, [C.c_void_p, _f32p, C.c_size_t, _f32p]),
+        "vx_selector_set_params": (C.c_int, [C.c_void_p, _f32p]),
+        "vx_selector_get_params": (C.c_int, [C.c_void_p, _f32p]),
+        "vx_heuristic_create": (C.c_int, [C.c_size_t, C.c_double, C.c_double, C.POINTER(C.c_void_p)]),
+        "vx_heuristic_destroy": (C.c_int, [C.c_void_p]),
+        "vx_heuristic_decide": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.POINTER(C.c_int)]),
+        "vx_heuristic_observe": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        from . import last_error
+
+        raise RuntimeError(f"vx_b200 error {rc}: {last_error()}")
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class MLPSelector:
+    """The 16-64-64-2 network on the GPU (vx_selector_*)."""
+
+    def __init__(self, seed: int = 1):
+        self.lib = _lib()
+        self.h = C.c_void_p()
+        _check(self.lib.vx_selector_create(seed, C.byref(self.h)))
+        self.mean = 0.0
+        self.std = 1.0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.vx_selector_destroy(self.h)
+            self.h = None
+
+    @property
+    def params(self) -> np.ndarray:
+        out = np.empty(N_PARAMS, np.float32)
+        _check(self.lib.vx_selector_get_params(self.h, out.ctypes.data_as(_f32p)))
+        return out
+
+    @params.setter
+    def params(self, p) -> None:
+        p = _f32(p)
+        assert p.size == N_PARAMS
+        _check(self.lib.vx_selector_set_params(self.h, p.ctypes.data_as(_f32p)))
+
+    def gradients(self, X, Y):
+        X, Y = _f32(X), _f32(Y)
+        g = np.empty(N_PARAMS, np.float32)
+        loss = C.c_float()
+        _check(self.lib.vx_selector_gradients(self.h, X.ctypes.data_as(_f32p), Y.ctypes.data_as(_f32p), len(X),
+                                              g.ctypes.data_as(_f32p), C.byref(loss)))
+        return g, loss.value
+
+    def fit(self, X, t_repair, t_full, epochs: int = 300, batch: int = 32, lr: float = 3e-3, seed: int = 7) -> float:
+        """Train on log(us) of both arms, standardised with one shared mean/std."""
+        logs = np.log(np.stack([t_repair, t_full], axis=1))
+        self.mean, self.std = float(logs.mean()), float(logs.std() + 1e-6)
+        Y = _f32((logs - self.mean) / self.std)
+        X = _f32(X)
+        loss = C.c_float()
+        _check(self.lib.vx_selector_train(self.h, X.ctypes.data_as(_f32p), Y.ctypes.data_as(_f32p), len(X), epochs,
+                                          batch, lr, seed, C.byref(loss)))
+        return loss.value
+
+    def predict_log(self, X) -> np.ndarray:
+        X = _f32(X).reshape(-1, N_FEATURES)
+        Y = np.empty((len(X), 2), np.float32)
+        if len(X):
+            _check(self.lib.vx_selector_predict(self.h, X.ctypes.data_as(_f32p), len(X), Y.ctypes.data_as(_f32p)))
+        return Y
+
+    def choose_full(self, X) -> np.ndarray:
+        """(choose_full, ok): full where it is predicted no slower (full wins
+        ties); ok is False where a prediction is not finite, and the caller
+        then falls back to the heuristic."""
+        Y = self.predict_log(X)
+        ok = np.all(np.isfinite(Y), axis=1)
+        return np.where(ok, Y[:, 1] <= Y[:, 0], False), ok
+
+
+class Heuristic:
+    """The reference's adaptive selector (publication_policy_bfs.cpp:163-235)."""
+
+    def __init__(self, vertices: int, initial_reachable_fraction: float, initial_full_us: float):
+        self.lib = _lib()
+        self.h = C.c_void_p()
+        _check(self.lib.vx_heuristic_create(vertices, initial_reachable_fraction, initial_full_us, C.byref(self.h)))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.vx_heuristic_destroy(self.h)
+            self.h = None
+
+    def decide(self, update_fraction: float, shallow_fraction: float) -> bool:
+        out = C.c_int()
+        _check(self.lib.vx_heuristic_decide(self.h, update_fraction, shallow_fraction, C.byref(out)))
+        return bool(out.value)
+
+    def observe(self, full: bool, execution_us: float, affected_fraction: float) -> None:
+        _check(self.lib.vx_heuristic_observe(self.h, int(full), execution_us, affected_fraction))
+
+
+@dataclass
+class RegimeData:
+    name: str
+    vertices: int
+    features: np.ndarray
+    t_repair: np.ndarray  # us
+    t_full: np.ndarray  # us
+    update_fraction: np.ndarray
+    shallow_fraction: np.ndarray
+    affected_fraction: np.ndarray
+    initial_full_us: float
+    initial_reachable_fraction: float
+    exact: bool
+    extra: dict = field(default_factory=dict)
+
+
+def collect(name: str, edges: np.ndarray, vertices: int, root: int, sizes, insert_fraction: float, seed: int,
+            fallback_fraction: float = 2.0, check_every: int = 1) -> RegimeData:
+    """Runs the stream on two replicas (repair arm / full arm) and records
+    features and both arms' GPU times for every batch."""
+    import torch
+
+    lib = _lib()
+    gA, gB = Graph(vertices, False), Graph(vertices, False)
+    gA.bulk_load_edges(edges)
+    gB.bulk_load_edges(edges)
+    # the reference harness disables the internal fallback (fraction 2.0) so
+    # the selector alone owns recomputation (publication_policy_bfs.cpp:59)
+    bA = IncrementalBFS(gA, root, fallback_fraction)
+    bB = IncrementalBFS(gB, root, fallback_fraction)
+    sA = torch.cuda.ExternalStream(gA.stream)
+    sB = torch.cuda.ExternalStream(gB.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(sB)
+    bB.recompute()
+    e1.record(sB)
+    e1.synchronize()
+    initial_full_us = e0.elapsed_time(e1) * 1e3
+    reach0 = bA.reachable_count / max(1, vertices)
+    stream = w.mixed_stream(edges, vertices, sizes, insert_fraction, seed=seed)
+    n = stream.batches
+    feats = np.zeros((n, N_FEATURES), np.float32)
+    t_rep = np.zeros(n)
+    t_full = np.zeros(n)
+    upd = np.zeros(n)
+    shallow = np.zeros(n)
+    aff = np.zeros(n)
+    prev_aff = 0.0
+    exact = True
+    f16 = np.zeros(N_FEATURES, np.float32)
+    for i in range(n):
+        s, d, a = (np.ascontiguousarray(x) for x in stream.batch(i))
+        edges_now = gA.edge_count_directed()
+        upd[i] = len(s) / max(1, edges_now)
+        # features of the staged batch (pre-batch state, identical on both replicas)
+        _check(lib.vx_bfs_stage(C.c_void_p(bA.handle), s.ctypes.data_as(_u32p), d.ctypes.data_as(_u32p),
+                                a.ctypes.data_as(_u8p), len(s)))
+        _check(lib.vx_bfs_staged_features(C.c_void_p(bA.handle), prev_aff, f16.ctypes.data_as(_f32p)))
+        feats[i] = f16
+        if i == 0:
+            shallow[i] = shallow_parent_deletion_fraction(s, d, a, bA.distances_array())
+        # repair arm on A (staging already done; it is common to both arms and
+        # timed separately on B below, so both times include it)
+        torch.cuda.synchronize()
+        e0.record(sB)
+        _check(lib.vx_bfs_stage(C.c_void_p(bB.handle), s.ctypes.data_as(_u32p), d.ctypes.data_as(_u32p),
+                                a.ctypes.data_as(_u8p), len(s)))
+        e1.record(sB)
+        e1.synchronize()
+        t_stage = e0.elapsed_time(e1) * 1e3
+        e0.record(sA)
+        _check(lib.vx_bfs_run_repair(C.c_void_p(bA.handle)))
+        e1.record(sA)
+        e1.synchronize()
+        t_rep[i] = t_stage + e0.elapsed_time(e1) * 1e3
+        e0.record(sB)
+        _check(lib.vx_bfs_run_full(C.c_void_p(bB.handle)))
+        e1.record(sB)
+        e1.synchronize()
+        t_full[i] = t_stage + e0.elapsed_time(e1) * 1e3
+        bA.mark_stale()
+        bB.mark_stale()
+        st = bA.stats()
+        prev_aff = st["last_affected_vertices"] / max(1, vertices)
+        aff[i] = prev_aff
+        if check_every and i % check_every == 0:
+            exact = exact and _same_distances(bA, bB)
+    return RegimeData(name, vertices, feats, t_rep, t_full, upd, shallow, aff, initial_full_us, reach0, exact)
+
+
+def shallow_parent_deletion_fraction(src, dst, add, dist, depth: int = 3) -> float:
+    """Deletions of a shortest-parent arc at depth <= 3, both directions of an
+    undirected graph, over the raw op count (adaptive_policy_bfs.cpp:126-147);
+    the heuristic reads it on the first batch only."""
+    unreachable = np.uint32(0xFFFFFFFF)
+    rm = add == 0
+    u = src[rm].astype(np.int64)
+    v = dst[rm].astype(np.int64)
+    ok = (u < dist.size) & (v < dist.size)
+    du = dist[u[ok]]
+    dv = dist[v[ok]]
+    both = (du != unreachable) & (dv != unreachable)
+    du64, dv64 = du.astype(np.int64), dv.astype(np.int64)
+    fwd = both & (du64 + 1 == dv64) & (dv64 <= depth)
+    bwd = both & (dv64 + 1 == du64) & (du64 <= depth)
+    return float(fwd.sum() + bwd.sum()) / max(1, len(src))
+
+
+class _DeviceU32:
+    """A device array of uint32 seen by torch through __cuda_array_interface__."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i4", "data": (ptr, False), "version": 3,
+                                         "strides": None}
+
+
+def _same_distances(a: IncrementalBFS, b: IncrementalBFS) -> bool:
+    """Bit-for-bit comparison of two BFS distance arrays, on the device."""
+    import torch
+
+    pa, na = a.distances_device_ptr()
+    pb, nb = b.distances_device_ptr()
+    if na != nb:
+        return False
+    if na == 0:
+        return True
+    ta = torch.as_tensor(_DeviceU32(pa, na), device="cuda")
+    tb = torch.as_tensor(_DeviceU32(pb, nb), device="cuda")
+    torch.cuda.synchronize()
+    return bool(torch.equal(ta, tb))
+
+
+def regret(t_chosen, t_repair, t_full):
+    oracle = np.minimum(t_repair, t_full)
+    return np.maximum(0.0, (t_chosen - oracle) / oracle)
+
+
+def evaluate(regimes: list[RegimeData], train_fraction: float = 0.3, seed: int = 1, epochs: int = 300) -> dict:
+    """Trains on the first train_fraction of every regime (pooled) and compares
+    the MLP with the heuristic on the rest."""
+    tr_X, tr_r, tr_f = [], [], []
+    for rg in regimes:
+        k = max(1, int(len(rg.t_repair) * train_fraction))
+        tr_X.append(rg.features[:k])
+        tr_r.append(rg.t_repair[:k])
+        tr_f.append(rg.t_full[:k])
+    mlp = MLPSelector(seed)
+    loss = mlp.fit(np.concatenate(tr_X), np.concatenate(tr_r), np.concatenate(tr_f), epochs=epochs, seed=seed)
+    out = {"train_loss": loss, "regimes": {}}
+    all_m, all_h = [], []
+    wrong_m = wrong_h = total = 0
+    fallbacks = 0
+    for rg in regimes:
+        k = max(1, int(len(rg.t_repair) * train_fraction))
+        X = rg.features[k:]
+        tr, tf = rg.t_repair[k:], rg.t_full[k:]
+        oracle_full = tf <= tr
+        m_full, ok = mlp.choose_full(X)
+        # heuristic replayed online with the measured time of the arm it picks
+        h = Heuristic(rg.vertices, rg.initial_reachable_fraction, rg.initial_full_us)
+        for i in range(k):  # warm its EMA state on the training prefix, as the harness would
+            full = h.decide(rg.update_fraction[i], rg.shallow_fraction[i])
+            h.observe(full, rg.t_full[i] if full else rg.t_repair[i], 0.0 if full else rg.affected_fraction[i])
+        h_full = np.zeros(len(tr), bool)
+        for j in range(len(tr)):
+            i = k + j
+            full = h.decide(rg.update_fraction[i], rg.shallow_fraction[i])
+            h_full[j] = full
+            h.observe(full, tf[j] if full else tr[j], 0.0 if full else rg.affected_fraction[i])
+        # invalid network output falls back to the heuristic's choice
+        m_full = np.where(ok, m_full, h_full)
+        fallbacks += int((~ok).sum())
+        rm = regret(np.where(m_full, tf, tr), tr, tf)
+        rh = regret(np.where(h_full, tf, tr), tr, tf)
+        all_m.append(rm)
+        all_h.append(rh)
+        wrong_m += int((m_full != oracle_full).sum())
+        wrong_h += int((h_full != oracle_full).sum())
+        total += len(tr)
+        out["regimes"][rg.name] = {
+            "batches": len(tr), "mlp_mean_regret": float(rm.mean()), "heuristic_mean_regret": float(rh.mean()),
+            "mlp_wrong_arm": float((m_full != oracle_full).mean()),
+            "heuristic_wrong_arm": float((h_full != oracle_full).mean()),
+            "full_share_oracle": float(oracle_full.mean()), "exact": rg.exact,
+        }
+    cat_m, cat_h = np.concatenate(all_m), np.concatenate(all_h)
+    out["mlp"] = {"equal_regime_mean_regret": float(np.mean([r.mean() for r in all_m])),
+                  "sample_weighted_regret": float(cat_m.mean()), "p95_regret": float(np.percentile(cat_m, 95)),
+                  "max_regret": float(cat_m.max()), "wrong_arm_rate": wrong_m / max(1, total),
+                  "fallbacks": fallbacks}
+    out["heuristic"] = {"equal_regime_mean_regret": float(np.mean([r.mean() for r in all_h])),
+                        "sample_weighted_regret": float(cat_h.mean()), "p95_regret": float(np.percentile(cat_h, 95)),
+                        "max_regret": float(cat_h.max()), "wrong_arm_rate": wrong_h / max(1, total)}
+    out["exact"] = all(r.exact for r in regimes)
+    return out
+
+
+def regime_graphs(scale_rmat: int = 20, er_vertices: int = 1 << 20, grid_side: int = 2048, seed: int = 5):
+    """The three graphs of the selector study: R-MAT, Erdos-Renyi (avg degree
+    16), and a lattice with 0.1% random long-range edges."""
+    rm = w.rmat_edges(scale_rmat, seed=seed)
+    er = w.uniform_edges(er_vertices, er_vertices * 8, seed=seed + 1)
+    gr = w.grid_edges(grid_side, grid_side, 0.001, seed=seed + 2)
+    return [("rmat", rm, 1 << scale_rmat), ("er", er, er_vertices), ("grid", gr, grid_side * grid_side)]
+
+
+def study(batches_per_regime: int = 1111, sizes=(10, 1000, 100000), insert_fraction: float = 0.75,
+          train_fraction: float = 0.3, epochs: int = 300, scale_rmat: int = 20, er_vertices: int = 1 << 20,
+          grid_side: int = 2048, seed: int = 5, log=None) -> dict:
+    """The 9-regime selector study: {R-MAT, Erdos-Renyi, lattice} x batch sizes,
+    both arms timed on every batch, distances compared bit for bit, MLP trained
+    on the first train_fraction of each regime and scored on the rest."""
+    regimes = []
+    for gname, edges, V in regime_graphs(scale_rmat, er_vertices, grid_side, seed):
+        root = w.max_degree_root(edges, V)
+        for k, size in enumerate(sizes):
+            rd = collect(f"{gname}_{size}", edges, V, root, np.full(batches_per_regime, size), insert_fraction,
+                         seed=seed * 100 + k)
+            if log:
+                log(f"{rd.name}: repair median {np.median(rd.t_repair):.1f} us, full median "
+                    f"{np.median(rd.t_full):.1f} us, full wins {np.mean(rd.t_full <= rd.t_repair):.2f}, "
+                    f"exact {rd.exact}")
+            regimes.append(rd)
+    rep = evaluate(regimes, train_fraction=train_fraction, epochs=epochs)
+    rep["config"] = {"batches_per_regime": batches_per_regime, "sizes": list(sizes),
+                     "insert_fraction": insert_fraction, "train_fraction": train_fraction, "epochs": epochs,
+                     "graphs": {"rmat_scale": scale_rmat, "er_vertices": er_vertices, "grid_side": grid_side},
+                     "seed": seed}
+    rep["medians_us"] = {r.name: {"repair": float(np.median(r.t_repair)), "full": float(np.median(r.t_full))}
+                         for r in regimes}
+    return rep
+
+
+if __name__ == "__main__":
+    import argparse
+    import json
+    import sys
+
+    ap = argparse.ArgumentParser(description="selector regret study (both arms timed on the GPU)")
+    ap.add_argument("--batches", type=int, default=1111, help="batches per regime")
+    ap.add_argument("--sizes", type=int, nargs="+", default=[10, 1000, 100000])
+    ap.add_argument("--scale", type=int, default=20)
+    ap.add_argument("--er-vertices", type=int, default=1 << 20)
+    ap.add_argument("--grid-side", type=int, default=2048)
+    ap.add_argument("--epochs", type=int, default=300)
+    ap.add_argument("--out", default=None)
+    a = ap.parse_args()
+    res = study(a.batches, tuple(a.sizes), scale_rmat=a.scale, er_vertices=a.er_vertices, grid_side=a.grid_side,
+                epochs=a.epochs, log=lambda m: print(m, file=sys.stderr, flush=True))
+    text = json.dumps(res, indent=1)
+    if a.out:
+        with open(a.out, "w") as f:
+            f.write(text)
+    print(text)
