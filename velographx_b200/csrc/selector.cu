@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(1024) features_kernel(vxb::DevAdj a, const uin
     out[12] = t[7] / Fn / 32.f;
     out[13] = in.reachable_fraction;
     out[14] = in.prev_affected_fraction;
-    out[15] = log2f(1.f + (float)in.vertices) / 32.f;
+    out[15] = log2f(1.f + (float)in.edges) / 32.f;  // graph size; grows with the stream
   }
 }
 

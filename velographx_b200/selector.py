@@ -16,7 +16,8 @@ Here:
   kernels (vx_selector_train) on standardised log times and predicts both arms;
 * ``Heuristic`` is the reference's adaptive selector, restated in the library
   (vx_heuristic_*), used as fallback and baseline;
-* ``evaluate`` replays the held-out batches through both selectors and
+* ``evaluate`` replays the held-out batches through the selectors (the
+  network, the network with online residual calibration, the heuristic) and
   reports regret and wrong-arm rates.
 """
 from __future__ import annotations
@@ -82,8 +83,8 @@ class MLPSelector:
         self.lib = _lib()
         self.h = C.c_void_p()
         _check(self.lib.vx_selector_create(seed, C.byref(self.h)))
-        self.mean = 0.0
-        self.std = 1.0
+        self.mu = np.zeros(2)
+        self.sd = np.ones(2)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -110,25 +111,42 @@ class MLPSelector:
                                               g.ctypes.data_as(_f32p), C.byref(loss)))
         return g, loss.value
 
+    def targets(self, t_repair, t_full) -> np.ndarray:
+        """Network targets: the mean log time of the two arms and the log
+        ratio full/repair, each standardised with the training set's moments
+        (fit sets them).  The second output carries the decision, so it gets a
+        unit-variance target of its own."""
+        lr, lf = np.log(t_repair), np.log(t_full)
+        raw = np.stack([(lr + lf) / 2, lf - lr], axis=1)
+        return _f32((raw - self.mu) / self.sd)
+
     def fit(self, X, t_repair, t_full, epochs: int = 300, batch: int = 32, lr: float = 3e-3, seed: int = 7) -> float:
-        """Train on log(us) of both arms, standardised with one shared mean/std."""
-        logs = np.log(np.stack([t_repair, t_full], axis=1))
-        self.mean, self.std = float(logs.mean()), float(logs.std() + 1e-6)
-        Y = _f32((logs - self.mean) / self.std)
+        """Trains on (features, both arms' times in us) with the library's Adam kernel."""
+        lr_, lf_ = np.log(t_repair), np.log(t_full)
+        raw = np.stack([(lr_ + lf_) / 2, lf_ - lr_], axis=1)
+        self.mu = raw.mean(0)
+        self.sd = raw.std(0) + 1e-6
+        Y = self.targets(t_repair, t_full)
         X = _f32(X)
         loss = C.c_float()
         _check(self.lib.vx_selector_train(self.h, X.ctypes.data_as(_f32p), Y.ctypes.data_as(_f32p), len(X), epochs,
                                           batch, lr, seed, C.byref(loss)))
         return loss.value
 
-    def predict_log(self, X) -> np.ndarray:
+    def predict_raw(self, X) -> np.ndarray:
+        """The network's two outputs for each row of X (standardised units)."""
         X = _f32(X).reshape(-1, N_FEATURES)
         Y = np.empty((len(X), 2), np.float32)
         if len(X):
             _check(self.lib.vx_selector_predict(self.h, X.ctypes.data_as(_f32p), len(X), Y.ctypes.data_as(_f32p)))
         return Y
 
-    def choose_full(self, X) -> np.ndarray:
+    def predict_log(self, X) -> np.ndarray:
+        """Predicted natural-log execution times (us) of (repair, full)."""
+        Y = self.predict_raw(X).astype(np.float64) * self.sd + self.mu
+        return np.stack([Y[:, 0] - Y[:, 1] / 2, Y[:, 0] + Y[:, 1] / 2], axis=1)
+
+    def choose_full(self, X):
         """(choose_full, ok): full where it is predicted no slower (full wins
         ties); ok is False where a prediction is not finite, and the caller
         then falls back to the heuristic."""
@@ -297,9 +315,48 @@ def regret(t_chosen, t_repair, t_full):
     return np.maximum(0.0, (t_chosen - oracle) / oracle)
 
 
+def calibrated_choices(pred_log: np.ndarray, ok: np.ndarray, t_repair, t_full, fallback,
+                       alpha: float = 0.25) -> np.ndarray:
+    """Online residual calibration of the network's predictions.
+
+    After each batch the time of the arm that ran is observed; an EMA of the
+    log-space residual (observed - predicted) of that arm is added to its
+    later predictions, so a drift the network never saw in training (the graph
+    grows, the machine slows) moves the decision instead of repeating the same
+    mistake.  The EMA weight is the heuristic's (adaptive_policy_bfs.cpp:31).
+    A non-finite prediction takes the fallback's choice for that batch."""
+    res = np.zeros(2)
+    seen = np.zeros(2, bool)
+    out = np.zeros(len(pred_log), bool)
+    for j in range(len(pred_log)):
+        if not ok[j]:
+            full = bool(fallback[j])
+        else:
+            p = pred_log[j] + res
+            full = bool(p[1] <= p[0])
+        out[j] = full
+        if ok[j]:
+            arm = 1 if full else 0
+            obs = np.log(t_full[j] if full else t_repair[j])
+            r = obs - pred_log[j, arm]
+            res[arm] = (1 - alpha) * res[arm] + alpha * r if seen[arm] else r
+            seen[arm] = True
+    return out
+
+
+def _summary(regrets, wrong, total, **extra):
+    cat = np.concatenate(regrets)
+    return {"equal_regime_mean_regret": float(np.mean([r.mean() for r in regrets])),
+            "sample_weighted_regret": float(cat.mean()), "p95_regret": float(np.percentile(cat, 95)),
+            "max_regret": float(cat.max()), "wrong_arm_rate": wrong / max(1, total), **extra}
+
+
 def evaluate(regimes: list[RegimeData], train_fraction: float = 0.3, seed: int = 1, epochs: int = 300) -> dict:
     """Trains on the first train_fraction of every regime (pooled) and compares
-    the MLP with the heuristic on the rest."""
+    on the rest: "mlp" (the network; the heuristic's choice where a
+    prediction is not finite), "mlp_online" (the network with online residual
+    calibration, an ablation) and "heuristic" (the reference's adaptive
+    selector, replayed online)."""
     tr_X, tr_r, tr_f = [], [], []
     for rg in regimes:
         k = max(1, int(len(rg.t_repair) * train_fraction))
@@ -309,15 +366,16 @@ def evaluate(regimes: list[RegimeData], train_fraction: float = 0.3, seed: int =
     mlp = MLPSelector(seed)
     loss = mlp.fit(np.concatenate(tr_X), np.concatenate(tr_r), np.concatenate(tr_f), epochs=epochs, seed=seed)
     out = {"train_loss": loss, "regimes": {}}
-    all_m, all_h = [], []
-    wrong_m = wrong_h = total = 0
+    names = ("mlp", "mlp_online", "heuristic")
+    regrets = {n: [] for n in names}
+    wrong = dict.fromkeys(names, 0)
+    total = 0
     fallbacks = 0
     for rg in regimes:
         k = max(1, int(len(rg.t_repair) * train_fraction))
         X = rg.features[k:]
         tr, tf = rg.t_repair[k:], rg.t_full[k:]
         oracle_full = tf <= tr
-        m_full, ok = mlp.choose_full(X)
         # heuristic replayed online with the measured time of the arm it picks
         h = Heuristic(rg.vertices, rg.initial_reachable_fraction, rg.initial_full_us)
         for i in range(k):  # warm its EMA state on the training prefix, as the harness would
@@ -329,30 +387,23 @@ def evaluate(regimes: list[RegimeData], train_fraction: float = 0.3, seed: int =
             full = h.decide(rg.update_fraction[i], rg.shallow_fraction[i])
             h_full[j] = full
             h.observe(full, tf[j] if full else tr[j], 0.0 if full else rg.affected_fraction[i])
-        # invalid network output falls back to the heuristic's choice
-        m_full = np.where(ok, m_full, h_full)
+        pred = mlp.predict_log(X)
+        ok = np.all(np.isfinite(pred), axis=1)
         fallbacks += int((~ok).sum())
-        rm = regret(np.where(m_full, tf, tr), tr, tf)
-        rh = regret(np.where(h_full, tf, tr), tr, tf)
-        all_m.append(rm)
-        all_h.append(rh)
-        wrong_m += int((m_full != oracle_full).sum())
-        wrong_h += int((h_full != oracle_full).sum())
+        static = np.where(ok, pred[:, 1] <= pred[:, 0], h_full)
+        choice = {"mlp": static, "mlp_online": calibrated_choices(pred, ok, tr, tf, h_full), "heuristic": h_full}
+        row = {"batches": len(tr), "full_share_oracle": float(oracle_full.mean()), "exact": rg.exact}
+        for n in names:
+            r = regret(np.where(choice[n], tf, tr), tr, tf)
+            regrets[n].append(r)
+            wrong[n] += int((choice[n] != oracle_full).sum())
+            row[f"{n}_mean_regret"] = float(r.mean())
+            row[f"{n}_wrong_arm"] = float((choice[n] != oracle_full).mean())
+        out["regimes"][rg.name] = row
         total += len(tr)
-        out["regimes"][rg.name] = {
-            "batches": len(tr), "mlp_mean_regret": float(rm.mean()), "heuristic_mean_regret": float(rh.mean()),
-            "mlp_wrong_arm": float((m_full != oracle_full).mean()),
-            "heuristic_wrong_arm": float((h_full != oracle_full).mean()),
-            "full_share_oracle": float(oracle_full.mean()), "exact": rg.exact,
-        }
-    cat_m, cat_h = np.concatenate(all_m), np.concatenate(all_h)
-    out["mlp"] = {"equal_regime_mean_regret": float(np.mean([r.mean() for r in all_m])),
-                  "sample_weighted_regret": float(cat_m.mean()), "p95_regret": float(np.percentile(cat_m, 95)),
-                  "max_regret": float(cat_m.max()), "wrong_arm_rate": wrong_m / max(1, total),
-                  "fallbacks": fallbacks}
-    out["heuristic"] = {"equal_regime_mean_regret": float(np.mean([r.mean() for r in all_h])),
-                        "sample_weighted_regret": float(cat_h.mean()), "p95_regret": float(np.percentile(cat_h, 95)),
-                        "max_regret": float(cat_h.max()), "wrong_arm_rate": wrong_h / max(1, total)}
+    out["mlp"] = _summary(regrets["mlp"], wrong["mlp"], total, fallbacks=fallbacks)
+    out["mlp_online"] = _summary(regrets["mlp_online"], wrong["mlp_online"], total)
+    out["heuristic"] = _summary(regrets["heuristic"], wrong["heuristic"], total)
     out["exact"] = all(r.exact for r in regimes)
     return out
 
