@@ -504,6 +504,65 @@ struct TouchChildren {
   }
 };
 
+// ------------------------------------------------ long rows of the repair --
+// A repair frontier is small, so a hub in it would leave one warp walking
+// tens of thousands of arcs while the rest of the grid waits at the next
+// barrier.  The warp passes therefore defer rows of at least large_row arcs
+// to a list, and the whole grid walks those rows after the barrier.
+
+__device__ __forceinline__ bool defer_row(const Params& p, const DevAdj& a, uint32_t v) {
+  return degree_of(a, v) >= p.large_row;
+}
+
+// Lane form for expand_lanes callers: a lane whose row is long appends its
+// vertex to p.big and hands expand_lanes an empty range instead.
+__device__ __forceinline__ void defer_lanes(const Params& p, uint32_t* cnt, bool act, uint32_t u, uint64_t& b,
+                                            uint64_t& e, uint2& dr) {
+  const bool big = act && (e - b) + dr.y >= p.large_row;
+  const uint32_t slot = vxb::warp_append(big, cnt);
+  if (big) {
+    p.big[slot] = u;
+    b = e = 0;
+    dr = make_uint2(0, 0);
+  }
+}
+
+// Surviving-parent test of the deferred vertices p.big[0, nb): every warp scans
+// a 32-arc slice of the row per step; found[r] (p.tent, zeroed by the warp
+// pass) is set by the first warp that sees a surviving parent, and the others
+// stop at their next step.
+__device__ void grid_parent_probe(const Params& p, uint32_t nb, uint32_t d) {
+  const DevAdj& a = p.g.in;
+  const int lane = threadIdx.x & 31;
+  for (uint32_t r = 0; r < nb; ++r) {
+    const uint32_t v = p.big[r];
+    uint64_t b, e;
+    vxb::base_range(a, v, b, e);
+    const uint2 dr = a.drow[v];
+    const uint64_t nbase = e - b, total = nbase + dr.y;
+    for (uint64_t k0 = (uint64_t)gwarp() * 32; k0 < total; k0 += (uint64_t)nwarps() * 32) {
+      if (ld_cg(&p.tent[r])) break;  // one load for the warp: the break is warp-uniform
+      const uint64_t k = k0 + lane;
+      bool ok = false;
+      if (k < total) {
+        uint32_t x;
+        bool valid = true;
+        if (k < nbase) {
+          x = a.col[b + k];
+          valid = !(x & kTomb);
+        } else {
+          x = a.darena[dr.x + (uint32_t)(k - nbase)];
+        }
+        ok = valid && x < p.dist_len && p.dist[x] + 1 == d && !test_bit(p.aff, x);
+      }
+      if (__any_sync(FULL, ok)) {
+        if (lane == 0) atomicExch(&p.tent[r], 1u);
+        break;
+      }
+    }
+  }
+}
+
 // --------------------------------------------------- pre-batch fixpoint --
 
 // compute_affected_prebatch (bfs.hpp:222-259) level by level: at distance d
@@ -529,6 +588,8 @@ __device__ void repair_pre(const Params& p) {
     for (int k = 0; k < 3; ++k) {
       c->list_n[k] = 0;
       c->next_seed[k] = kUnreachable;
+      c->big_n[k] = 0;
+      c->big_t[k] = 0;
     }
     c->seed_min = kUnreachable;
   }
@@ -559,13 +620,31 @@ __device__ void repair_pre(const Params& p) {
     if (gtid() == 0) {
       c->list_n[k2] = 0;
       c->next_seed[k2] = kUnreachable;
+      c->big_n[k2] = 0;
+      c->big_t[k2] = 0;
     }
-    // every touched vertex at distance d: one warp each
+    // every touched vertex at distance d: one warp each, long rows deferred
     for (uint32_t i = gwarp(); i < np; i += nwarps()) {
       const uint32_t v = p.q[k][i];
+      if (defer_row(p, p.g.in, v)) {
+        if (lane == 0) {
+          const uint32_t slot = atomicAdd(&c->big_n[k], 1u);
+          p.big[slot] = v;
+          p.tent[slot] = 0u;
+        }
+        continue;
+      }
       if (!warp_has_surviving_parent(p, v, d) && lane == 0) mark_affected(p, v);
     }
     if (!sync_grid(p)) return;
+    const uint32_t nbp = ld_cg(&c->big_n[k]);
+    if (nbp) {
+      grid_parent_probe(p, nbp, d);
+      if (!sync_grid(p)) return;
+      for (uint32_t r = gtid(); r < nbp; r += nthreads())
+        if (!ld_cg(&p.tent[r])) mark_affected(p, p.big[r]);
+      if (!sync_grid(p)) return;
+    }
     const uint32_t a_tot = ld_cg(&c->a_n);
     if (a_tot > p.fallback_limit) {
       if (gtid() == 0) c->fallback = 1;
@@ -574,7 +653,14 @@ __device__ void repair_pre(const Params& p) {
     // next level's list: children of the vertices affected at d, candidates
     // at d+1; the nearest deeper candidate level for a jump
     TouchChildren tc{&p, d, p.q[k1], &c->list_n[k1]};
-    for (uint32_t i = a_prev + gwarp(); i < a_tot; i += nwarps()) warp_row(p.g.out, p.lst_a[i], tc);
+    for (uint32_t i = a_prev + gwarp(); i < a_tot; i += nwarps()) {
+      const uint32_t v = p.lst_a[i];
+      if (defer_row(p, p.g.out, v)) {
+        if (lane == 0) p.big[atomicAdd(&c->big_t[k], 1u)] = v;
+        continue;
+      }
+      warp_row(p.g.out, v, tc);
+    }
     for (uint32_t i = gtid(); i < ncand; i += nthreads()) {
       const uint32_t v = p.lst_t[i];
       const uint32_t dv = p.dist[v];
@@ -582,6 +668,11 @@ __device__ void repair_pre(const Params& p) {
       else if (dv != kUnreachable && dv > d + 1) atomicMin(&c->next_seed[k1], dv);
     }
     if (!sync_grid(p)) return;
+    const uint32_t nbt = ld_cg(&c->big_t[k]);
+    if (nbt) {
+      grid_rows(p.g.out, p.big, nbt, tc);
+      if (!sync_grid(p)) return;
+    }
     a_prev = a_tot;
     const uint32_t nn = ld_cg(&c->list_n[k1]);
     if (nn > 0) {
@@ -681,6 +772,34 @@ struct BoundaryMin {
   }
 };
 
+// Boundary distance of the deferred affected entries p.big[0, nb) (indices
+// into lst_a): each warp folds its slices into p.tent[i] by atomicMin.
+__device__ void grid_boundary_min(const Params& p, uint32_t nb) {
+  const DevAdj& a = p.g.in;
+  for (uint32_t r = 0; r < nb; ++r) {
+    const uint32_t i = p.big[r];
+    const uint32_t v = p.lst_a[i];
+    BoundaryMin bm{&p, kUnreachable};
+    uint64_t b, e;
+    vxb::base_range(a, v, b, e);
+    for (uint64_t j0 = b + (uint64_t)gwarp() * 32; j0 < e; j0 += (uint64_t)nwarps() * 32) {
+      const uint64_t j = j0 + (threadIdx.x & 31);
+      const uint32_t x = j < e ? a.col[j] : kTomb;
+      bm(!(x & kTomb), x & kIdMask, v);
+    }
+    const uint2 dr = a.drow[v];
+    for (uint32_t j0 = dr.x + gwarp() * 32; j0 < dr.x + dr.y; j0 += nwarps() * 32) {
+      const uint32_t j = j0 + (threadIdx.x & 31);
+      const bool ok = j < dr.x + dr.y;
+      bm(ok, ok ? a.darena[j] : 0u, v);
+    }
+    uint32_t best = bm.best;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(FULL, best, o));
+    if ((threadIdx.x & 31) == 0 && best != kUnreachable) atomicMin(&p.tent[i], best);
+  }
+}
+
 __device__ void repair_post(const Params& p) {
   BfsCounters* c = p.c;
   const int lane = threadIdx.x & 31;
@@ -705,12 +824,21 @@ __device__ void repair_post(const Params& p) {
       for (int k = 0; k < 3; ++k) {
         c->list_n[k] = 0;
         c->next_seed[k] = kUnreachable;
+        c->big_n[k] = 0;
+        c->big_t[k] = 0;
       }
     }
     if (!sync_grid(p)) return;
-    // boundary seeds, one warp per affected vertex
+    // boundary seeds, one warp per affected vertex, long in-rows deferred
     for (uint32_t i = gwarp(); i < na; i += nwarps()) {
       const uint32_t v = p.lst_a[i];
+      if (defer_row(p, p.g.in, v)) {
+        if (lane == 0) {
+          p.tent[i] = kUnreachable;
+          p.big[atomicAdd(&c->big_t[0], 1u)] = i;
+        }
+        continue;
+      }
       BoundaryMin bm{&p, kUnreachable};
       warp_row(p.g.in, v, bm);
       uint32_t best = bm.best;
@@ -726,6 +854,21 @@ __device__ void repair_post(const Params& p) {
       }
     }
     if (!sync_grid(p)) return;
+    const uint32_t nbb = ld_cg(&c->big_t[0]);
+    if (nbb) {
+      grid_boundary_min(p, nbb);
+      if (!sync_grid(p)) return;
+      for (uint32_t r = gtid(); r < nbb; r += nthreads()) {
+        const uint32_t i = p.big[r];
+        const uint32_t best = ld_cg(&p.tent[i]);
+        p.dist[p.lst_a[i]] = best;
+        if (best != kUnreachable) {
+          ++reach;
+          atomicMin(&c->seed_min, best);
+        }
+      }
+      if (!sync_grid(p)) return;
+    }
     // bucketed settle among affected vertices (unit-weight Dijkstra)
     uint32_t lvl = ld_cg(&c->seed_min);
     if (lvl != kUnreachable) {
@@ -740,6 +883,7 @@ __device__ void repair_post(const Params& p) {
         if (gtid() == 0) {
           c->list_n[k2] = 0;
           c->next_seed[k2] = kUnreachable;
+          c->big_n[k2] = 0;
         }
         SettleVisit sv{&p, lvl, p.q[k1], &c->list_n[k1], &reach};
         // items: seeds whose boundary distance is lvl and still hold it, then
@@ -764,9 +908,15 @@ __device__ void repair_post(const Params& p) {
             vxb::base_range(a, u, b, e);
             dr = a.drow[u];
           }
+          defer_lanes(p, &c->big_n[k], act, u, b, e, dr);
           expand_lanes(a, u, b, e, dr, sv);
         }
         if (!sync_grid(p)) return;
+        const uint32_t nbs = ld_cg(&c->big_n[k]);
+        if (nbs) {
+          grid_rows(a, p.big, nbs, sv);
+          if (!sync_grid(p)) return;
+        }
         const uint32_t nn = ld_cg(&c->list_n[k1]), ns = ld_cg(&c->next_seed[k1]);
         if (nn > 0) ++lvl;
         else if (ns != kUnreachable) lvl = ns;
@@ -778,7 +928,10 @@ __device__ void repair_post(const Params& p) {
   // affected vertices that ended below their old distance and the heads of
   // inserted arcs that relax
   if (gtid() == 0) {
-    for (int k = 0; k < 3; ++k) c->list_n[k] = 0;
+    for (int k = 0; k < 3; ++k) {
+      c->list_n[k] = 0;
+      c->big_n[k] = 0;
+    }
   }
   if (!sync_grid(p)) return;
   for (uint32_t i = gtid(); i < na; i += nthreads()) {
@@ -808,7 +961,10 @@ __device__ void repair_post(const Params& p) {
     const int k = r % 3, k1 = (r + 1) % 3, k2 = (r + 2) % 3;
     const uint32_t n = ld_cg(&c->list_n[k]);
     if (n == 0) break;
-    if (gtid() == 0) c->list_n[k2] = 0;
+    if (gtid() == 0) {
+      c->list_n[k2] = 0;
+      c->big_n[k2] = 0;
+    }
     uint32_t* inq_cur = p.inq[r & 1];
     PropVisit pv{&p, p.inq[(r + 1) & 1], p.q[k1], &c->list_n[k1], &reach};
     for (uint32_t base = gwarp() * 32; base < n; base += nwarps() * 32) {
@@ -822,9 +978,15 @@ __device__ void repair_post(const Params& p) {
         vxb::base_range(a, u, b, e);
         dr = a.drow[u];
       }
+      defer_lanes(p, &c->big_n[k], act, u, b, e, dr);
       expand_lanes(a, u, b, e, dr, pv);
     }
     if (!sync_grid(p)) return;
+    const uint32_t nbq = ld_cg(&c->big_n[k]);
+    if (nbq) {
+      grid_rows(a, p.big, nbq, pv);
+      if (!sync_grid(p)) return;
+    }
   }
   reach = vxb::warp_sum(reach);
   if (lane == 0) reach_add(p, reach);

@@ -30,6 +30,10 @@ struct BfsCounters {
   uint32_t next_seed[3]; // smallest pending seed level (rotating)
   uint32_t seed_min;     // smallest seed level of the settle phase
   unsigned long long scratch64;  // single-value readbacks
+  // rows of at least large_row arcs met by the repair loops, deferred to a
+  // pass of the whole grid (two rotating triples: a loop step has two phases)
+  uint32_t big_n[3];
+  uint32_t big_t[3];
 };
 
 struct BfsTuning {
