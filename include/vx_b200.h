@@ -122,6 +122,15 @@ int vx_bfs_reached_arcs(vx_bfs* b, uint64_t* out);
  * frontier size | bottom_up << 63}, then a closing timestamp; *n = entries.
  * No reference counterpart (diagnostics). */
 int vx_bfs_level_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
+/* Phase trace of the last incremental apply (21 entries): globaltimer ns at
+ * the pre-batch kernel's entry, after its seeds, after its cascade; at the
+ * post-batch kernel's entry, after the boundary distances, after its seeds,
+ * after the relaxation (0 = phase not run); the work items pushed by the
+ * cascade and by the relaxation; then, for the cascade and the relaxation,
+ * the work-ring processing rounds, tickets, idle rounds, termination checks,
+ * SM cycles spent processing (summed over blocks) and the longest round.
+ * No reference counterpart (diagnostics). */
+int vx_bfs_phase_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
 /* Direction switch (alpha, beta) and grid-expanded row length of the full BFS.
  * No reference counterpart: the reference BFS is top-down only. */
 int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row);

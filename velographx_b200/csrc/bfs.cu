@@ -12,12 +12,12 @@
 //              the frontier bitmap.  Claims are atomicOr on the visited bitmap,
 //              frontier queues are appended with warp-aggregated atomics.
 //   kModePre   the pre-batch part of apply (bfs.hpp:38-70, 222-259): deletion
-//              candidates and the support-count fixpoint, level by level in
-//              ascending distance order.
+//              candidates and the support-count fixpoint, run as one
+//              asynchronous cascade over a work ring (no barrier per level).
 //   kModePost  the post-batch part (bfs.hpp:72-97, 261-354): either the
-//              fallback full BFS, or invalidate / boundary seed / bucketed
-//              settle of the affected vertices followed by insertion relax and
-//              decrease propagation.
+//              fallback full BFS, or invalidation and boundary distances of
+//              the affected vertices, then one asynchronous label-correcting
+//              relaxation from them and from the heads of inserted arcs.
 #include <algorithm>
 #include <cstring>
 
@@ -50,9 +50,14 @@ struct Params {
   uint32_t* big;
   uint32_t* lst_a;
   uint32_t* lst_t;
-  uint32_t* old;
   uint32_t* tent;
-  uint32_t* lost;
+  unsigned long long* sw;  // support words of the pre-batch cascade (zero between batches)
+  unsigned long long* ring;  // work ring of the repair phases (kSent between phases)
+  uint32_t ring_mask;
+  uint32_t* rq_head;       // ring counters, each on its own 128-byte line: the
+  uint32_t* rq_tail;       // idle blocks poll them while the working ones push
+  uint32_t* rq_done;
+  unsigned long long* rq_stat;  // drain statistics of the last phase (own line)
   uint32_t* aff;
   uint32_t* inq[2];
   const uint32_t* fu;
@@ -338,9 +343,7 @@ __device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, u
 
 // ------------------------------------------------------------ full BFS --
 
-__device__ void full_bfs(const Params& p) {
-  __shared__ BlockQueue bq;
-  __shared__ LbStage lbst;
+__device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
   BfsCounters* c = p.c;
   if (threadIdx.x == 0) bq.cnt = 0;
   const uint32_t V = p.V;
@@ -450,553 +453,698 @@ __device__ __forceinline__ bool is_sp(const Params& p, uint32_t u, uint32_t v) {
   return du != kUnreachable && dv != kUnreachable && du + 1 == dv;
 }
 
-// Does v (at distance d >= 1) keep a shortest parent: an in-neighbour x at
-// distance d-1 that is not affected, in the pre-batch graph minus the batch's
-// deletions (already committed)?  Whole warp, stops at the first such parent.
-// "v has none" is exactly the reference's lost >= support test
-// (bfs.hpp:229-240): lost counts every shortest parent that is deleted or
-// affected, each once, and support counts all of them.
-__device__ bool warp_has_surviving_parent(const Params& p, uint32_t v, uint32_t d) {
-  const DevAdj& a = p.g.in;
-  const int lane = threadIdx.x & 31;
-  uint64_t b, e;
-  vxb::base_range(a, v, b, e);
-  const uint2 dr = a.drow[v];
-  const uint64_t nb = e - b, total = nb + dr.y;
-  for (uint64_t k0 = 0; k0 < total; k0 += 32) {
-    const uint64_t k = k0 + lane;
-    bool ok = false;
-    if (k < total) {
-      uint32_t x;
-      bool valid = true;
-      if (k < nb) {
-        x = a.col[b + k];
-        valid = !(x & kTomb);
-      } else {
-        x = a.darena[dr.x + (uint32_t)(k - nb)];
-      }
-      ok = valid && x < p.dist_len && p.dist[x] + 1 == d && !test_bit(p.aff, x);
+__device__ __forceinline__ void reach_add(const Params& p, long long d) {
+  if (d) atomicAdd(&p.c->reachable, (unsigned long long)d);
+}
+
+// ------------------------------------------------- asynchronous work ring --
+// The repair phases are dependency chains a few vertices wide and as deep as
+// the tree below a deletion or an insertion.  Level-synchronous rounds would
+// pay a grid barrier per level; instead each phase drains a work ring: blocks
+// claim items, expand their rows, and push the vertices they change, with no
+// barrier until the ring is empty.
+//
+// The ring holds 64-bit items (kSent = empty slot) at slot[i & ring_mask]:
+// bits 0-30 a vertex, bit 31 the cascade's expand kind, bits 32-62 the chunk
+// of the vertex's row the item covers (rows longer than kChunk arcs are split
+// by the block that claims their first chunk, so a hub is spread over
+// blocks), bit 63 the cascade's chunk-check kind;
+// head / tail / done count claimed, pushed and finished items.  A block ends
+// the phase once it sees done == tail (read in that order): every push happens
+// while its pusher's item is unfinished, so at that moment nothing is in
+// flight.  Every wait is bounded and records kErrDrainTimeout when it gives up.
+
+constexpr unsigned long long kSent = ~0ull;
+constexpr uint32_t kChunk = 128;  // arcs of one ring item: a 32-item round stays within 4096 arcs
+
+// Bit test through L2: bits another block sets during a phase.
+__device__ __forceinline__ bool test_bit_cg(const uint32_t* bm, uint32_t v) {
+  return (__ldcg(&bm[v >> 5]) >> (v & 31)) & 1u;
+}
+constexpr uint32_t kKindBit = 0x80000000u;  // cascade items: set = expand an affected vertex
+constexpr unsigned long long kChunkCheckBit = 1ull << 63;  // cascade items: one chunk of a long check
+constexpr uint32_t kDrainIdleLimit = 1u << 20;  // idle rounds of a block (up to 2 us each)
+
+__device__ __forceinline__ void ring_push(const Params& p, bool pred, unsigned long long item) {
+  const uint32_t s = vxb::warp_append(pred, p.rq_tail);  // warp-uniform
+  if (pred) __stcg(&p.ring[s & p.ring_mask], item);
+}
+
+__device__ __forceinline__ uint32_t item_vertex(unsigned long long it) { return (uint32_t)it & ~kKindBit; }
+__device__ __forceinline__ uint32_t item_chunk(unsigned long long it) { return (uint32_t)(it >> 32) & 0x7FFFFFFFu; }
+
+// Stages the rows of n <= kThreads items (one per thread; kSent items have no
+// row) with their degree prefix in shared memory, then every warp of the block
+// takes 32 consecutive arcs of the flattened range per step, so one long row
+// is spread over the whole block.  f(valid, x, j) gets the owning item's index
+// and is called warp-uniformly.  With 64-bit ring items (p non-null) an item
+// covers one kChunk-arc chunk of its row, and the claimer of a row's first
+// chunk pushes the rest as items of their own.
+template <class T, class F>
+__device__ void block_rows(const DevAdj& a, const T* items, uint32_t n, LbStage& st, F& f,
+                           const Params* p = nullptr) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ uint32_t wsum[kThreads / 32];
+  uint32_t len = 0;
+  if (threadIdx.x < n) {
+    const T it = items[threadIdx.x];
+    uint64_t b = 0, e = 0;
+    uint2 dr = make_uint2(0, 0);
+    if (it != (T)kSent) {
+      const uint32_t u = (uint32_t)it & ~kKindBit;
+      vxb::base_range(a, u, b, e);
+      dr = a.drow[u];
     }
-    if (__any_sync(FULL, ok)) return true;
+    uint32_t blen = (uint32_t)(e - b), dx = dr.x, dlen = dr.y;
+    if (p && it != (T)kSent) {
+      const uint32_t total = blen + dlen, c = (uint32_t)((unsigned long long)it >> 32) & 0x7FFFFFFFu;
+      const uint32_t lo = c * kChunk, hi = min(total, lo + kChunk);
+      if (c == 0 && total > kChunk) {  // hand the other chunks to other blocks
+        const uint32_t more = (total - 1) / kChunk;
+        const uint32_t s0 = atomicAdd(p->rq_tail, more);
+        for (uint32_t k = 0; k < more; ++k)
+          __stcg(&p->ring[(s0 + k) & p->ring_mask], ((unsigned long long)it & 0xFFFFFFFFull) |
+                                                        ((unsigned long long)(k + 1) << 32));
+      }
+      const uint32_t bl = lo < blen ? min(blen, hi) - lo : 0u;
+      const uint32_t dl = hi > max(lo, blen) ? hi - max(lo, blen) : 0u;
+      b += lo < blen ? lo : blen;
+      dx += lo > blen ? lo - blen : 0u;
+      blen = bl;
+      dlen = dl;
+    }
+    st.base[threadIdx.x] = b;
+    st.blen[threadIdx.x] = blen;
+    st.dx[threadIdx.x] = dx;
+    len = blen + dlen;
   }
-  return false;
+  uint32_t incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(FULL, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t w = lane < kThreads / 32 ? wsum[lane] : 0u;
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (lane < kThreads / 32) wsum[lane] = wi - w;
+  }
+  __syncthreads();
+  const uint32_t ex = wsum[warp] + incl - len;
+  if (threadIdx.x < n) st.pref[threadIdx.x] = ex;
+  if (threadIdx.x + 1 == n) st.pref[n] = ex + len;
+  __syncthreads();
+  const uint32_t M = n ? st.pref[n] : 0u;
+  for (uint32_t e0 = (uint32_t)warp * 32; e0 < M; e0 += kThreads) {
+    const uint32_t e = e0 + lane;
+    bool valid = false;
+    uint32_t x = 0, j = 0;
+    if (e < M) {
+      uint32_t lo = 0, hi = n;  // last j with pref[j] <= e
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (st.pref[mid] <= e) lo = mid;
+        else hi = mid;
+      }
+      j = lo;
+      const uint32_t k = e - st.pref[j];
+      if (k < st.blen[j]) {
+        x = a.col[st.base[j] + k];
+        valid = !(x & kTomb);
+        x &= kIdMask;
+      } else {
+        x = a.darena[st.dx[j] + (k - st.blen[j])];
+        valid = true;
+      }
+    }
+    f(valid, x, j);
+  }
+  __syncthreads();  // st is reused by the next call
 }
 
-__device__ __forceinline__ void mark_affected(const Params& p, uint32_t v) {
-  atomicOr(&p.aff[v >> 5], 1u << (v & 31));
-  const uint32_t slot = atomicAdd(&p.c->a_n, 1u);
-  p.lst_a[slot] = v;
-}
-
-// Children one level deeper of a newly affected vertex become touched.
-struct TouchChildren {
-  const Params* p;
-  uint32_t d;
-  uint32_t* plist;
-  uint32_t* pcount;
-  __device__ __forceinline__ void operator()(bool valid, uint32_t x, uint32_t) {
-    bool fresh = false;
-    if (valid && x < p->dist_len && p->dist[x] == d + 1) fresh = atomicOr(&p->lost[x], 1u) == 0u;
-    const uint32_t s1 = vxb::warp_append(fresh, pcount);
-    if (fresh) plist[s1] = x;
-    const uint32_t s2 = vxb::warp_append(fresh, &p->c->touched_n);
-    if (fresh) p->lst_t[s2] = x;
-  }
+// Shared memory of one block for the repair phases.
+struct RepairSmem {
+  unsigned long long items[kThreads];  // claimed ring items
+  uint32_t sv[kThreads];     // check items (vertex); boundary chunk vertices
+  unsigned long long ex[kThreads];     // expand items (vertex, chunk)
+  uint32_t cnt[kThreads];    // chunk + 1 of a chunk-check sv item (0: plain check); boundary minima
+  uint32_t d[kThreads];      // distance of each staged item
+  uint32_t g0, n, stop, nsv, nex, fallback;
 };
 
-// ------------------------------------------------ long rows of the repair --
-// A repair frontier is small, so a hub in it would leave one warp walking
-// tens of thousands of arcs while the rest of the grid waits at the next
-// barrier.  The warp passes therefore defer rows of at least large_row arcs
-// to a list, and the whole grid walks those rows after the barrier.
+// Drains the ring; W::process(sm, n) handles sm.items[0, n) block-uniformly.
+//
+// A block takes a ticket of kClaim consecutive ring indices (one atomicAdd,
+// which never fails) and warp 0 polls the ticket's own slots: items pushed
+// into them are processed as they arrive, and the next ticket is taken once
+// the current one is used up.  Indices past the tail belong to whichever
+// block holds them, so pushes spread over the blocks waiting for work, and no
+// two blocks poll the same address.  Every few idle rounds a block checks
+// done == tail and leaves the phase.
+constexpr uint32_t kClaim = 32;
 
-__device__ __forceinline__ bool defer_row(const Params& p, const DevAdj& a, uint32_t v) {
-  return degree_of(a, v) >= p.large_row;
-}
-
-// Lane form for expand_lanes callers: a lane whose row is long appends its
-// vertex to p.big and hands expand_lanes an empty range instead.
-__device__ __forceinline__ void defer_lanes(const Params& p, uint32_t* cnt, bool act, uint32_t u, uint64_t& b,
-                                            uint64_t& e, uint2& dr) {
-  const bool big = act && (e - b) + dr.y >= p.large_row;
-  const uint32_t slot = vxb::warp_append(big, cnt);
-  if (big) {
-    p.big[slot] = u;
-    b = e = 0;
-    dr = make_uint2(0, 0);
-  }
-}
-
-// Surviving-parent test of the deferred vertices p.big[0, nb): every warp scans
-// a 32-arc slice of the row per step; found[r] (p.tent, zeroed by the warp
-// pass) is set by the first warp that sees a surviving parent, and the others
-// stop at their next step.
-__device__ void grid_parent_probe(const Params& p, uint32_t nb, uint32_t d) {
-  const DevAdj& a = p.g.in;
+template <class W>
+__device__ void drain(const Params& p, RepairSmem& sm, W& w) {
+  BfsCounters* c = p.c;
   const int lane = threadIdx.x & 31;
-  for (uint32_t r = 0; r < nb; ++r) {
-    const uint32_t v = p.big[r];
-    uint64_t b, e;
-    vxb::base_range(a, v, b, e);
-    const uint2 dr = a.drow[v];
-    const uint64_t nbase = e - b, total = nbase + dr.y;
-    for (uint64_t k0 = (uint64_t)gwarp() * 32; k0 < total; k0 += (uint64_t)nwarps() * 32) {
-      if (ld_cg(&p.tent[r])) break;  // one load for the warp: the break is warp-uniform
-      const uint64_t k = k0 + lane;
-      bool ok = false;
-      if (k < total) {
-        uint32_t x;
-        bool valid = true;
-        if (k < nbase) {
-          x = a.col[b + k];
-          valid = !(x & kTomb);
-        } else {
-          x = a.darena[dr.x + (uint32_t)(k - nbase)];
+  uint32_t cur = 0, end = 0;  // warp 0's ticket [cur, end), uniform over its lanes
+  uint32_t idle = 0;
+  for (;;) {
+    if (threadIdx.x < 32) {
+      uint32_t n = 0, stop = 0;
+      if (ld_cg(&c->err)) {
+        stop = 1;
+      } else {
+        if (cur == end) {
+          uint32_t s0 = 0;
+          if (lane == 0) {
+            s0 = atomicAdd(p.rq_head, kClaim);
+            atomicAdd(&p.rq_stat[1], 1ull);
+          }
+          cur = __shfl_sync(FULL, s0, 0);
+          end = cur + kClaim;
         }
-        ok = valid && x < p.dist_len && p.dist[x] + 1 == d && !test_bit(p.aff, x);
+        const uint32_t k = cur + lane;
+        unsigned long long v = kSent;
+        if (k < end) v = __ldcg(&p.ring[k & p.ring_mask]);
+        const uint32_t have = __ballot_sync(FULL, v != kSent);
+        n = have == FULL ? 32u : (uint32_t)(__ffs(~have) - 1);  // leading filled slots
+        if ((uint32_t)lane < n) {
+          sm.items[lane] = v;
+          __stcg(&p.ring[k & p.ring_mask], kSent);
+        }
+        cur += n;
+        if (n == 0 && (idle & 7) == 7) {
+          uint32_t st = 0;
+          if (lane == 0) {
+            const uint32_t dn = ld_cg(p.rq_done);
+            __threadfence();
+            st = dn == ld_cg(p.rq_tail);
+            atomicAdd(&p.rq_stat[3], 1ull);
+          }
+          stop = __shfl_sync(FULL, st, 0);
+        }
       }
-      if (__any_sync(FULL, ok)) {
-        if (lane == 0) atomicExch(&p.tent[r], 1u);
+      if (lane == 0) {
+        sm.n = n;
+        sm.stop = stop;
+      }
+    }
+    __syncthreads();
+    const uint32_t n = sm.n, stop = sm.stop;
+    __syncthreads();  // every thread has read the words before warp 0 rewrites them
+    if (stop) break;
+    if (n == 0) {
+      if (threadIdx.x == 0) atomicAdd(&p.rq_stat[2], 1ull);
+      if (++idle > kDrainIdleLimit) {
+        if (threadIdx.x == 0) atomicOr(&c->err, vxb::kErrDrainTimeout);
         break;
       }
+      __nanosleep(32u << min(idle >> 2, 5u));  // back off to 1 us
+      continue;
+    }
+    idle = 0;
+    const long long t0 = clock64();
+    w.process(sm, n);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();  // this block's pushes are visible before its items count as done
+      atomicAdd(p.rq_done, n);
+      atomicAdd(&p.rq_stat[0], 1ull);
+      const unsigned long long dt = (unsigned long long)(clock64() - t0);
+      atomicAdd(&p.rq_stat[4], dt);
+      atomicMax(&p.rq_stat[5], dt);
     }
   }
 }
 
 // --------------------------------------------------- pre-batch fixpoint --
+//
+// compute_affected_prebatch (bfs.hpp:222-259): a touched vertex x at
+// distance d is affected iff none of its shortest parents survives -- every
+// in-neighbour at d-1 is reached over a deleted arc or is affected itself
+// (the reference's lost >= support).  The fixpoint does not depend on the
+// order, so it runs as one asynchronous cascade with a witness per vertex:
+//
+//   check(x)   scan x's in-row from the saved position for the first parent
+//              that survives and is not affected; record it as the witness,
+//              or mark x affected when the row is exhausted.  Affectedness
+//              only grows, so a rescan never goes back.
+//   expand(y)  y became affected: its children whose witness is y (or that
+//              no check has touched yet) get a check.
+//
+// In-rows longer than kChunk arcs are checked in chunks by many warps at once
+// (chunk_check); their passes always start from the row's beginning.
+//
+// sw[x] packs bit 63 touched, bits 32-62 witness + 1 (0 = none yet), bits
+// 0-31 the scan position.  A check stores its witness, fences, and re-reads
+// the witness's affected bit; mark_affected sets the bit and fences before
+// the expand item is pushed -- so either the check sees the parent affected
+// and scans on, or the expansion sees the witness and asks for a recheck.
+// Requests are deduplicated by a bit in inq[1], cleared when a check starts.
 
-// compute_affected_prebatch (bfs.hpp:222-259) level by level: at distance d
-// the touched vertices (deletion candidates at d, children of vertices that
-// became affected at d-1) are affected iff no shortest parent survives; the
-// children of those at d+1 are touched next.  The fallback limit is checked
-// after every level (the affected count only grows).
-__device__ void repair_pre(const Params& p) {
-  BfsCounters* c = p.c;
+constexpr unsigned long long kSwTouched = 1ull << 63;
+
+// Marks v affected once (the affected bit decides); true for the caller that set it.
+__device__ __forceinline__ bool mark_affected(const Params& p, uint32_t v) {
+  const uint32_t bit = 1u << (v & 31);
+  if (atomicOr(&p.aff[v >> 5], bit) & bit) return false;
+  const uint32_t slot = atomicAdd(&p.c->a_n, 1u);
+  p.lst_a[slot] = v;
+  if (slot + 1 > p.fallback_limit) p.c->fallback = 1;
+  __threadfence();  // the affected bit is visible before the expand item is
+  return true;
+}
+
+// Warp-uniform: request a check of x where pred holds (first touch is recorded
+// in sw and in the touched list; a pending request is not repeated).
+__device__ __forceinline__ void request_check(const Params& p, bool pred, uint32_t x, uint32_t* first_count) {
+  bool first = false, push = false;
+  if (pred) {
+    first = !(atomicOr(&p.sw[x], kSwTouched) & kSwTouched);
+    const uint32_t bit = 1u << (x & 31);
+    push = !(atomicOr(&p.inq[1][x >> 5], bit) & bit);
+  }
+  const uint32_t slot = vxb::warp_append(first, &p.c->touched_n);
+  if (first) p.lst_t[slot] = x;
+  if (first_count) vxb::warp_append(first, first_count);
+  ring_push(p, push, x);
+}
+
+// check(x), whole warp.
+__device__ void check_vertex(const Params& p, uint32_t x) {
+  const DevAdj& a = p.g.in;
   const int lane = threadIdx.x & 31;
-  const uint32_t F = *p.F;
-  for (uint32_t i = gtid(); i < F; i += nthreads()) {
-    const uint8_t f = p.ff[i];
-    if ((f & kFAdd) || !(f & kFCur)) continue;
-    const uint32_t u = p.fu[i], v = p.fv[i];
-    if (!is_sp(p, u, v)) continue;
-    if (atomicOr(&p.lost[v], 1u) == 0u) {
-      const uint32_t slot = atomicAdd(&c->cand_n, 1u);
-      p.lst_t[slot] = v;
-    }
+  if (lane == 0) atomicAnd(&p.inq[1][x >> 5], ~(1u << (x & 31)));
+  __syncwarp();
+  __threadfence();  // the request bit is clear before the state is read
+  const uint32_t d = p.dist[x];
+  uint64_t b, e;
+  vxb::base_range(a, x, b, e);
+  const uint2 dr = a.drow[x];
+  const uint32_t nb = (uint32_t)(e - b), total = nb + dr.y;
+  if (total > kChunk) {
+    // long in-row: one chunk-check item per kChunk arcs, scanned by many warps;
+    // tent[x] counts the chunks of the pass in flight.  A request that finds a
+    // pass in flight is covered by it: the pass clears tent[x] before it
+    // verifies its final witness.
+    const uint32_t K = (total + kChunk - 1) / kChunk;
+    bool start = false;
+    if (lane == 0) start = atomicCAS(&p.tent[x], 0u, K) == 0u;
+    start = __shfl_sync(FULL, start, 0);
+    if (start)
+      for (uint32_t c0 = 0; c0 < K; c0 += 32)
+        ring_push(p, c0 + lane < K, kChunkCheckBit | ((unsigned long long)(c0 + lane) << 32) | x);
+    return;
   }
-  if (gtid() == 0) {
-    for (int k = 0; k < 3; ++k) {
-      c->list_n[k] = 0;
-      c->next_seed[k] = kUnreachable;
-      c->big_n[k] = 0;
-      c->big_t[k] = 0;
-    }
-    c->seed_min = kUnreachable;
-  }
-  if (!sync_grid(p)) return;
-  const uint32_t ncand = ld_cg(&c->cand_n);
-  if (gtid() == 0) {
-    c->candidates = ncand;
-    c->touched_n = ncand;
-  }
-  if (ncand == 0) return;
-  for (uint32_t i = gtid(); i < ncand; i += nthreads()) atomicMin(&c->seed_min, p.dist[p.lst_t[i]]);
-  if (!sync_grid(p)) return;
-  uint32_t d = ld_cg(&c->seed_min);
-  // level-d work list: candidates at d (and later the children touched at d)
-  for (uint32_t i = gtid(); i < ncand; i += nthreads()) {
-    const uint32_t v = p.lst_t[i];
-    if (p.dist[v] == d) p.q[0][atomicAdd(&c->list_n[0], 1u)] = v;
-  }
-  if (!sync_grid(p)) return;
-  uint32_t a_prev = 0;
-  for (uint32_t it = 0;; ++it) {
-    if (it > p.dist_len + 1) {
-      if (gtid() == 0) atomicOr(&c->err, vxb::kErrLoopBound);
-      break;
-    }
-    const int k = it % 3, k1 = (it + 1) % 3, k2 = (it + 2) % 3;
-    const uint32_t np = ld_cg(&c->list_n[k]);
-    if (gtid() == 0) {
-      c->list_n[k2] = 0;
-      c->next_seed[k2] = kUnreachable;
-      c->big_n[k2] = 0;
-      c->big_t[k2] = 0;
-    }
-    // every touched vertex at distance d: one warp each, long rows deferred
-    for (uint32_t i = gwarp(); i < np; i += nwarps()) {
-      const uint32_t v = p.q[k][i];
-      if (defer_row(p, p.g.in, v)) {
-        if (lane == 0) {
-          const uint32_t slot = atomicAdd(&c->big_n[k], 1u);
-          p.big[slot] = v;
-          p.tent[slot] = 0u;
-        }
-        continue;
+  uint32_t k0 = (uint32_t)__ldcg(&p.sw[x]);
+  bool resolved = false;
+  while (k0 < total && !resolved) {
+    const uint32_t k = k0 + lane;
+    bool ok = false;
+    uint32_t y = 0;
+    if (k < total) {
+      bool valid = true;
+      if (k < nb) {
+        y = a.col[b + k];
+        valid = !(y & kTomb);
+        y &= kIdMask;
+      } else {
+        y = a.darena[dr.x + (k - nb)];
       }
-      if (!warp_has_surviving_parent(p, v, d) && lane == 0) mark_affected(p, v);
+      ok = valid && y < p.dist_len && p.dist[y] + 1 == d && !test_bit_cg(p.aff, y);
     }
-    if (!sync_grid(p)) return;
-    const uint32_t nbp = ld_cg(&c->big_n[k]);
-    if (nbp) {
-      grid_parent_probe(p, nbp, d);
-      if (!sync_grid(p)) return;
-      for (uint32_t r = gtid(); r < nbp; r += nthreads())
-        if (!ld_cg(&p.tent[r])) mark_affected(p, p.big[r]);
-      if (!sync_grid(p)) return;
-    }
-    const uint32_t a_tot = ld_cg(&c->a_n);
-    if (a_tot > p.fallback_limit) {
-      if (gtid() == 0) c->fallback = 1;
-      break;
-    }
-    // next level's list: children of the vertices affected at d, candidates
-    // at d+1; the nearest deeper candidate level for a jump
-    TouchChildren tc{&p, d, p.q[k1], &c->list_n[k1]};
-    for (uint32_t i = a_prev + gwarp(); i < a_tot; i += nwarps()) {
-      const uint32_t v = p.lst_a[i];
-      if (defer_row(p, p.g.out, v)) {
-        if (lane == 0) p.big[atomicAdd(&c->big_t[k], 1u)] = v;
-        continue;
-      }
-      warp_row(p.g.out, v, tc);
-    }
-    for (uint32_t i = gtid(); i < ncand; i += nthreads()) {
-      const uint32_t v = p.lst_t[i];
-      const uint32_t dv = p.dist[v];
-      if (dv == d + 1) p.q[k1][atomicAdd(&c->list_n[k1], 1u)] = v;
-      else if (dv != kUnreachable && dv > d + 1) atomicMin(&c->next_seed[k1], dv);
-    }
-    if (!sync_grid(p)) return;
-    const uint32_t nbt = ld_cg(&c->big_t[k]);
-    if (nbt) {
-      grid_rows(p.g.out, p.big, nbt, tc);
-      if (!sync_grid(p)) return;
-    }
-    a_prev = a_tot;
-    const uint32_t nn = ld_cg(&c->list_n[k1]);
-    if (nn > 0) {
-      ++d;
+    const uint32_t ball = __ballot_sync(FULL, ok);
+    if (!ball) {
+      k0 += 32;
       continue;
     }
-    const uint32_t ns = ld_cg(&c->next_seed[k1]);
-    if (ns == kUnreachable) break;
-    // every block must have read list_n[k1] == 0 before it is refilled, or a
-    // late block would see the refilled count and take the other branch
-    if (!sync_grid(p)) return;
-    d = ns;  // no touched vertex at d+1: jump to the next candidate level
-    for (uint32_t i = gtid(); i < ncand; i += nthreads()) {
-      const uint32_t v = p.lst_t[i];
-      if (p.dist[v] == d) p.q[k1][atomicAdd(&c->list_n[k1], 1u)] = v;
+    const int f = __ffs(ball) - 1;
+    const uint32_t yw = __shfl_sync(FULL, y, f);
+    const uint32_t kw = k0 + (uint32_t)f;
+    bool still = false;
+    if (lane == 0) {
+      __stcg(&p.sw[x], kSwTouched | ((unsigned long long)(yw + 1) << 32) | kw);
+      __threadfence();
+      still = !test_bit_cg(p.aff, yw);
     }
-    if (!sync_grid(p)) return;
+    resolved = __shfl_sync(FULL, still, 0);
+    k0 = kw + 1;  // the witness turned affected meanwhile: scan on past it
   }
-  if (gtid() == 0) c->affected = ld_cg(&c->a_n);
+  if (!resolved) {
+    bool push = false;
+    if (lane == 0) {
+      __stcg(&p.sw[x], kSwTouched | (unsigned long long)total);
+      push = mark_affected(p, x);
+    }
+    ring_push(p, push, (unsigned long long)(x | kKindBit));
+  }
+}
+
+// One chunk of a long check (whole warp): scan [c * kChunk, (c + 1) * kChunk)
+// of x's in-row for a surviving, non-affected parent, unless another chunk
+// found one already (kFoundBit in tent[x]).  The last chunk of the pass clears
+// tent[x], then either verifies the recorded witness (asking for a new check
+// if it turned affected) or, when no chunk found one, marks x affected.
+constexpr uint32_t kFoundBit = 0x80000000u;
+
+__device__ void chunk_check(const Params& p, uint32_t x, uint32_t c) {
+  const DevAdj& a = p.g.in;
+  const int lane = threadIdx.x & 31;
+  const uint32_t d = p.dist[x];
+  uint64_t b, e;
+  vxb::base_range(a, x, b, e);
+  const uint2 dr = a.drow[x];
+  const uint32_t nb = (uint32_t)(e - b), total = nb + dr.y;
+  const uint32_t lo = c * kChunk, hi = min(total, lo + kChunk);
+  uint32_t k0 = lo;
+  bool found = (ld_cg(&p.tent[x]) & kFoundBit) != 0u;
+  while (k0 < hi && !found) {
+    const uint32_t k = k0 + lane;
+    bool ok = false;
+    uint32_t y = 0;
+    if (k < hi) {
+      bool valid = true;
+      if (k < nb) {
+        y = a.col[b + k];
+        valid = !(y & kTomb);
+        y &= kIdMask;
+      } else {
+        y = a.darena[dr.x + (k - nb)];
+      }
+      ok = valid && y < p.dist_len && p.dist[y] + 1 == d && !test_bit_cg(p.aff, y);
+    }
+    const uint32_t ball = __ballot_sync(FULL, ok);
+    if (!ball) {
+      k0 += 32;
+      if (((k0 - lo) & 127) == 0) found = (ld_cg(&p.tent[x]) & kFoundBit) != 0u;  // one load per warp
+      continue;
+    }
+    const int f = __ffs(ball) - 1;
+    const uint32_t yw = __shfl_sync(FULL, y, f);
+    bool good = false;
+    if (lane == 0) {
+      __stcg(&p.sw[x], kSwTouched | ((unsigned long long)(yw + 1) << 32));
+      __threadfence();
+      good = !test_bit_cg(p.aff, yw);
+      if (good) atomicOr(&p.tent[x], kFoundBit);
+    }
+    found = __shfl_sync(FULL, good, 0);
+    k0 += (uint32_t)f + 1;
+  }
+  bool recheck = false, aff = false;
+  if (lane == 0) {
+    __threadfence();
+    const uint32_t old = atomicSub(&p.tent[x], 1u);
+    if ((old & ~kFoundBit) == 1u) {  // the pass's last chunk
+      atomicExch(&p.tent[x], 0u);
+      __threadfence();
+      if (old & kFoundBit) {
+        const uint32_t w1 = (uint32_t)(__ldcg(&p.sw[x]) >> 32) & 0x7FFFFFFFu;
+        recheck = w1 == 0u || test_bit_cg(p.aff, w1 - 1);
+      } else {
+        aff = mark_affected(p, x);
+      }
+    }
+  }
+  request_check(p, recheck, x, nullptr);
+  ring_push(p, aff, (unsigned long long)(x | kKindBit));
+}
+
+struct Cascade {
+  const Params* p;
+  LbStage* lb;
+  __device__ void process(RepairSmem& sm, uint32_t n) {
+    const Params& P = *p;
+    BfsCounters* c = P.c;
+    const uint32_t t = threadIdx.x;
+    if (t == 0) {
+      sm.nsv = 0;
+      sm.nex = 0;
+      sm.fallback = ld_cg(&c->fallback);
+    }
+    __syncthreads();
+    if (t < n) {
+      const unsigned long long it = sm.items[t];
+      if (it != kSent) {
+        if (it & kChunkCheckBit) {
+          const uint32_t k = atomicAdd(&sm.nsv, 1u);
+          sm.sv[k] = item_vertex(it);
+          sm.cnt[k] = item_chunk(it) + 1;
+        } else if ((uint32_t)it & kKindBit) {
+          sm.ex[atomicAdd(&sm.nex, 1u)] = it;
+        } else {
+          const uint32_t k = atomicAdd(&sm.nsv, 1u);
+          sm.sv[k] = (uint32_t)it;
+          sm.cnt[k] = 0u;
+        }
+      }
+    }
+    __threadfence();  // expand items were pushed after their affected bits
+    __syncthreads();
+    if (sm.fallback) {
+      // past the fallback limit: drop the items, keeping the request bits clear
+      for (uint32_t i = t; i < sm.nsv; i += kThreads)
+        if (sm.cnt[i] == 0u) atomicAnd(&P.inq[1][sm.sv[i] >> 5], ~(1u << (sm.sv[i] & 31)));
+      return;
+    }
+    const uint32_t nsv = sm.nsv, nex = sm.nex;
+    for (uint32_t i = t >> 5; i < nsv; i += kThreads / 32) {
+      if (sm.cnt[i]) chunk_check(P, sm.sv[i], sm.cnt[i] - 1);
+      else check_vertex(P, sm.sv[i]);
+    }
+    if (nex) {
+      if (t < nex) sm.d[t] = P.dist[item_vertex(sm.ex[t])];
+      __syncthreads();
+      auto expand = [&](bool valid, uint32_t x, uint32_t j) {
+        bool need = false;
+        if (valid && x < P.dist_len && P.dist[x] == sm.d[j] + 1) {
+          const unsigned long long w = __ldcg(&P.sw[x]);
+          const uint32_t wit = (uint32_t)(w >> 32) & 0x7FFFFFFFu;
+          need = !(w & kSwTouched) || wit == item_vertex(sm.ex[j]) + 1;
+        }
+        request_check(P, need, x, nullptr);
+      };
+      block_rows(P.g.out, sm.ex, nex, *lb, expand, &P);
+    }
+  }
+};
+
+__device__ void reset_ring(const Params& p) {
+  if (gtid() == 0) {
+    *p.rq_head = 0;
+    *p.rq_tail = 0;
+    *p.rq_done = 0;
+    for (int k = 0; k < 6; ++k) p.rq_stat[k] = 0;
+  }
+}
+
+__device__ __forceinline__ void stamp(const Params& p, int k) {
+  if (gtid() == 0) p.c->rtrace[k] = globaltimer();
+}
+
+__device__ void repair_pre(const Params& p, RepairSmem& sm, LbStage& lb) {
+  BfsCounters* c = p.c;
+  const int lane = threadIdx.x & 31;
+  stamp(p, 0);
+  reset_ring(p);
+  if (!sync_grid(p)) return;
+  // deletion candidates (bfs.hpp:52-63): heads of deleted shortest-parent
+  // arcs, each checked once
+  const uint32_t F = *p.F;
+  for (uint32_t base = gwarp() * 32; base < F; base += nwarps() * 32) {
+    const uint32_t i = base + lane;
+    bool cand = false;
+    uint32_t v = 0;
+    if (i < F) {
+      const uint8_t f = p.ff[i];
+      const uint32_t u = p.fu[i];
+      v = p.fv[i];
+      cand = !(f & kFAdd) && (f & kFCur) && is_sp(p, u, v);
+    }
+    request_check(p, cand, v, &c->cand_n);
+  }
+  if (!sync_grid(p)) return;
+  stamp(p, 1);
+  const uint32_t ncand = ld_cg(&c->cand_n);
+  if (gtid() == 0) c->candidates = ncand;
+  if (ncand == 0) return;
+  Cascade w{&p, &lb};
+  drain(p, sm, w);
+  if (!sync_grid(p)) return;
+  stamp(p, 2);
+  if (gtid() == 0) {
+    c->affected = ld_cg(&c->a_n);
+    c->rtrace[7] = ld_cg(p.rq_tail);
+    for (int k = 0; k < 6; ++k) c->rtrace[9 + k] = __ldcg(&p.rq_stat[k]);
+  }
+  reset_ring(p);  // for the post-batch kernel
 }
 
 // -------------------------------------------------- post-batch repair --
 
-__device__ __forceinline__ void reach_add(const Params& p, long long d) {
-  if (d) atomicAdd(&p.c->reachable, (unsigned long long)d);
-}
-
 __device__ void clear_workspace(const Params& p) {
   const uint32_t nt = ld_cg(&p.c->touched_n), na = ld_cg(&p.c->a_n);
-  for (uint32_t i = gtid(); i < nt; i += nthreads()) p.lost[p.lst_t[i]] = 0u;
+  for (uint32_t i = gtid(); i < nt; i += nthreads()) {
+    p.sw[p.lst_t[i]] = 0ull;
+    p.tent[p.lst_t[i]] = 0u;  // chunk counts left by a pass the fallback dropped
+  }
   for (uint32_t i = gtid(); i < na; i += nthreads()) p.aff[p.lst_a[i] >> 5] = 0u;
 }
 
-// Lower dist[x] to cand; on success (INF -> finite counted) queue x once per
-// round through the inq bitmap.
-__device__ __forceinline__ void lower_and_queue(const Params& p, uint32_t x, uint32_t cand, uint32_t* inq_next,
-                                                uint32_t* qn, uint32_t* cnt, long long& reach) {
-  if (cand >= ld_cg(&p.dist[x])) return;
+// Lower dist[x] to cand; true when this thread lowered it (INF -> finite
+// counted in reach).
+__device__ __forceinline__ bool lower(const Params& p, uint32_t x, uint32_t cand, long long& reach) {
+  if (cand >= ld_cg(&p.dist[x])) return false;
   const uint32_t old = atomicMin(&p.dist[x], cand);
-  if (old <= cand) return;
+  if (old <= cand) return false;
   if (old == kUnreachable) ++reach;
-  const uint32_t bit = 1u << (x & 31);
-  if (!(atomicOr(&inq_next[x >> 5], bit) & bit)) {
-    const uint32_t s = atomicAdd(cnt, 1u);
-    qn[s] = x;
-  }
+  return true;
 }
 
-// Bucketed settle: relax affected out-neighbours of level-lvl vertices.
-struct SettleVisit {
+// Queue x unless it is queued already (inq bit; cleared when claimed).
+__device__ __forceinline__ void lower_and_push(const Params& p, bool lowered, uint32_t x) {
+  bool push = false;
+  if (lowered) {
+    const uint32_t bit = 1u << (x & 31);
+    push = !(atomicOr(&p.inq[0][x >> 5], bit) & bit);
+  }
+  ring_push(p, push, x);
+}
+
+// Label-correcting relaxation (the settle of repair_affected, bfs.hpp:272-310,
+// and propagate_decreases, :341-354, as one phase): every label is an upper
+// bound of the post-batch distance, and relaxing from every changed label
+// until nothing lowers gives the exact distances in any order.
+struct Relax {
   const Params* p;
-  uint32_t lvl;
-  uint32_t* qn;
-  uint32_t* cnt;
+  LbStage* lb;
   long long* reach;
-  __device__ __forceinline__ void operator()(bool valid, uint32_t x, uint32_t) {
-    bool lowered = false;
-    if (valid && test_bit(p->aff, x)) {
-      const uint32_t cand = lvl + 1;
-      if (cand < ld_cg(&p->dist[x])) {
-        const uint32_t old = atomicMin(&p->dist[x], cand);
-        if (old > cand) {
-          lowered = true;
-          if (old == kUnreachable) ++*reach;
-        }
+  __device__ void process(RepairSmem& sm, uint32_t n) {
+    const Params& P = *p;
+    const uint32_t t = threadIdx.x;
+    if (t < n) {
+      const unsigned long long it = sm.items[t];
+      uint32_t du = kUnreachable;
+      if (it != kSent) {
+        const uint32_t u = item_vertex(it);
+        if (item_chunk(it) == 0) atomicAnd(&P.inq[0][u >> 5], ~(1u << (u & 31)));
+        du = ld_cg(&P.dist[u]);
       }
+      sm.d[t] = du;
     }
-    const uint32_t s = vxb::warp_append(lowered, cnt);
-    if (lowered) qn[s] = x;
+    __syncthreads();
+    auto relax = [&](bool valid, uint32_t x, uint32_t j) {
+      const uint32_t du = sm.d[j];
+      const bool lowered = valid && du != kUnreachable && x < P.dist_len && lower(P, x, du + 1, *reach);
+      lower_and_push(P, lowered, x);
+    };
+    block_rows(P.g.out, sm.items, n, *lb, relax, &P);
   }
 };
 
-// Decrease propagation: relax every out-neighbour of a queued vertex.
-struct PropVisit {
-  const Params* p;
-  uint32_t* inq_next;
-  uint32_t* qn;
-  uint32_t* cnt;
-  long long* reach;
-  __device__ __forceinline__ void operator()(bool valid, uint32_t x, uint32_t u) {
-    if (!valid) return;
-    const uint32_t du = ld_cg(&p->dist[u]);
-    if (du == kUnreachable) return;
-    lower_and_queue(*p, x, du + 1, inq_next, qn, cnt, *reach);
-  }
-};
-
-// Warp-uniform minimum of dist+1 over non-affected in-neighbours
-// (best_boundary_distance, bfs.hpp:261-269).
-struct BoundaryMin {
-  const Params* p;
-  uint32_t best;
-  __device__ __forceinline__ void operator()(bool valid, uint32_t x, uint32_t) {
-    if (!valid || x >= p->dist_len || test_bit(p->aff, x)) return;
-    const uint32_t dx = p->dist[x];
-    if (dx != kUnreachable && dx + 1 < best) best = dx + 1;
-  }
-};
-
-// Boundary distance of the deferred affected entries p.big[0, nb) (indices
-// into lst_a): each warp folds its slices into p.tent[i] by atomicMin.
-__device__ void grid_boundary_min(const Params& p, uint32_t nb) {
-  const DevAdj& a = p.g.in;
-  for (uint32_t r = 0; r < nb; ++r) {
-    const uint32_t i = p.big[r];
-    const uint32_t v = p.lst_a[i];
-    BoundaryMin bm{&p, kUnreachable};
-    uint64_t b, e;
-    vxb::base_range(a, v, b, e);
-    for (uint64_t j0 = b + (uint64_t)gwarp() * 32; j0 < e; j0 += (uint64_t)nwarps() * 32) {
-      const uint64_t j = j0 + (threadIdx.x & 31);
-      const uint32_t x = j < e ? a.col[j] : kTomb;
-      bm(!(x & kTomb), x & kIdMask, v);
+// Boundary distances (best_boundary_distance, bfs.hpp:261-269) of the
+// affected vertices, a block-sized chunk of them at a time: min of dist + 1
+// over non-affected in-neighbours, folded per vertex in shared memory; each
+// finite one seeds the relaxation.
+__device__ void boundary_seeds(const Params& p, RepairSmem& sm, LbStage& lb, uint32_t na, long long& reach) {
+  const uint32_t per = min((uint32_t)kThreads, max(1u, (na + gridDim.x - 1) / gridDim.x));
+  for (uint32_t i0 = blockIdx.x * per; i0 < na; i0 += gridDim.x * per) {
+    const uint32_t k = min(per, na - i0);
+    if (threadIdx.x < k) {
+      sm.sv[threadIdx.x] = p.lst_a[i0 + threadIdx.x];
+      sm.cnt[threadIdx.x] = kUnreachable;
     }
-    const uint2 dr = a.drow[v];
-    for (uint32_t j0 = dr.x + gwarp() * 32; j0 < dr.x + dr.y; j0 += nwarps() * 32) {
-      const uint32_t j = j0 + (threadIdx.x & 31);
-      const bool ok = j < dr.x + dr.y;
-      bm(ok, ok ? a.darena[j] : 0u, v);
+    __syncthreads();
+    auto bmin = [&](bool valid, uint32_t x, uint32_t j) {
+      if (!valid || x >= p.dist_len || test_bit(p.aff, x)) return;
+      const uint32_t dx = p.dist[x];
+      if (dx != kUnreachable) atomicMin(&sm.cnt[j], dx + 1);
+    };
+    block_rows(p.g.in, sm.sv, k, lb, bmin);
+    bool seed = false;
+    uint32_t v = 0;
+    if (threadIdx.x < k) {
+      v = sm.sv[threadIdx.x];
+      const uint32_t best = sm.cnt[threadIdx.x];
+      // by atomicMin: an inserted arc may lower v first
+      if (best != kUnreachable) seed = lower(p, v, best, reach);
     }
-    uint32_t best = bm.best;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(FULL, best, o));
-    if ((threadIdx.x & 31) == 0 && best != kUnreachable) atomicMin(&p.tent[i], best);
+    lower_and_push(p, seed, v);
+    __syncthreads();
   }
 }
 
-__device__ void repair_post(const Params& p) {
+__device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQueue& bq) {
   BfsCounters* c = p.c;
   const int lane = threadIdx.x & 31;
   if (ld_cg(&c->fallback)) {
     clear_workspace(p);
     if (!sync_grid(p)) return;
-    full_bfs(p);
+    full_bfs(p, bq, lb);
     if (gtid() == 0) c->full = 1;
     return;
   }
+  // the ring counters are zero here: the pre-batch kernel (or the previous
+  // batch) left them so, and the first push comes after a barrier of this
+  // kernel or a kernel boundary
+  stamp(p, 3);
   const uint32_t na = ld_cg(&c->a_n);
   long long reach = 0;
   if (na > 0) {
-    for (uint32_t i = gtid(); i < na; i += nthreads()) {
-      const uint32_t v = p.lst_a[i];
-      p.old[i] = p.dist[v];
-      p.dist[v] = kUnreachable;
-    }
-    if (gtid() == 0) {
-      reach_add(p, -(long long)na);
-      c->seed_min = kUnreachable;
-      for (int k = 0; k < 3; ++k) {
-        c->list_n[k] = 0;
-        c->next_seed[k] = kUnreachable;
-        c->big_n[k] = 0;
-        c->big_t[k] = 0;
-      }
-    }
+    // invalidate the affected vertices (repair_affected, bfs.hpp:272-283)
+    for (uint32_t i = gtid(); i < na; i += nthreads()) p.dist[p.lst_a[i]] = kUnreachable;
+    if (gtid() == 0) reach_add(p, -(long long)na);
     if (!sync_grid(p)) return;
-    // boundary seeds, one warp per affected vertex, long in-rows deferred
-    for (uint32_t i = gwarp(); i < na; i += nwarps()) {
-      const uint32_t v = p.lst_a[i];
-      if (defer_row(p, p.g.in, v)) {
-        if (lane == 0) {
-          p.tent[i] = kUnreachable;
-          p.big[atomicAdd(&c->big_t[0], 1u)] = i;
-        }
-        continue;
-      }
-      BoundaryMin bm{&p, kUnreachable};
-      warp_row(p.g.in, v, bm);
-      uint32_t best = bm.best;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(FULL, best, o));
-      if (lane == 0) {
-        p.tent[i] = best;
-        p.dist[v] = best;
-        if (best != kUnreachable) {
-          ++reach;
-          atomicMin(&c->seed_min, best);
-        }
-      }
-    }
-    if (!sync_grid(p)) return;
-    const uint32_t nbb = ld_cg(&c->big_t[0]);
-    if (nbb) {
-      grid_boundary_min(p, nbb);
-      if (!sync_grid(p)) return;
-      for (uint32_t r = gtid(); r < nbb; r += nthreads()) {
-        const uint32_t i = p.big[r];
-        const uint32_t best = ld_cg(&p.tent[i]);
-        p.dist[p.lst_a[i]] = best;
-        if (best != kUnreachable) {
-          ++reach;
-          atomicMin(&c->seed_min, best);
-        }
-      }
-      if (!sync_grid(p)) return;
-    }
-    // bucketed settle among affected vertices (unit-weight Dijkstra)
-    uint32_t lvl = ld_cg(&c->seed_min);
-    if (lvl != kUnreachable) {
-      const DevAdj& a = p.g.out;
-      for (uint32_t it = 0;; ++it) {
-        if (it > p.dist_len + 1) {
-          if (gtid() == 0) atomicOr(&c->err, vxb::kErrLoopBound);
-          break;
-        }
-        const int k = it % 3, k1 = (it + 1) % 3, k2 = (it + 2) % 3;
-        const uint32_t nr = ld_cg(&c->list_n[k]);
-        if (gtid() == 0) {
-          c->list_n[k2] = 0;
-          c->next_seed[k2] = kUnreachable;
-          c->big_n[k2] = 0;
-        }
-        SettleVisit sv{&p, lvl, p.q[k1], &c->list_n[k1], &reach};
-        // items: seeds whose boundary distance is lvl and still hold it, then
-        // the vertices relaxed to lvl at the previous level
-        for (uint32_t base = gwarp() * 32; base < na + nr; base += nwarps() * 32) {
-          const uint32_t i = base + lane;
-          bool act = false;
-          uint32_t u = 0;
-          if (i < na) {
-            const uint32_t t = p.tent[i];
-            u = p.lst_a[i];
-            const uint32_t du = ld_cg(&p.dist[u]);
-            act = t == lvl && du == lvl;
-            if (!act && t != kUnreachable && t > lvl && du == t) atomicMin(&c->next_seed[k1], t);
-          } else if (i < na + nr) {
-            u = p.q[k][i - na];
-            act = true;
-          }
-          uint64_t b = 0, e = 0;
-          uint2 dr = make_uint2(0, 0);
-          if (act) {
-            vxb::base_range(a, u, b, e);
-            dr = a.drow[u];
-          }
-          defer_lanes(p, &c->big_n[k], act, u, b, e, dr);
-          expand_lanes(a, u, b, e, dr, sv);
-        }
-        if (!sync_grid(p)) return;
-        const uint32_t nbs = ld_cg(&c->big_n[k]);
-        if (nbs) {
-          grid_rows(a, p.big, nbs, sv);
-          if (!sync_grid(p)) return;
-        }
-        const uint32_t nn = ld_cg(&c->list_n[k1]), ns = ld_cg(&c->next_seed[k1]);
-        if (nn > 0) ++lvl;
-        else if (ns != kUnreachable) lvl = ns;
-        else break;
-      }
-    }
+    stamp(p, 4);
+    boundary_seeds(p, sm, lb, na, reach);
   }
-  // decrease propagation (bfs.hpp:312-318, 91-96, 341-354): seeds are the
-  // affected vertices that ended below their old distance and the heads of
-  // inserted arcs that relax
-  if (gtid() == 0) {
-    for (int k = 0; k < 3; ++k) {
-      c->list_n[k] = 0;
-      c->big_n[k] = 0;
-    }
-  }
-  if (!sync_grid(p)) return;
-  for (uint32_t i = gtid(); i < na; i += nthreads()) {
-    const uint32_t v = p.lst_a[i];
-    const uint32_t dv = ld_cg(&p.dist[v]);
-    if (dv != kUnreachable && dv < p.old[i]) {
-      const uint32_t bit = 1u << (v & 31);
-      if (!(atomicOr(&p.inq[0][v >> 5], bit) & bit)) p.q[0][atomicAdd(&c->list_n[0], 1u)] = v;
-    }
-  }
+  // inserted arcs relax their heads (bfs.hpp:91-96)
   const uint32_t F = *p.F;
-  for (uint32_t i = gtid(); i < F; i += nthreads()) {
-    if (!(p.ff[i] & kFAdd)) continue;
-    const uint32_t u = p.fu[i], v = p.fv[i];
-    if (u >= p.dist_len || v >= p.dist_len) continue;
-    const uint32_t du = ld_cg(&p.dist[u]);
-    if (du == kUnreachable) continue;
-    lower_and_queue(p, v, du + 1, p.inq[0], p.q[0], &c->list_n[0], reach);
+  for (uint32_t base = gwarp() * 32; base < F; base += nwarps() * 32) {
+    const uint32_t i = base + lane;
+    bool lowered = false;
+    uint32_t v = 0;
+    if (i < F && (p.ff[i] & kFAdd)) {
+      const uint32_t u = p.fu[i];
+      v = p.fv[i];
+      if (u < p.dist_len && v < p.dist_len) {
+        const uint32_t du = ld_cg(&p.dist[u]);
+        if (du != kUnreachable) lowered = lower(p, v, du + 1, reach);
+      }
+    }
+    lower_and_push(p, lowered, v);
   }
   if (!sync_grid(p)) return;
-  const DevAdj& a = p.g.out;
-  for (uint32_t r = 0;; ++r) {
-    if (r > p.dist_len + 1) {
-      if (gtid() == 0) atomicOr(&c->err, vxb::kErrLoopBound);
-      break;
-    }
-    const int k = r % 3, k1 = (r + 1) % 3, k2 = (r + 2) % 3;
-    const uint32_t n = ld_cg(&c->list_n[k]);
-    if (n == 0) break;
-    if (gtid() == 0) {
-      c->list_n[k2] = 0;
-      c->big_n[k2] = 0;
-    }
-    uint32_t* inq_cur = p.inq[r & 1];
-    PropVisit pv{&p, p.inq[(r + 1) & 1], p.q[k1], &c->list_n[k1], &reach};
-    for (uint32_t base = gwarp() * 32; base < n; base += nwarps() * 32) {
-      const uint32_t i = base + lane;
-      const bool act = i < n;
-      const uint32_t u = act ? p.q[k][i] : 0u;
-      uint64_t b = 0, e = 0;
-      uint2 dr = make_uint2(0, 0);
-      if (act) {
-        atomicAnd(&inq_cur[u >> 5], ~(1u << (u & 31)));
-        vxb::base_range(a, u, b, e);
-        dr = a.drow[u];
-      }
-      defer_lanes(p, &c->big_n[k], act, u, b, e, dr);
-      expand_lanes(a, u, b, e, dr, pv);
-    }
-    if (!sync_grid(p)) return;
-    const uint32_t nbq = ld_cg(&c->big_n[k]);
-    if (nbq) {
-      grid_rows(a, p.big, nbq, pv);
-      if (!sync_grid(p)) return;
-    }
+  stamp(p, 5);
+  Relax w{&p, &lb, &reach};
+  drain(p, sm, w);
+  if (!sync_grid(p)) return;
+  stamp(p, 6);
+  if (gtid() == 0) {
+    c->rtrace[8] = ld_cg(p.rq_tail);
+    for (int k = 0; k < 6; ++k) c->rtrace[15 + k] = __ldcg(&p.rq_stat[k]);
   }
   reach = vxb::warp_sum(reach);
   if (lane == 0) reach_add(p, reach);
   clear_workspace(p);
+  reset_ring(p);
 }
 
 __global__ void __launch_bounds__(kThreads, 3) bfs_kernel(Params p, int mode) {
-  if (mode == kModeFull) full_bfs(p);
-  else if (mode == kModePre) repair_pre(p);
-  else repair_post(p);
+  __shared__ BlockQueue bq;
+  __shared__ LbStage lb;
+  __shared__ RepairSmem sm;
+  if (mode == kModeFull) full_bfs(p, bq, lb);
+  else if (mode == kModePre) repair_pre(p, sm, lb);
+  else repair_post(p, sm, lb, bq);
 }
 
 __global__ void reached_arcs_kernel(vxb::DevAdj a, const uint32_t* dist, uint32_t n,
@@ -1039,7 +1187,7 @@ static int ensure_capacity(Bfs* b, size_t V) {
   const size_t oldw = b->cap ? (b->cap + 31) / 32 + 1 : 0;
   int rc = 0;
   rc |= realloc_copy(&b->dist, c, b->cap, 0xFF);
-  rc |= realloc_copy(&b->lost, c, b->cap, 0);
+  rc |= realloc_copy(&b->sw, 2 * c, 0, 0);
   rc |= realloc_copy(&b->vis, words, 0, 0);
   rc |= realloc_copy(&b->aff, words, oldw, 0);
   rc |= realloc_copy(&b->inq[0], words, oldw, 0);
@@ -1051,10 +1199,32 @@ static int ensure_capacity(Bfs* b, size_t V) {
   rc |= realloc_copy(&b->big, c, 0, 0);
   rc |= realloc_copy(&b->lst_a, c, 0, 0);
   rc |= realloc_copy(&b->lst_t, c, 0, 0);
-  rc |= realloc_copy(&b->old, c, 0, 0);
   rc |= realloc_copy(&b->tent, c, 0, 0);
   if (rc) return -4;
   b->cap = c;
+  return 0;
+}
+
+// The work ring holds at most one pending item per vertex plus the extra
+// chunks of long rows (one per kChunk arcs), so it is sized for capacity +
+// arcs / kChunk, checked before every staged batch (the arcs grow).
+static int ensure_ring(Bfs* b) {
+  const Adjacency& a = b->g->adj[0];
+  // + the tickets blocks hold past the tail (kClaim each) and slack
+  const size_t need = b->cap + (size_t)((a.A + a.arena_bound) / kChunk) + (size_t)kThreads * 1024;
+  size_t slots = 1;
+  while (slots < need) slots <<= 1;
+  if (slots <= b->ring_slots) return 0;
+  VX_CUDA_TRY(cudaStreamSynchronize(b->g->stream));
+  cudaFree(b->ring);
+  b->ring = nullptr;
+  b->ring_slots = 0;
+  if (cudaMalloc(&b->ring, slots * sizeof(unsigned long long)) != cudaSuccess) {
+    set_error("BFS work ring allocation of %zu bytes failed", slots * 8);
+    return -4;
+  }
+  VX_CUDA_TRY(cudaMemset(b->ring, 0xFF, slots * sizeof(unsigned long long)));
+  b->ring_slots = slots;
   return 0;
 }
 
@@ -1075,9 +1245,14 @@ static Params make_params(Bfs* b, uint32_t V, uint32_t dist_len) {
   p.big = b->big;
   p.lst_a = b->lst_a;
   p.lst_t = b->lst_t;
-  p.old = b->old;
   p.tent = b->tent;
-  p.lost = b->lost;
+  p.sw = reinterpret_cast<unsigned long long*>(b->sw);
+  p.ring = b->ring;
+  p.ring_mask = b->ring_slots ? (uint32_t)(b->ring_slots - 1) : 0u;
+  p.rq_head = b->rq;
+  p.rq_tail = b->rq + 32;
+  p.rq_done = b->rq + 64;
+  p.rq_stat = reinterpret_cast<unsigned long long*>(b->rq + 96);
   p.aff = b->aff;
   p.inq[0] = b->inq[0];
   p.inq[1] = b->inq[1];
@@ -1122,6 +1297,7 @@ int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac) {
       cudaMalloc(&b->trace, 2 * (kTraceLevels + 1) * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&b->barrier, vxb::kBarrierWords * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&b->features, 64 * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&b->rq, 128 * sizeof(uint32_t)) != cudaSuccess ||
       cudaMallocHost(&b->hctr, sizeof(BfsCounters)) != cudaSuccess) {
     set_error("BFS counter allocation failed");
     bfs_destroy(b);
@@ -1129,6 +1305,7 @@ int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac) {
   }
   cudaMemsetAsync(b->ctr, 0, sizeof(BfsCounters), g->stream);
   cudaMemsetAsync(b->barrier, 0, vxb::kBarrierWords * sizeof(uint32_t), g->stream);
+  cudaMemsetAsync(b->rq, 0, 128 * sizeof(uint32_t), g->stream);
   memset(b->hctr, 0, sizeof(BfsCounters));
   if (int rc = bfs_recompute(b)) {
     bfs_destroy(b);
@@ -1142,12 +1319,14 @@ void bfs_destroy(Bfs* b) {
   if (!b) return;
   if (b->g && b->g->stream) cudaStreamSynchronize(b->g->stream);
   uint32_t* ptrs[] = {b->dist, b->vis, b->fb[0], b->fb[1], b->fb[2], b->q[0], b->q[1], b->q[2], b->big,
-                      b->lst_a, b->lst_t, b->old, b->tent, b->lost, b->aff, b->inq[0], b->inq[1]};
+                      b->lst_a, b->lst_t, b->tent, b->sw, b->aff, b->inq[0], b->inq[1]};
   for (uint32_t* p : ptrs) cudaFree(p);
   cudaFree(b->ctr);
   cudaFree(b->trace);
   cudaFree(b->barrier);
   cudaFree(b->features);
+  cudaFree(b->rq);
+  cudaFree(b->ring);
   cudaFreeHost(b->hctr);
   delete b;
 }
@@ -1176,8 +1355,10 @@ int bfs_stage(Bfs* b, size_t n, size_t vertex_bound) {
   b->staged_len_pre = b->dist_len;
   if (n == 0) return 0;
   VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->cand_n, 0, 3 * sizeof(uint32_t), s));
+  VX_CUDA_TRY(cudaMemsetAsync(b->ctr->rtrace, 0, sizeof(b->ctr->rtrace), s));
   if (int rc = graph_stage_batch(g, n, vertex_bound)) return rc;
-  return ensure_capacity(b, std::max<size_t>(g->V, 1));
+  if (int rc = ensure_capacity(b, std::max<size_t>(g->V, 1))) return rc;
+  return ensure_ring(b);
 }
 
 int bfs_repair_staged(Bfs* b) {
@@ -1255,6 +1436,14 @@ int bfs_level_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n) {
   *n = 2 * ((size_t)levels + 1);
   const size_t m = std::min(cap, *n);
   if (out && m) VX_CUDA_TRY(cudaMemcpy(out, b->trace, m * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int bfs_phase_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n) {
+  if (int rc = bfs_sync(b)) return rc;
+  constexpr size_t kN = sizeof(b->hctr->rtrace) / sizeof(b->hctr->rtrace[0]);
+  *n = kN;
+  for (size_t i = 0; i < std::min(cap, kN); ++i) out[i] = b->hctr->rtrace[i];
   return 0;
 }
 }  // namespace vxh

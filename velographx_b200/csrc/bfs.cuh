@@ -23,17 +23,17 @@ struct BfsCounters {
   uint32_t lvl_big[3];
   unsigned long long lvl_m[3];
   // repair bookkeeping
-  uint32_t cand_n;       // deletion candidates list length
-  uint32_t touched_n;    // vertices whose lost counter is non-zero
+  uint32_t cand_n;       // deletion candidates (distinct heads)
+  uint32_t touched_n;    // vertices whose support word is non-zero (lst_t)
   uint32_t a_n;          // affected list length
-  uint32_t list_n[3];    // rotating frontier lists of the repair loops
-  uint32_t next_seed[3]; // smallest pending seed level (rotating)
-  uint32_t seed_min;     // smallest seed level of the settle phase
   unsigned long long scratch64;  // single-value readbacks
-  // rows of at least large_row arcs met by the repair loops, deferred to a
-  // pass of the whole grid (two rotating triples: a loop step has two phases)
-  uint32_t big_n[3];
-  uint32_t big_t[3];
+  // globaltimer stamps of the last repair: pre entry, after its seeds, after
+  // its cascade; post entry, after the boundary distances, after its seeds,
+  // after the relaxation; then the items pushed by the cascade and by the
+  // relaxation; then the drain statistics of the cascade and of the
+  // relaxation (claims, failed claims, idle rounds, slot waits, cycles
+  // spent processing summed over blocks, and the longest processing round)
+  unsigned long long rtrace[21];
 };
 
 struct BfsTuning {
@@ -55,9 +55,11 @@ struct Bfs {
   uint32_t* big = nullptr;
   uint32_t* lst_a = nullptr;  // affected list
   uint32_t* lst_t = nullptr;  // touched (lost > 0) list
-  uint32_t* old = nullptr;    // pre-repair distance of each affected entry
   uint32_t* tent = nullptr;   // boundary seed distance of each affected entry
-  uint32_t* lost = nullptr;   // lost-parent counters (zero between batches)
+  uint32_t* sw = nullptr;     // 64-bit support words, as pairs of u32 (zero between batches)
+  unsigned long long* ring = nullptr;  // work ring of the repair phases (ring_slots, a power of two)
+  size_t ring_slots = 0;
+  uint32_t* rq = nullptr;     // ring counters head / tail / done, one 128-byte line each
   uint32_t* aff = nullptr;    // affected bitmap (zero between batches)
   uint32_t* inq[2] = {nullptr, nullptr};  // queued bitmaps of the decrease propagation
   BfsCounters* ctr = nullptr;
@@ -86,5 +88,6 @@ int bfs_reached_arcs(Bfs* b, unsigned long long* arcs);  // sum of degrees of re
 // Per-level trace of the last full BFS: pairs {globaltimer ns, n_f | bottom_up << 63}
 // for every level, then a closing timestamp.  Writes up to cap u64 values.
 int bfs_level_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n);
+int bfs_phase_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n);
 
 }  // namespace vxh

@@ -313,6 +313,11 @@ int vx_bfs_reached_arcs(vx_bfs* b, uint64_t* out) {
   return VX_OK;
 }
 
+int vx_bfs_phase_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n) {
+  if (!b || !n || (cap && !out)) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::bfs_phase_trace(b->b, reinterpret_cast<unsigned long long*>(out), cap, n);
+}
+
 int vx_bfs_level_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n) {
   if (!b || !n) return fail(VX_ERR_INVALID, "null argument");
   return vxh::bfs_level_trace(b->b, reinterpret_cast<unsigned long long*>(out), cap, n);

@@ -343,8 +343,9 @@ __device__ uint32_t warp_bases_1024(uint32_t warp_count, uint32_t* wsum, uint32_
   return wsum[warp];
 }
 
-// Warp w owns items [w * 1024, (w + 1) * 1024) and reads them in 32 coalesced
-// rounds; ballots give each selected item its position inside the warp.
+// Round r takes items [r * 1024, (r + 1) * 1024), one per thread, so a list
+// of F canonical arcs costs ceil(F / 1024) rounds of coalesced loads; ballots
+// and a block scan of the warp counts give each selected item its position.
 __global__ void __launch_bounds__(kListThreads) build_list_kernel(const uint32_t* fu, const uint32_t* fv,
                                                                    const uint8_t* ff, const uint32_t* count,
                                                                    int mode, uint32_t* lu, uint32_t* lv,
@@ -352,43 +353,37 @@ __global__ void __launch_bounds__(kListThreads) build_list_kernel(const uint32_t
                                                                    uint32_t* nruns) {
   __shared__ uint32_t wsum[32];
   __shared__ uint32_t total;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t F = *count;
-  const uint32_t w0 = (uint32_t)warp * 32 * kListItems;
   auto selected = [&](uint32_t i) {
     if (i >= F) return false;
     const uint8_t f = ff[i];
     return !(f & kFInBase) && (f & kFChanged) && (((f & kFAdd) != 0) == (mode == 1));
   };
-  uint32_t cnt = 0;
-  for (int r = 0; r < kListItems; ++r) cnt += __popc(__ballot_sync(0xFFFFFFFFu, selected(w0 + r * 32 + lane)));
-  uint32_t pos = warp_bases_1024(cnt, wsum, &total);
-  const uint32_t n = total;
-  for (int r = 0; r < kListItems; ++r) {
-    const uint32_t i = w0 + r * 32 + lane;
+  uint32_t n = 0;
+  for (uint32_t r0 = 0; r0 < F; r0 += kListThreads) {
+    const uint32_t i = r0 + threadIdx.x;
     const bool sel = selected(i);
     const uint32_t m = __ballot_sync(0xFFFFFFFFu, sel);
+    const uint32_t wb = warp_bases_1024(__popc(m), wsum, &total);
     if (sel) {
-      const uint32_t o = pos + __popc(m & vxb::lanemask_lt());
+      const uint32_t o = n + wb + __popc(m & vxb::lanemask_lt());
       lu[o] = fu[i];
       lv[o] = fv[i];
     }
-    pos += __popc(m);
+    n += total;
   }
   if (threadIdx.x == 0) *nlist = n;
   __syncthreads();  // the compacted list is visible to the whole block
-  auto starts = [&](uint32_t k) { return k < n && (k == 0 || lu[k] != lu[k - 1]); };
-  cnt = 0;
-  for (int r = 0; r < kListItems; ++r) cnt += __popc(__ballot_sync(0xFFFFFFFFu, starts(w0 + r * 32 + lane)));
-  pos = warp_bases_1024(cnt, wsum, &total);
-  for (int r = 0; r < kListItems; ++r) {
-    const uint32_t k = w0 + r * 32 + lane;
-    const bool st = starts(k);
+  uint32_t nr = 0;
+  for (uint32_t r0 = 0; r0 < n; r0 += kListThreads) {
+    const uint32_t k = r0 + threadIdx.x;
+    const bool st = k < n && (k == 0 || lu[k] != lu[k - 1]);
     const uint32_t m = __ballot_sync(0xFFFFFFFFu, st);
-    if (st) runs[pos + __popc(m & vxb::lanemask_lt())] = k;
-    pos += __popc(m);
+    const uint32_t wb = warp_bases_1024(__popc(m), wsum, &total);
+    if (st) runs[nr + wb + __popc(m & vxb::lanemask_lt())] = k;
+    nr += total;
   }
-  if (threadIdx.x == 0) *nruns = total;
+  if (threadIdx.x == 0) *nruns = nr;
 }
 
 // One warp per row run: drop the run's arcs from the row's sorted delta list

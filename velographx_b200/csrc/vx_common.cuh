@@ -32,6 +32,7 @@ constexpr uint32_t kErrBarrierTimeout = 1u << 0;
 constexpr uint32_t kErrLoopBound = 1u << 1;
 constexpr uint32_t kErrArenaOverflow = 1u << 2;
 constexpr uint32_t kErrBadVertex = 1u << 3;
+constexpr uint32_t kErrDrainTimeout = 1u << 4;  // a repair work ring stopped draining
 constexpr uint32_t kErrQueueOverflow = 1u << 4;
 
 struct DevAdj {

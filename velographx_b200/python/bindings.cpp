@@ -256,6 +256,15 @@ PYBIND11_MODULE(_velographx, m) {
              detail::check(vx_bfs_reached_arcs(x.handle(), &a));
              return a;
            })
+      .def("phase_trace",
+           [](IncrementalBFS& x) {
+             std::uint64_t t[32] = {};
+             std::size_t n = 0;
+             detail::check(vx_bfs_phase_trace(x.handle(), t, 32, &n));
+             py::list out;
+             for (std::size_t i = 0; i < n && i < 32; ++i) out.append(t[i]);
+             return out;
+           })
       .def("level_trace",
            [](IncrementalBFS& x) {
              std::size_t n = 0;
