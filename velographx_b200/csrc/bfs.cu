@@ -57,6 +57,7 @@ struct Params {
   uint32_t* rq_head;       // ring counters, each on its own 128-byte line: the
   uint32_t* rq_tail;       // idle blocks poll them while the working ones push
   uint32_t* rq_done;
+  uint32_t* rq_fin;        // set by the first block that sees the phase finished
   unsigned long long* rq_stat;  // drain statistics of the last phase (own line)
   uint32_t* aff;
   uint32_t* inq[2];
@@ -607,7 +608,8 @@ struct RepairSmem {
 // the current one is used up.  Indices past the tail belong to whichever
 // block holds them, so pushes spread over the blocks waiting for work, and no
 // two blocks poll the same address.  Every few idle rounds a block checks
-// done == tail and leaves the phase.
+// done == tail; the first to see it raises rq_fin, which the other idle
+// blocks read every round, and all leave the phase.
 constexpr uint32_t kClaim = 32;
 
 template <class W>
@@ -641,13 +643,17 @@ __device__ void drain(const Params& p, RepairSmem& sm, W& w) {
           __stcg(&p.ring[k & p.ring_mask], kSent);
         }
         cur += n;
-        if (n == 0 && (idle & 7) == 7) {
+        if (n == 0) {
           uint32_t st = 0;
           if (lane == 0) {
-            const uint32_t dn = ld_cg(p.rq_done);
-            __threadfence();
-            st = dn == ld_cg(p.rq_tail);
-            atomicAdd(&p.rq_stat[3], 1ull);
+            st = ld_cg(p.rq_fin);
+            if (!st && (idle & 3) == 3) {
+              const uint32_t dn = ld_cg(p.rq_done);
+              __threadfence();
+              st = dn == ld_cg(p.rq_tail);
+              if (st) atomicExch(p.rq_fin, 1u);  // releases the other blocks at their next idle round
+              atomicAdd(&p.rq_stat[3], 1ull);
+            }
           }
           stop = __shfl_sync(FULL, st, 0);
         }
@@ -667,7 +673,7 @@ __device__ void drain(const Params& p, RepairSmem& sm, W& w) {
         if (threadIdx.x == 0) atomicOr(&c->err, vxb::kErrDrainTimeout);
         break;
       }
-      __nanosleep(32u << min(idle >> 2, 5u));  // back off to 1 us
+      __nanosleep(32u << min(idle >> 2, 4u));  // back off to 512 ns
       continue;
     }
     idle = 0;
@@ -942,6 +948,7 @@ __device__ void reset_ring(const Params& p) {
     *p.rq_head = 0;
     *p.rq_tail = 0;
     *p.rq_done = 0;
+    *p.rq_fin = 0;
     for (int k = 0; k < 6; ++k) p.rq_stat[k] = 0;
   }
 }
@@ -1252,6 +1259,7 @@ static Params make_params(Bfs* b, uint32_t V, uint32_t dist_len) {
   p.rq_head = b->rq;
   p.rq_tail = b->rq + 32;
   p.rq_done = b->rq + 64;
+  p.rq_fin = b->rq + 128;
   p.rq_stat = reinterpret_cast<unsigned long long*>(b->rq + 96);
   p.aff = b->aff;
   p.inq[0] = b->inq[0];
@@ -1297,7 +1305,7 @@ int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac) {
       cudaMalloc(&b->trace, 2 * (kTraceLevels + 1) * sizeof(unsigned long long)) != cudaSuccess ||
       cudaMalloc(&b->barrier, vxb::kBarrierWords * sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&b->features, 64 * sizeof(float)) != cudaSuccess ||
-      cudaMalloc(&b->rq, 128 * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&b->rq, 160 * sizeof(uint32_t)) != cudaSuccess ||
       cudaMallocHost(&b->hctr, sizeof(BfsCounters)) != cudaSuccess) {
     set_error("BFS counter allocation failed");
     bfs_destroy(b);
@@ -1305,7 +1313,7 @@ int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac) {
   }
   cudaMemsetAsync(b->ctr, 0, sizeof(BfsCounters), g->stream);
   cudaMemsetAsync(b->barrier, 0, vxb::kBarrierWords * sizeof(uint32_t), g->stream);
-  cudaMemsetAsync(b->rq, 0, 128 * sizeof(uint32_t), g->stream);
+  cudaMemsetAsync(b->rq, 0, 160 * sizeof(uint32_t), g->stream);
   memset(b->hctr, 0, sizeof(BfsCounters));
   if (int rc = bfs_recompute(b)) {
     bfs_destroy(b);

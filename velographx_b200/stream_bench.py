@@ -1,0 +1,150 @@
+"""Update-stream measurements beyond the headline benchmark.
+
+``grid``       4096 x 4096 lattice (4-neighbour) + 0.1% seeded long-range
+               edges, root at corner 0, batches of 1,000 ops with half of them
+               deletions drawn from the edges nearest the root (the ones whose
+               endpoints have the smallest distances) -- deep subtree
+               invalidation and repair.
+``lognormal``  R-MAT scale 20 with update batches of lognormal sizes (median
+               500 ops, sigma 2, clipped to [1, 200000]; 80% insertions),
+               applied one batch at a time through the public API, each
+               batch's host arrays copied in and the stream synchronised per
+               batch.
+
+Every run times batches with CUDA events on the graph's stream and checks the
+maintained distances against a fresh full BFS at regular batches.
+
+  python -m velographx_b200.stream_bench --workload grid [--batches 500]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+import time
+
+import numpy as np
+
+from . import Graph, IncrementalBFS
+from . import workloads as w
+
+
+def _events():
+    import torch
+
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def near_root_stream(edges: np.ndarray, vertices: int, dist: np.ndarray, batches: int, ops: int,
+                     delete_fraction: float, seed: int) -> w.Stream:
+    """Batches of `ops` updates: round(ops * delete_fraction) deletions of edges
+    drawn at random from the 2x-sized pool of edges nearest the root (by the
+    larger endpoint distance), the rest uniform-random insertions; each batch
+    shuffled."""
+    rng = np.random.default_rng(seed)
+    e = edges[edges[:, 0] != edges[:, 1]]
+    nd = int(round(ops * delete_fraction))
+    total = nd * batches
+    key = np.maximum(dist[e[:, 0]].astype(np.uint64), dist[e[:, 1]].astype(np.uint64))
+    pool = np.argsort(key, kind="stable")[: min(e.shape[0], 2 * total)]
+    pick = rng.choice(pool, size=total, replace=total > pool.size)
+    ni = ops - nd
+    src = np.empty(batches * ops, np.uint32)
+    dst = np.empty(batches * ops, np.uint32)
+    add = np.empty(batches * ops, np.uint8)
+    for b in range(batches):
+        s = np.concatenate([e[pick[b * nd:(b + 1) * nd], 0], rng.integers(0, vertices, ni, dtype=np.uint32)])
+        d = np.concatenate([e[pick[b * nd:(b + 1) * nd], 1], rng.integers(0, vertices, ni, dtype=np.uint32)])
+        a = np.concatenate([np.zeros(nd, np.uint8), np.ones(ni, np.uint8)])
+        perm = rng.permutation(ops)
+        lo = b * ops
+        src[lo:lo + ops], dst[lo:lo + ops], add[lo:lo + ops] = s[perm], d[perm], a[perm]
+    offsets = np.arange(batches + 1, dtype=np.int64) * ops
+    return w.Stream(src, dst, add, offsets)
+
+
+def run_stream(g: Graph, bfs: IncrementalBFS, root: int, stream: w.Stream, check_every: int) -> dict:
+    """Device-resident batches (apply_device), timed back to back with events
+    between batches; exactness against a fresh full BFS every check_every
+    batches (outside the timed spans)."""
+    import torch
+
+    V = g.vertex_count
+    cs = torch.cuda.ExternalStream(g.stream)
+    ds = torch.from_numpy(stream.src.view(np.int32)).cuda()
+    dd = torch.from_numpy(stream.dst.view(np.int32)).cuda()
+    da = torch.from_numpy(stream.add).cuda()
+    torch.cuda.synchronize()
+    per, fallbacks, affected, exact, checked = [], 0, [], True, 0
+    nb = stream.batches
+    k = 0
+    while k < nb:
+        seg = min(nb, (k // check_every + 1) * check_every) if check_every else nb
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(seg - k + 1)]
+        ev[0].record(cs)
+        for i in range(k, seg):
+            lo, hi = int(stream.offsets[i]), int(stream.offsets[i + 1])
+            bfs.apply_device(ds.data_ptr() + 4 * lo, dd.data_ptr() + 4 * lo, da.data_ptr() + lo, hi - lo, V)
+            ev[i - k + 1].record(cs)
+        torch.cuda.synchronize()
+        per += [ev[j].elapsed_time(ev[j + 1]) * 1e3 for j in range(seg - k)]
+        st = bfs.stats()
+        fallbacks += int(st["last_used_full_recompute"])
+        affected.append(st["last_affected_vertices"])
+        if check_every:
+            fresh = IncrementalBFS(g, root)
+            same = np.array_equal(fresh.distances_array(), bfs.distances_array())
+            exact = exact and same and fresh.reachable_count == bfs.reachable_count
+            checked += 1
+            del fresh
+        k = seg
+    per = np.asarray(per)
+    return {"batches": nb, "seconds": float(per.sum() * 1e-6), "batches_per_s": float(nb / (per.sum() * 1e-6)),
+            "us_median": float(np.median(per)), "us_p90": float(np.percentile(per, 90)), "us_max": float(per.max()),
+            "exact": bool(exact), "exact_checks": checked}
+
+
+def grid(side: int = 4096, long_range: float = 0.001, batches: int = 500, ops: int = 1000,
+         delete_fraction: float = 0.5, seed: int = 44, check_every: int = 50) -> dict:
+    import torch
+
+    edges = w.grid_edges(side, side, long_range, seed=seed)
+    V = side * side
+    g = Graph(V, False)
+    g.bulk_load_edges(edges)
+    root = 0
+    bfs = IncrementalBFS(g, root)
+    cs = torch.cuda.ExternalStream(g.stream)
+    e0, e1 = _events()
+    torch.cuda.synchronize()
+    e0.record(cs)
+    bfs.recompute()
+    e1.record(cs)
+    e1.synchronize()
+    full_ms = e0.elapsed_time(e1)
+    levels = bfs.stats()["levels"]
+    stream = near_root_stream(edges, V, bfs.distances_array(), batches, ops, delete_fraction, seed + 1)
+    res = run_stream(g, bfs, root, stream, check_every)
+    res.update({"workload": f"grid{side}x{side}+{long_range:g}-long-range-root0-{ops}-op-batches-"
+                            f"{int(delete_fraction * 100)}pct-near-root-deletions",
+                "vertices": V, "arcs": int(g.edge_count_directed()), "full_bfs_ms": full_ms,
+                "full_bfs_levels": int(levels)})
+    return res
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--workload", choices=["grid"], default="grid")
+    ap.add_argument("--side", type=int, default=4096)
+    ap.add_argument("--batches", type=int, default=500)
+    ap.add_argument("--ops", type=int, default=1000)
+    ap.add_argument("--check-every", type=int, default=50)
+    a = ap.parse_args()
+    t0 = time.time()
+    res = grid(a.side, batches=a.batches, ops=a.ops, check_every=a.check_every)
+    res["wall_s"] = time.time() - t0
+    print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    sys.exit(main())
