@@ -122,15 +122,35 @@ int vx_bfs_reached_arcs(vx_bfs* b, uint64_t* out);
  * frontier size | bottom_up << 63}, then a closing timestamp; *n = entries.
  * No reference counterpart (diagnostics). */
 int vx_bfs_level_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
-/* Phase trace of the last incremental apply (21 entries): globaltimer ns at
+/* Phase trace of the last incremental apply (27 entries): globaltimer ns at
  * the pre-batch kernel's entry, after its seeds, after its cascade; at the
  * post-batch kernel's entry, after the boundary distances, after its seeds,
  * after the relaxation (0 = phase not run); the work items pushed by the
  * cascade and by the relaxation; then, for the cascade and the relaxation,
  * the work-ring processing rounds, tickets, idle rounds, termination checks,
- * SM cycles spent processing (summed over blocks) and the longest round.
- * No reference counterpart (diagnostics). */
+ * SM cycles spent processing (summed over blocks) and the longest round;
+ * then the ns the last vx_bfs_apply_stream launch spent in each per-batch
+ * phase (classify, removals, cascade, insertions, post-batch repair,
+ * end-of-batch barrier), summed over its batches.  No reference counterpart
+ * (diagnostics). */
 int vx_bfs_phase_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
+/* A stream of update batches applied in order, with the same result after
+ * every batch as vx_bfs_apply on each: batch t is ops [offsets[t],
+ * offsets[t+1]) of the host arrays (offsets[0] == 0, nbatches + 1 entries).
+ * Undirected graphs run the whole stream in one persistent launch after one
+ * upload and one stream-wide canonicalisation; other streams are applied
+ * batch by batch.  Optional host outputs: digests[t] = vx_bfs_digest after
+ * batch t; stats[4t..4t+3] = {last_deletion_candidates,
+ * last_affected_vertices, last_used_full_recompute, reachable_count mod
+ * 2^32} after batch t.  The reference applies batches one call at a time
+ * (bfs.hpp:29-98); this entry has no counterpart there. */
+int vx_bfs_apply_stream(vx_bfs* b, const uint32_t* src, const uint32_t* dst, const uint8_t* add,
+                        const uint64_t* offsets, size_t nbatches, uint64_t* digests, uint32_t* stats);
+/* Order-independent 64-bit digest of the current distances: the sum over v of
+ * splitmix64((v << 32) | dist[v]) modulo 2^64 (splitmix64: add
+ * 0x9E3779B97F4A7C15, then the two xor-shift-multiply rounds and the final
+ * xor-shift of Steele et al.).  No reference counterpart (verification). */
+int vx_bfs_digest(vx_bfs* b, uint64_t* out);
 /* Direction switch (alpha, beta) and grid-expanded row length of the full BFS.
  * No reference counterpart: the reference BFS is top-down only. */
 int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row);

@@ -20,8 +20,10 @@
 //              relaxation from them and from the heads of inserted arcs.
 #include <algorithm>
 #include <cstring>
+#include <vector>
 
 #include "bfs.cuh"
+#include "graph_dev.cuh"
 #include "frontier.cuh"
 
 namespace vxh {
@@ -957,35 +959,56 @@ __device__ __forceinline__ void stamp(const Params& p, int k) {
   if (gtid() == 0) p.c->rtrace[k] = globaltimer();
 }
 
-__device__ void repair_pre(const Params& p, RepairSmem& sm, LbStage& lb) {
+// Deletion candidates (bfs.hpp:52-63): heads of deleted shortest-parent arcs.
+// The first touch of each records it in the touched list, so the list's
+// first cand_n entries are the candidates.  Warp-uniform.
+__device__ void register_candidates(const Params& p) {
   BfsCounters* c = p.c;
   const int lane = threadIdx.x & 31;
-  stamp(p, 0);
-  reset_ring(p);
-  if (!sync_grid(p)) return;
-  // deletion candidates (bfs.hpp:52-63): heads of deleted shortest-parent
-  // arcs, each checked once
   const uint32_t F = *p.F;
   for (uint32_t base = gwarp() * 32; base < F; base += nwarps() * 32) {
     const uint32_t i = base + lane;
-    bool cand = false;
+    bool first = false;
     uint32_t v = 0;
     if (i < F) {
       const uint8_t f = p.ff[i];
       const uint32_t u = p.fu[i];
       v = p.fv[i];
-      cand = !(f & kFAdd) && (f & kFCur) && is_sp(p, u, v);
+      if (!(f & kFAdd) && (f & kFCur) && is_sp(p, u, v)) first = !(atomicOr(&p.sw[v], kSwTouched) & kSwTouched);
     }
-    request_check(p, cand, v, &c->cand_n);
+    const uint32_t slot = vxb::warp_append(first, &c->touched_n);
+    if (first) p.lst_t[slot] = v;
+    vxb::warp_append(first, &c->cand_n);
   }
+}
+
+// The cascade after the candidates are registered (and the batch's deletions
+// committed): every candidate is checked in place, one warp each; the ring
+// is drained only when a check left work in it (an affected vertex to expand,
+// chunks of a long in-row), which most small batches never do.
+__device__ bool cascade(const Params& p, RepairSmem& sm, LbStage& lb, uint32_t ncand) {
+  for (uint32_t i = gwarp(); i < ncand; i += nwarps()) check_vertex(p, p.lst_t[i]);
+  if (!sync_grid(p)) return false;
+  if (ld_cg(p.rq_tail)) {
+    Cascade w{&p, &lb};
+    drain(p, sm, w);
+    if (!sync_grid(p)) return false;
+  }
+  return true;
+}
+
+__device__ void repair_pre(const Params& p, RepairSmem& sm, LbStage& lb) {
+  BfsCounters* c = p.c;
+  stamp(p, 0);
+  reset_ring(p);
+  if (!sync_grid(p)) return;
+  register_candidates(p);
   if (!sync_grid(p)) return;
   stamp(p, 1);
   const uint32_t ncand = ld_cg(&c->cand_n);
   if (gtid() == 0) c->candidates = ncand;
   if (ncand == 0) return;
-  Cascade w{&p, &lb};
-  drain(p, sm, w);
-  if (!sync_grid(p)) return;
+  if (!cascade(p, sm, lb, ncand)) return;
   stamp(p, 2);
   if (gtid() == 0) {
     c->affected = ld_cg(&c->a_n);
@@ -1024,6 +1047,46 @@ __device__ __forceinline__ void lower_and_push(const Params& p, bool lowered, ui
     push = !(atomicOr(&p.inq[0][x >> 5], bit) & bit);
   }
   ring_push(p, push, x);
+}
+
+// Per-lane form of a queued push (any lane, no warp aggregation).
+__device__ __forceinline__ void push_one(const Params& p, uint32_t x) {
+  const uint32_t bit = 1u << (x & 31);
+  if (atomicOr(&p.inq[0][x >> 5], bit) & bit) return;
+  const uint32_t s = atomicAdd(p.rq_tail, 1u);
+  __stcg(&p.ring[s & p.ring_mask], (unsigned long long)x);
+}
+
+constexpr uint32_t kInlineRelax = 8;  // rows this short are relaxed where they are lowered
+
+// A seed v just lowered: a short row is relaxed here by its lane (the
+// vertices it lowers are queued), a longer one is queued.  Any later lowering
+// of v queues v again, so relaxing from the current label loses nothing.
+__device__ void seed_relax(const Params& p, bool lowered, uint32_t v, long long& reach) {
+  bool queue = false;
+  if (lowered) {
+    const DevAdj& a = p.g.out;
+    uint64_t b, e;
+    vxb::base_range(a, v, b, e);
+    const uint2 dr = a.drow[v];
+    const uint32_t deg = (uint32_t)(e - b) + dr.y;
+    if (deg > kInlineRelax) {
+      queue = true;
+    } else {
+      const uint32_t dv = ld_cg(&p.dist[v]);
+      for (uint32_t k = 0; k < deg; ++k) {
+        uint32_t x;
+        if (k < e - b) {
+          x = a.col[b + k];
+          if (x & kTomb) continue;
+        } else {
+          x = a.darena[dr.x + (k - (uint32_t)(e - b))];
+        }
+        if (x < p.dist_len && lower(p, x, dv + 1, reach)) push_one(p, x);
+      }
+    }
+  }
+  lower_and_push(p, queue, v);
 }
 
 // Label-correcting relaxation (the settle of repair_affected, bfs.hpp:272-310,
@@ -1084,7 +1147,7 @@ __device__ void boundary_seeds(const Params& p, RepairSmem& sm, LbStage& lb, uin
       // by atomicMin: an inserted arc may lower v first
       if (best != kUnreachable) seed = lower(p, v, best, reach);
     }
-    lower_and_push(p, seed, v);
+    seed_relax(p, seed, v, reach);
     __syncthreads();
   }
 }
@@ -1127,13 +1190,15 @@ __device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQ
         if (du != kUnreachable) lowered = lower(p, v, du + 1, reach);
       }
     }
-    lower_and_push(p, lowered, v);
+    seed_relax(p, lowered, v, reach);
   }
   if (!sync_grid(p)) return;
   stamp(p, 5);
-  Relax w{&p, &lb, &reach};
-  drain(p, sm, w);
-  if (!sync_grid(p)) return;
+  if (ld_cg(p.rq_tail)) {  // the relaxation runs only when a seed left work queued
+    Relax w{&p, &lb, &reach};
+    drain(p, sm, w);
+    if (!sync_grid(p)) return;
+  }
   stamp(p, 6);
   if (gtid() == 0) {
     c->rtrace[8] = ld_cg(p.rq_tail);
@@ -1145,6 +1210,262 @@ __device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQ
   reset_ring(p);
 }
 
+// ------------------------------------------------------- batched stream --
+//
+// A whole update stream applied in one persistent launch: the batches' canonical
+// arcs come sorted by (batch, u, v) from one stream-wide sort, and every batch
+// runs classify + tombstones, delta removals + deletion candidates, the
+// cascade, tombstone revivals + delta insertions, and the post-batch repair,
+// separated by grid barriers, with no launch or host synchronisation between
+// batches.  The result after every batch is the one IncrementalBFS::apply
+// gives (bfs.hpp:29-98); an optional per-batch digest of the distances and
+// per-batch counters make every batch checkable.
+
+struct StreamArgs {
+  const uint32_t* fu;        // canonical arcs of the stream, batch-major
+  const uint32_t* fv;
+  uint8_t* ff;               // in: desired state (bit 0); out: classification flags
+  uint64_t* fpos;
+  const uint32_t* boff;      // nb + 1 offsets of the batches' arcs
+  const uint32_t* bcnt;      // nb arc counts
+  const uint32_t* vpost;     // vertex count after each batch
+  uint32_t* scratch;         // one batch's arcs: the insertions of each row run
+  unsigned long long* digest;  // nb digests of the distances (optional)
+  uint32_t* bstats;          // nb x 4: candidates, affected, full recompute, reachable (optional)
+  GraphCounters* gc;
+  unsigned long long arena_cap;
+  double frac;
+  uint32_t nb, V0, len0;
+  uint32_t v_single;    // vertex count after the batch when vpost is null (one staged batch)
+  uint32_t classified;  // the arcs carry their classification already (a staged batch)
+};
+
+// Order-independent 64-bit digest of dist[0, n): sum of splitmix64(v << 32 | dist[v]).
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__device__ void digest_pass(const uint32_t* dist, uint32_t n, unsigned long long* out) {
+  unsigned long long h = 0;
+  for (uint32_t v = gtid(); v < n; v += nthreads()) h += mix64(((unsigned long long)v << 32) | ld_cg(&dist[v]));
+  h = vxb::warp_sum(h);
+  if ((threadIdx.x & 31) == 0 && h) atomicAdd(out, h);
+}
+
+// End of the row run of canonical arcs starting at s (same u), whole warp.
+__device__ __forceinline__ uint32_t run_end(const uint32_t* fu, uint32_t s, uint32_t F) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t u = fu[s];
+  for (uint32_t k = s + 1;; k += 32) {
+    const uint32_t i = k + lane;
+    const uint32_t m = __ballot_sync(FULL, i >= F || fu[i] != u);
+    if (m) return k + (uint32_t)(__ffs(m) - 1);
+  }
+}
+
+__device__ __forceinline__ bool delta_op(uint8_t f, bool insertion) {
+  return !(f & kFInBase) && (f & kFChanged) && (((f & kFAdd) != 0) == insertion);
+}
+
+// Delta removals of one row run (whole warp): the row's sorted delta list
+// keeps every entry that is not a removal of the run (delta_remove_kernel of
+// the per-batch path, on the canonical arcs directly).
+__device__ void run_remove(vxb::DevAdj& a, const uint32_t* fv, const uint8_t* ff, uint32_t s, uint32_t e, uint32_t u,
+                           GraphCounters* gc) {
+  const int lane = threadIdx.x & 31;
+  bool any = false;
+  for (uint32_t k = s + lane; k < e; k += 32) any |= delta_op(ff[k], false);
+  if (!__any_sync(FULL, any)) return;
+  const uint2 row = a.drow[u];
+  uint32_t* A = a.darena + row.x;
+  uint32_t written = 0;
+  for (uint32_t base = 0; base < row.y; base += 32) {
+    const uint32_t j = base + lane;
+    const bool in = j < row.y;
+    const uint32_t x = in ? A[j] : 0u;
+    bool keep = in;
+    if (in) {
+      const uint32_t q = vxb::lower_bound_u32(fv, s, e, x);
+      if (q < e && fv[q] == x && delta_op(ff[q], false)) keep = false;
+    }
+    const uint32_t mask = __ballot_sync(FULL, keep);
+    const uint32_t p = written + __popc(mask & vxb::lanemask_lt());
+    __syncwarp();
+    if (keep) A[p] = x;
+    written += __popc(mask);
+    __syncwarp();
+  }
+  if (lane == 0) {
+    a.drow[u].y = written;
+    atomicAdd(&gc->delta_live[0], (unsigned long long)(-(long long)(row.y - written)));
+    gdev::mark_dirty(a.dirty, u, &gc->dirty_rows[0]);
+  }
+}
+
+// Delta insertions of one row run (whole warp): the run's insertions are
+// compacted into scratch[s, s + nB) and merged into the row's delta list, in
+// place when its block has room, else into a new power-of-two arena block
+// (delta_insert_kernel of the per-batch path).
+__device__ void run_insert(vxb::DevAdj& a, const uint32_t* fv, const uint8_t* ff, uint32_t* scratch, uint32_t s,
+                           uint32_t e, uint32_t u, GraphCounters* gc, unsigned long long arena_cap) {
+  const int lane = threadIdx.x & 31;
+  uint32_t nB = 0;
+  for (uint32_t base = s; base < e; base += 32) {
+    const uint32_t k = base + lane;
+    const bool ins = k < e && delta_op(ff[k], true);
+    const uint32_t m = __ballot_sync(FULL, ins);
+    if (ins) scratch[s + nB + __popc(m & vxb::lanemask_lt())] = fv[k];
+    nB += __popc(m);
+  }
+  if (nB == 0) return;
+  __syncwarp();
+  const uint2 row = a.drow[u];
+  const uint32_t cap = a.dcap[u];
+  const uint32_t cnew = row.y + nB;
+  if (cnew <= cap) {
+    gdev::warp_merge_inplace(a.darena + row.x, row.y, scratch + s, nB);
+    if (lane == 0) a.drow[u].y = cnew;
+  } else {
+    uint32_t ncap = 8;
+    while (ncap < cnew) ncap <<= 1;
+    unsigned long long off = 0;
+    if (lane == 0) off = atomicAdd(&gc->arena_top[0], (unsigned long long)ncap);
+    off = __shfl_sync(FULL, off, 0);
+    if (off + ncap > arena_cap) {
+      if (lane == 0) atomicOr(&gc->err, vxb::kErrArenaOverflow);
+      return;
+    }
+    gdev::warp_merge_to(a.darena + off, a.darena + row.x, row.y, scratch + s, nB);
+    if (lane == 0) {
+      a.drow[u] = make_uint2((uint32_t)off, cnew);
+      a.dcap[u] = ncap;
+    }
+  }
+  if (lane == 0) {
+    atomicAdd(&gc->delta_live[0], (unsigned long long)nB);
+    gdev::mark_dirty(a.dirty, u, &gc->dirty_rows[0]);
+  }
+}
+
+// Every row run of the batch's canonical arcs [0, F): warp w takes arc
+// indices w, w + nwarps, ... and processes the run that starts at each (a
+// run start is an arc whose row differs from its predecessor's), so the runs
+// of a batch spread over all warps.
+template <bool kInsert>
+__device__ void for_each_run(const Params& p, const StreamArgs& s, uint32_t off, uint32_t F) {
+  vxb::DevAdj a = p.g.out;
+  const uint32_t* fu = s.fu + off;
+  const uint32_t* fv = s.fv + off;
+  const uint8_t* ff = s.ff + off;
+  for (uint32_t i = gwarp(); i < F; i += nwarps()) {
+    if (i > 0 && fu[i] == fu[i - 1]) continue;  // same load on every lane: warp-uniform
+    const uint32_t en = run_end(fu, i, F);
+    if (kInsert) run_insert(a, fv, ff, s.scratch, i, en, fu[i], s.gc, s.arena_cap);
+    else run_remove(a, fv, ff, i, en, fu[i], s.gc);
+  }
+}
+
+__device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm, LbStage& lb, BlockQueue& bq) {
+  BfsCounters* c = p.c;
+  const int lane = threadIdx.x & 31;
+  unsigned long long tmark = globaltimer();
+  auto phase = [&](int k) {  // gtid 0 accumulates the time since the previous mark
+    if (gtid() == 0) {
+      const unsigned long long now = globaltimer();
+      c->stream_ns[k] += now - tmark;
+      tmark = now;
+    }
+  };
+  if (gtid() == 0)
+    for (int k = 0; k < 6; ++k) c->stream_ns[k] = 0;
+  for (uint32_t bi = 0; bi < s.nb; ++bi) {
+    const uint32_t off = s.boff ? s.boff[bi] : 0u, F = s.bcnt[bi];
+    const uint32_t Vpre = bi ? s.vpost[bi - 1] : s.V0, lpre = bi ? s.vpost[bi - 1] : s.len0;
+    const uint32_t Vpost = s.vpost ? s.vpost[bi] : s.v_single;
+    Params q = p;
+    q.fu = s.fu + off;
+    q.fv = s.fv + off;
+    q.ff = s.ff + off;
+    q.F = &s.bcnt[bi];
+    q.V = Vpre;
+    q.dist_len = lpre;
+    const unsigned long long lim = (unsigned long long)((double)Vpre * s.frac);
+    q.fallback_limit = lim < 1 ? 1 : lim;
+    if (gtid() == 0) {  // last_* counters and the repair lists start empty (bfs.hpp:30-33)
+      c->candidates = c->affected = c->full = c->fallback = 0;
+      c->cand_n = c->touched_n = c->a_n = 0;
+    }
+    stamp(q, 0);
+    // A: classification against the pre-batch graph; tombstone the deleted base arcs
+    {
+      vxb::DevAdj a = p.g.out;
+      long long tombs = 0;
+      for (uint32_t i = gtid(); i < F; i += nthreads()) {
+        uint8_t f = s.ff[off + i];
+        if (!s.classified) {
+          f = gdev::classify_arc(a, s.fu[off + i], s.fv[off + i], f, s.fpos[off + i]);
+          s.ff[off + i] = f;
+        }
+        tombs += gdev::tomb_arc(a, s.fu[off + i], f, s.fpos[off + i], 0, &s.gc->dirty_rows[0]);
+      }
+      tombs = vxb::warp_sum(tombs);
+      if (lane == 0 && tombs) atomicAdd(&s.gc->tombs[0], (unsigned long long)tombs);
+      if (s.digest && bi > 0) digest_pass(p.dist, lpre, &s.digest[bi - 1]);
+    }
+    if (!sync_grid(p)) return;
+    phase(0);
+    // B: delta removals; deletion candidates registered
+    for_each_run<false>(q, s, off, F);
+    register_candidates(q);
+    if (!sync_grid(p)) return;
+    phase(1);
+    stamp(q, 1);
+    // C: the cascade over the graph without the batch's deletions
+    const uint32_t ncand = ld_cg(&c->cand_n);
+    if (gtid() == 0) c->candidates = ncand;
+    if (ncand) {
+      if (!cascade(q, sm, lb, ncand)) return;
+      if (gtid() == 0) c->affected = ld_cg(&c->a_n);
+      reset_ring(q);
+    }
+    phase(2);
+    stamp(q, 2);
+    // D: revive re-added base arcs, delta insertions; new vertices start unreachable
+    {
+      vxb::DevAdj a = p.g.out;
+      long long tombs = 0;
+      for (uint32_t i = gtid(); i < F; i += nthreads())
+        tombs += gdev::tomb_arc(a, s.fu[off + i], s.ff[off + i], s.fpos[off + i], 1, &s.gc->dirty_rows[0]);
+      tombs = vxb::warp_sum(tombs);
+      if (lane == 0 && tombs) atomicAdd(&s.gc->tombs[0], (unsigned long long)tombs);
+      for (uint32_t v = lpre + gtid(); v < Vpost; v += nthreads()) p.dist[v] = kUnreachable;
+    }
+    for_each_run<true>(q, s, off, F);
+    if (!sync_grid(p)) return;
+    phase(3);
+    // E: the post-batch repair (or the fallback full BFS) on the new graph
+    q.V = Vpost;
+    q.dist_len = Vpost;
+    repair_post(q, sm, lb, bq);
+    if (ld_cg(&c->err)) return;
+    phase(4);
+    // every block's counter updates are in before they are recorded, and
+    // recorded before the next batch resets them (same thread)
+    if (!sync_grid(p)) return;
+    phase(5);
+    if (gtid() == 0 && s.bstats) {
+      s.bstats[4 * bi + 0] = ld_cg(&c->candidates);
+      s.bstats[4 * bi + 1] = ld_cg(&c->affected);
+      s.bstats[4 * bi + 2] = ld_cg(&c->full);
+      s.bstats[4 * bi + 3] = (uint32_t)__ldcg(&c->reachable);
+    }
+  }
+  if (s.digest && s.nb) digest_pass(p.dist, s.vpost[s.nb - 1], &s.digest[s.nb - 1]);
+}
+
 __global__ void __launch_bounds__(kThreads, 3) bfs_kernel(Params p, int mode) {
   __shared__ BlockQueue bq;
   __shared__ LbStage lb;
@@ -1153,6 +1474,90 @@ __global__ void __launch_bounds__(kThreads, 3) bfs_kernel(Params p, int mode) {
   else if (mode == kModePre) repair_pre(p, sm, lb);
   else repair_post(p, sm, lb, bq);
 }
+
+__global__ void __launch_bounds__(kThreads, 2) bfs_stream_kernel(Params p, StreamArgs s) {
+  __shared__ BlockQueue bq;
+  __shared__ LbStage lb;
+  __shared__ RepairSmem sm;
+  stream_kernel_body(p, s, sm, lb, bq);
+}
+
+// Stream canonicalisation: both arcs of every non-self-loop op keyed by
+// (batch, u, v) with the op's stream index as the value; a stable sort then
+// leaves each batch's ops for one arc in order, and the last one wins.
+__global__ void stream_keys_kernel(const uint32_t* src, const uint32_t* dst, const uint8_t* add,
+                                   const uint64_t* boff, uint32_t nb, size_t n, int b, uint64_t* keys,
+                                   uint32_t* vals) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = nb;  // the batch t with boff[t] <= i < boff[t + 1]
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (boff[mid] <= i) lo = mid;
+      else hi = mid;
+    }
+    const uint64_t t = (uint64_t)lo << (2 * b);
+    const uint32_t u = src[i], v = dst[i];
+    const uint32_t val = ((uint32_t)i << 1) | (add[i] ? 1u : 0u);
+    const bool ok = u != v;
+    keys[2 * i] = ok ? (t | ((uint64_t)u << b) | v) : ~0ull;
+    keys[2 * i + 1] = ok ? (t | ((uint64_t)v << b) | u) : ~0ull;
+    vals[2 * i] = val;
+    vals[2 * i + 1] = val;
+  }
+}
+
+__global__ void stream_last_kernel(const uint64_t* keys, size_t m, uint32_t* flag) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    flag[i] = (k != ~0ull) && (i + 1 == m || keys[i + 1] != k);
+  }
+}
+
+__global__ void stream_compact_kernel(const uint64_t* keys, const uint32_t* vals, const uint32_t* flag,
+                                      const uint32_t* pos, size_t m, int b, uint32_t* fu, uint32_t* fv, uint8_t* ff,
+                                      uint32_t* bid) {
+  const uint64_t mask = ((uint64_t)1 << b) - 1;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
+    if (!flag[i]) continue;
+    const uint32_t q = pos[i];
+    const uint64_t k = keys[i];
+    fu[q] = (uint32_t)((k >> b) & mask);
+    fv[q] = (uint32_t)(k & mask);
+    ff[q] = (uint8_t)(vals[i] & 1u);
+    bid[q] = (uint32_t)(k >> (2 * b));
+  }
+}
+
+// boff[t] = first canonical arc of batch t (t <= nb), bcnt[t] = its arc count.
+__global__ void stream_bounds_kernel(const uint32_t* bid, const uint32_t* total, uint32_t nb, uint32_t* boff,
+                                     uint32_t* bcnt) {
+  const uint32_t F = *total;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t <= nb; t += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = F;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (bid[mid] < t) lo = mid + 1;
+      else hi = mid;
+    }
+    boff[t] = lo;
+    uint32_t lo2 = lo, hi2 = F;
+    while (lo2 < hi2) {
+      const uint32_t mid = (lo2 + hi2) >> 1;
+      if (bid[mid] <= t) lo2 = mid + 1;
+      else hi2 = mid;
+    }
+    if (t < nb) bcnt[t] = lo2 - lo;
+  }
+}
+
+__global__ void digest_kernel(const uint32_t* dist, uint32_t n, unsigned long long* out) {
+  unsigned long long h = 0;
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+    h += mix64(((unsigned long long)v << 32) | dist[v]);
+  h = vxb::warp_sum(h);
+  if ((threadIdx.x & 31) == 0 && h) atomicAdd(out, h);
+}
+
 
 __global__ void reached_arcs_kernel(vxb::DevAdj a, const uint32_t* dist, uint32_t n,
                                     unsigned long long* out) {
@@ -1335,6 +1740,7 @@ void bfs_destroy(Bfs* b) {
   cudaFree(b->features);
   cudaFree(b->rq);
   cudaFree(b->ring);
+  b->sb.free_all();
   cudaFreeHost(b->hctr);
   delete b;
 }
@@ -1369,10 +1775,60 @@ int bfs_stage(Bfs* b, size_t n, size_t vertex_bound) {
   return ensure_ring(b);
 }
 
+static int launch_stream(Bfs* b, Params& p, StreamArgs& sa) {
+  if (!b->stream_grid) {
+    int per_sm = 0;
+    VX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_stream_kernel, kThreads, 0));
+    if (per_sm < 1) {
+      set_error("stream kernel cannot be resident on an SM");
+      return -3;
+    }
+    b->stream_grid = per_sm * sm_count();
+  }
+  p.nblocks = (uint32_t)b->stream_grid;
+  void* args[] = {&p, &sa};
+  count_launch();
+  VX_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)bfs_stream_kernel, dim3(b->stream_grid), dim3(kThreads), args,
+                                          0, b->g->stream));
+  return 0;
+}
+
+// The staged batch of an undirected graph as a one-batch stream: tombstones,
+// delta removals, the cascade, delta insertions and the post-batch repair in
+// one persistent launch (the arcs were classified when they were staged).
+static int repair_fused(Bfs* b) {
+  Graph* g = b->g;
+  const size_t n = b->staged_ops, m = 2 * n;
+  StreamArgs sa;
+  memset(&sa, 0, sizeof(sa));
+  sa.fu = g->batch.fu;
+  sa.fv = g->batch.fv;
+  sa.ff = g->batch.ff;
+  sa.fpos = g->batch.fpos;
+  sa.bcnt = &g->ctr->final_arcs;
+  sa.scratch = g->batch.lu;
+  sa.gc = g->ctr;
+  sa.arena_cap = g->adj[0].arena_cap;
+  sa.frac = b->frac;
+  sa.nb = 1;
+  sa.V0 = (uint32_t)b->staged_V_pre;
+  sa.len0 = (uint32_t)b->staged_len_pre;
+  sa.v_single = (uint32_t)g->V;
+  sa.classified = 1;
+  Params p = make_params(b, (uint32_t)g->V, (uint32_t)g->V);
+  if (int rc = launch_stream(b, p, sa)) return rc;
+  g->adj[0].arena_bound += 8ull * m + 8;  // the bound the staging reserved for
+  ++g->version;
+  b->dist_len = std::max<size_t>(b->dist_len, g->V);
+  b->staged_ops = 0;
+  return 0;
+}
+
 int bfs_repair_staged(Bfs* b) {
   Graph* g = b->g;
   cudaStream_t s = g->stream;
   if (b->staged_ops == 0) return 0;
+  if (!g->directed) return repair_fused(b);
   const size_t V_pre = b->staged_V_pre, len_pre = b->staged_len_pre;
   const size_t V_post = g->V;
   // fallback limit: max(1, size_t(double(V) * fraction))  (bfs.hpp:225-226)
@@ -1449,9 +1905,190 @@ int bfs_level_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n) {
 
 int bfs_phase_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n) {
   if (int rc = bfs_sync(b)) return rc;
-  constexpr size_t kN = sizeof(b->hctr->rtrace) / sizeof(b->hctr->rtrace[0]);
-  *n = kN;
-  for (size_t i = 0; i < std::min(cap, kN); ++i) out[i] = b->hctr->rtrace[i];
+  constexpr size_t kR = sizeof(b->hctr->rtrace) / sizeof(b->hctr->rtrace[0]);
+  constexpr size_t kS = sizeof(b->hctr->stream_ns) / sizeof(b->hctr->stream_ns[0]);
+  *n = kR + kS;
+  for (size_t i = 0; i < std::min(cap, kR); ++i) out[i] = b->hctr->rtrace[i];
+  for (size_t i = kR; i < std::min(cap, kR + kS); ++i) out[i] = b->hctr->stream_ns[i - kR];
+  return 0;
+}
+
+// ------------------------------------------------------- batched stream --
+
+void StreamBufs::free_all() {
+  void* ptrs[] = {src, dst, add, off, keys, keys_alt, vals, vals_alt, flag, pos, fu, fv, bid, ff, fpos,
+                  boff, bcnt, vpost, total, scratch, digest, bstats};
+  for (void* q : ptrs) cudaFree(q);
+  *this = StreamBufs();
+}
+
+int StreamBufs::ensure(size_t n, size_t nb, size_t maxf) {
+  if (n <= ops_cap && nb <= nb_cap && maxf <= maxf_cap) return 0;
+  const size_t N = std::max(n, ops_cap), B = std::max(nb, nb_cap), MF = std::max(maxf, maxf_cap);
+  free_all();
+  const size_t m = 2 * std::max<size_t>(N, 1);
+  bool ok = true;
+  auto al = [&](auto** q, size_t count, size_t size) {
+    if (ok && cudaMalloc((void**)q, std::max<size_t>(count, 1) * size) != cudaSuccess) ok = false;
+  };
+  al(&src, N, 4);
+  al(&dst, N, 4);
+  al(&add, N, 1);
+  al(&off, B + 1, 8);
+  al(&keys, m, 8);
+  al(&keys_alt, m, 8);
+  al(&vals, m, 4);
+  al(&vals_alt, m, 4);
+  al(&flag, m, 4);
+  al(&pos, m, 4);
+  al(&fu, m, 4);
+  al(&fv, m, 4);
+  al(&bid, m, 4);
+  al(&ff, m, 1);
+  al(&fpos, m, 8);
+  al(&boff, B + 1, 4);
+  al(&bcnt, B, 4);
+  al(&vpost, B, 4);
+  al(&total, 1, 4);
+  al(&scratch, MF, 4);
+  al(&digest, B, 8);
+  al(&bstats, 4 * B, 4);
+  if (!ok) {
+    free_all();
+    set_error("stream buffer allocation failed");
+    return -4;
+  }
+  ops_cap = N;
+  nb_cap = B;
+  maxf_cap = MF;
+  return 0;
+}
+
+int bfs_apply_stream(Bfs* b, const uint32_t* hs, const uint32_t* hd, const uint8_t* ha, const uint64_t* hoff,
+                     size_t nb, uint64_t* digests, uint32_t* stats, int* done) {
+  Graph* g = b->g;
+  cudaStream_t st = g->stream;
+  *done = 0;
+  if (nb == 0) {
+    *done = 1;
+    return 0;
+  }
+  if (hoff[0] != 0) {
+    set_error("batch offsets must start at 0");
+    return -1;
+  }
+  const size_t n = hoff[nb];
+  const size_t Vbefore = g->V;
+  // vertex count after every batch (the graph grows to max id + 1 over the
+  // non-self-loop ops, dynamic_graph.hpp:717-733) and the arena bound
+  std::vector<uint32_t> vpost(nb);
+  size_t V = g->V, maxf = 1;
+  uint64_t bound = 0;
+  size_t nonempty = 0;
+  for (size_t t = 0; t < nb; ++t) {
+    if (hoff[t + 1] < hoff[t]) {
+      set_error("batch offsets must not decrease");
+      return -1;
+    }
+    for (uint64_t i = hoff[t]; i < hoff[t + 1]; ++i)
+      if (hs[i] != hd[i]) V = std::max<size_t>(V, (size_t)std::max(hs[i], hd[i]) + 1);
+    if (V > vxb::kMaxVertices) {
+      set_error("vertex id beyond the supported maximum (2^31 - 1)");
+      return -2;
+    }
+    vpost[t] = (uint32_t)V;
+    const size_t m = 2 * (size_t)(hoff[t + 1] - hoff[t]);
+    if (m) {
+      bound += 8ull * m + 8;
+      ++nonempty;
+    }
+    maxf = std::max(maxf, m);
+  }
+  int bbits = 1;
+  while (bbits < 32 && ((size_t)1 << bbits) < std::max<size_t>(V, 2)) ++bbits;
+  int tbits = 1;
+  while (tbits < 40 && ((size_t)1 << tbits) < nb) ++tbits;
+  // the persistent path covers undirected graphs whose (batch, u, v) keys fit
+  // 64 bits and whose arena takes the whole stream; the caller loops otherwise
+  if (g->directed || 2 * bbits + tbits > 64 || n >= (1ull << 31)) return 0;
+  int fits = 0;
+  if (int rc = graph_reserve_stream(g, bound, &fits)) return rc;
+  if (!fits) return 0;
+  if (int rc = graph_grow(g, V)) return rc;
+  const uint32_t len0 = (uint32_t)b->dist_len;
+  if (int rc = ensure_capacity(b, std::max<size_t>(V, 1))) return rc;
+  Adjacency& a = g->adj[0];
+  a.arena_bound += bound;
+  if (int rc = ensure_ring(b)) return rc;
+  StreamBufs& S = b->sb;
+  if (int rc = S.ensure(n, nb, maxf)) return rc;
+  VX_CUDA_TRY(cudaMemcpyAsync(S.src, hs, n * 4, cudaMemcpyHostToDevice, st));
+  VX_CUDA_TRY(cudaMemcpyAsync(S.dst, hd, n * 4, cudaMemcpyHostToDevice, st));
+  VX_CUDA_TRY(cudaMemcpyAsync(S.add, ha, n, cudaMemcpyHostToDevice, st));
+  VX_CUDA_TRY(cudaMemcpyAsync(S.off, hoff, (nb + 1) * 8, cudaMemcpyHostToDevice, st));
+  VX_CUDA_TRY(cudaMemcpyAsync(S.vpost, vpost.data(), nb * 4, cudaMemcpyHostToDevice, st));
+  const size_t m = 2 * n;
+  const unsigned grid_n = (unsigned)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, (size_t)sm_count() * 32));
+  const unsigned grid_m = (unsigned)std::max<size_t>(1, std::min<size_t>((m + 255) / 256, (size_t)sm_count() * 32));
+  count_launch();
+  stream_keys_kernel<<<grid_n, 256, 0, st>>>(S.src, S.dst, S.add, S.off, (uint32_t)nb, n, bbits, S.keys, S.vals);
+  VX_CUDA_TRY(cudaGetLastError());
+  bool in_alt = false;
+  if (int rc = radix_sort_u64(S.keys, S.keys_alt, S.vals, S.vals_alt, m, 2 * bbits + tbits, &in_alt, g->scratch, st))
+    return rc;
+  uint64_t* keys = in_alt ? S.keys_alt : S.keys;
+  uint32_t* vals = in_alt ? S.vals_alt : S.vals;
+  count_launch();
+  stream_last_kernel<<<grid_m, 256, 0, st>>>(keys, m, S.flag);
+  if (int rc = scan_exclusive_u32(S.flag, S.pos, m, S.total, g->scratch, st)) return rc;
+  count_launch();
+  stream_compact_kernel<<<grid_m, 256, 0, st>>>(keys, vals, S.flag, S.pos, m, bbits, S.fu, S.fv, S.ff, S.bid);
+  count_launch();
+  stream_bounds_kernel<<<(unsigned)((nb + 256) / 256), 256, 0, st>>>(S.bid, S.total, (uint32_t)nb, S.boff, S.bcnt);
+  VX_CUDA_TRY(cudaGetLastError());
+  if (digests) VX_CUDA_TRY(cudaMemsetAsync(S.digest, 0, nb * 8, st));
+  StreamArgs sa;
+  memset(&sa, 0, sizeof(sa));
+  sa.fu = S.fu;
+  sa.fv = S.fv;
+  sa.ff = S.ff;
+  sa.fpos = S.fpos;
+  sa.boff = S.boff;
+  sa.bcnt = S.bcnt;
+  sa.vpost = S.vpost;
+  sa.scratch = S.scratch;
+  sa.digest = digests ? S.digest : nullptr;
+  sa.bstats = stats ? S.bstats : nullptr;
+  sa.gc = g->ctr;
+  sa.arena_cap = a.arena_cap;
+  sa.frac = b->frac;
+  sa.nb = (uint32_t)nb;
+  sa.V0 = (uint32_t)Vbefore;
+  sa.len0 = len0;
+  Params p = make_params(b, (uint32_t)V, (uint32_t)V);
+  if (int rc = launch_stream(b, p, sa)) return rc;
+  g->version += nonempty;
+  b->dist_len = V;
+  b->staged_ops = 0;
+  if (digests) VX_CUDA_TRY(cudaMemcpyAsync(digests, S.digest, nb * 8, cudaMemcpyDeviceToHost, st));
+  if (stats) VX_CUDA_TRY(cudaMemcpyAsync(stats, S.bstats, nb * 16, cudaMemcpyDeviceToHost, st));
+  if (digests || stats) VX_CUDA_TRY(cudaStreamSynchronize(st));
+  *done = 1;
+  return 0;
+}
+
+int bfs_digest(Bfs* b, uint64_t* out) {
+  cudaStream_t st = b->g->stream;
+  unsigned long long* d = &b->ctr->scratch64;
+  VX_CUDA_TRY(cudaMemsetAsync(d, 0, 8, st));
+  if (b->dist_len) {
+    count_launch();
+    digest_kernel<<<sm_count() * 8, 256, 0, st>>>(b->dist, (uint32_t)b->dist_len, d);
+    VX_CUDA_TRY(cudaGetLastError());
+  }
+  VX_CUDA_TRY(cudaMemcpyAsync(b->g->pinned_scalar, d, 8, cudaMemcpyDeviceToHost, st));
+  VX_CUDA_TRY(cudaStreamSynchronize(st));
+  *out = b->g->pinned_scalar[0];
   return 0;
 }
 }  // namespace vxh

@@ -34,12 +34,34 @@ struct BfsCounters {
   // relaxation (claims, failed claims, idle rounds, slot waits, cycles
   // spent processing summed over blocks, and the longest processing round)
   unsigned long long rtrace[21];
+  // time spent by the last stream launch in each of its per-batch phases
+  // (classify + tombstones, removals + candidates, cascade, insertions,
+  // post-batch repair, end-of-batch barrier), summed over its batches, ns
+  unsigned long long stream_ns[6];
 };
 
 struct BfsTuning {
   float alpha = 14.0f;       // top-down -> bottom-up when m_f * alpha > m_u
   float beta = 24.0f;        // bottom-up -> top-down when n_f * beta < V (shrinking)
   uint32_t large_row = 1024; // rows this long are expanded by the whole grid
+};
+
+// Device buffers of the batched stream path (kept between calls).
+struct StreamBufs {
+  size_t ops_cap = 0, nb_cap = 0, maxf_cap = 0;
+  uint32_t *src = nullptr, *dst = nullptr;
+  uint8_t* add = nullptr;
+  uint64_t* off = nullptr;
+  uint64_t *keys = nullptr, *keys_alt = nullptr;
+  uint32_t *vals = nullptr, *vals_alt = nullptr, *flag = nullptr, *pos = nullptr;
+  uint32_t *fu = nullptr, *fv = nullptr, *bid = nullptr;
+  uint8_t* ff = nullptr;
+  uint64_t* fpos = nullptr;
+  uint32_t *boff = nullptr, *bcnt = nullptr, *vpost = nullptr, *total = nullptr, *scratch = nullptr;
+  unsigned long long* digest = nullptr;
+  uint32_t* bstats = nullptr;
+  int ensure(size_t ops, size_t batches, size_t max_batch_arcs);
+  void free_all();
 };
 
 struct Bfs {
@@ -70,6 +92,8 @@ struct Bfs {
   size_t staged_ops = 0, staged_V_pre = 0, staged_len_pre = 0;  // batch staged by bfs_stage
   BfsTuning tune;
   int grid = 0;
+  int stream_grid = 0;
+  StreamBufs sb;
 };
 
 int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac);
@@ -89,5 +113,16 @@ int bfs_reached_arcs(Bfs* b, unsigned long long* arcs);  // sum of degrees of re
 // for every level, then a closing timestamp.  Writes up to cap u64 values.
 int bfs_level_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n);
 int bfs_phase_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n);
+// The batches [hoff[t], hoff[t+1]) of host arrays (hoff[0] == 0) applied in
+// order in one persistent launch; *done = 0 when the stream is not one the
+// persistent path takes (directed graph, keys past 64 bits, arena), and the
+// caller then applies the batches one by one.  digests / stats (optional,
+// host) receive the distance digest and {candidates, affected, full,
+// reachable} after every batch.
+int bfs_apply_stream(Bfs* b, const uint32_t* hs, const uint32_t* hd, const uint8_t* ha, const uint64_t* hoff,
+                     size_t nb, uint64_t* digests, uint32_t* stats, int* done);
+// Order-independent digest of the current distances: the sum over v of
+// splitmix64(v << 32 | dist[v]) modulo 2^64.
+int bfs_digest(Bfs* b, uint64_t* out);
 
 }  // namespace vxh

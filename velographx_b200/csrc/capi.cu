@@ -313,6 +313,35 @@ int vx_bfs_reached_arcs(vx_bfs* b, uint64_t* out) {
   return VX_OK;
 }
 
+int vx_bfs_apply_stream(vx_bfs* b, const uint32_t* src, const uint32_t* dst, const uint8_t* add,
+                        const uint64_t* offsets, size_t nbatches, uint64_t* digests, uint32_t* stats) {
+  if (!b || !offsets || (nbatches && offsets[nbatches] && (!src || !dst || !add)))
+    return fail(VX_ERR_INVALID, "null argument");
+  int done = 0;
+  if (int rc = vxh::bfs_apply_stream(b->b, src, dst, add, offsets, nbatches, digests, stats, &done)) return rc;
+  if (done) return VX_OK;
+  for (size_t t = 0; t < nbatches; ++t) {
+    const uint64_t lo = offsets[t];
+    if (int rc = vx_bfs_apply(b, src + lo, dst + lo, add + lo, offsets[t + 1] - lo)) return rc;
+    if (digests)
+      if (int rc = vxh::bfs_digest(b->b, reinterpret_cast<uint64_t*>(digests + t))) return rc;
+    if (stats) {
+      if (int rc = vxh::bfs_sync(b->b)) return rc;
+      const vxh::BfsCounters& c = *b->b->hctr;
+      stats[4 * t + 0] = c.candidates;
+      stats[4 * t + 1] = c.affected;
+      stats[4 * t + 2] = c.full;
+      stats[4 * t + 3] = (uint32_t)c.reachable;
+    }
+  }
+  return VX_OK;
+}
+
+int vx_bfs_digest(vx_bfs* b, uint64_t* out) {
+  if (!b || !out) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::bfs_digest(b->b, out);
+}
+
 int vx_bfs_phase_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n) {
   if (!b || !n || (cap && !out)) return fail(VX_ERR_INVALID, "null argument");
   return vxh::bfs_phase_trace(b->b, reinterpret_cast<unsigned long long*>(out), cap, n);

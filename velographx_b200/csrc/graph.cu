@@ -13,6 +13,7 @@
 #include <cstring>
 
 #include "graph.cuh"
+#include "graph_dev.cuh"
 
 namespace vxh {
 
@@ -38,58 +39,10 @@ inline int bits_for(size_t v) {  // bits to represent v - 1 (v >= 1)
   return b;
 }
 
-// ---------------------------------------------------------------- helpers --
-
-__device__ __forceinline__ bool bsearch_u32(const uint32_t* a, uint32_t lo, uint32_t hi, uint32_t x) {
-  const uint32_t p = vxb::lower_bound_u32(a, lo, hi, x);
-  return p < hi && a[p] == x;
-}
-
-// Merge-path co-rank: number of A elements among the k smallest of A U B
-// (both sorted, disjoint values).
-__device__ __forceinline__ uint32_t corank(uint32_t k, const uint32_t* A, uint32_t nA, const uint32_t* B,
-                                           uint32_t nB) {
-  uint32_t lo = k > nB ? k - nB : 0u, hi = k < nA ? k : nA;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (A[mid] < B[k - mid - 1]) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
-}
-
-__device__ __forceinline__ uint32_t merged_at(uint32_t k, const uint32_t* A, uint32_t nA, const uint32_t* B,
-                                              uint32_t nB) {
-  const uint32_t i = corank(k, A, nA, B, nB), j = k - i;
-  return (j >= nB || (i < nA && A[i] < B[j])) ? A[i] : B[j];
-}
-
-// Warp-cooperative merge of sorted B[0..nB) into sorted A[0..nA) where A has
-// room for nA + nB entries.  Output chunks are produced from the back; every
-// output k only reads A at positions <= k, so no unread input is overwritten.
-__device__ void warp_merge_inplace(uint32_t* A, uint32_t nA, const uint32_t* B, uint32_t nB) {
-  const int lane = threadIdx.x & 31;
-  const uint32_t total = nA + nB;
-  for (int64_t top = total; top > 0; top -= 32) {
-    const int64_t k = top - 32 + lane;
-    uint32_t val = 0;
-    if (k >= 0) val = merged_at((uint32_t)k, A, nA, B, nB);
-    __syncwarp();
-    if (k >= 0) A[k] = val;
-    __syncwarp();
-  }
-}
-
-__device__ void warp_merge_to(uint32_t* out, const uint32_t* A, uint32_t nA, const uint32_t* B, uint32_t nB) {
-  const int lane = threadIdx.x & 31;
-  for (uint32_t k = lane; k < nA + nB; k += 32) out[k] = merged_at(k, A, nA, B, nB);
-}
-
-__device__ __forceinline__ void mark_dirty(uint32_t* dirty, uint32_t u, unsigned long long* counter) {
-  const uint32_t bit = 1u << (u & 31);
-  const uint32_t old = atomicOr(&dirty[u >> 5], bit);
-  if (!(old & bit)) atomicAdd(counter, 1ull);
-}
+using gdev::bsearch_u32;
+using gdev::mark_dirty;
+using gdev::warp_merge_inplace;
+using gdev::warp_merge_to;
 
 // ----------------------------------------------------------- bulk build --
 
@@ -207,26 +160,8 @@ __global__ void compact_final_kernel(const uint64_t* keys, const uint32_t* vals,
 __global__ void classify_kernel(DevAdj a, const uint32_t* fu, const uint32_t* fv, uint8_t* ff, uint64_t* fpos,
                                 const uint32_t* count) {
   const uint32_t F = *count;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x) {
-    const uint32_t u = fu[i], v = fv[i];
-    uint8_t f = ff[i] & vxh::kFAdd;
-    uint64_t b, e;
-    vxb::base_range(a, u, b, e);
-    const uint64_t p = vxb::lower_bound_masked(a.col, b, e, v);
-    bool cur = false;
-    if (p < e && (a.col[p] & kIdMask) == v) {
-      f |= vxh::kFInBase;
-      cur = !(a.col[p] & kTomb);
-      fpos[i] = p;
-    } else {
-      const uint2 r = a.drow[u];
-      cur = bsearch_u32(a.darena, r.x, r.x + r.y, v);
-      fpos[i] = ~0ull;
-    }
-    if (cur) f |= vxh::kFCur;
-    if (cur != ((f & vxh::kFAdd) != 0)) f |= vxh::kFChanged;
-    ff[i] = f;
-  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
+    ff[i] = gdev::classify_arc(a, fu[i], fv[i], ff[i], fpos[i]);
 }
 
 // Reversed changed arcs (v, u) for the in-adjacency of directed graphs.
@@ -257,23 +192,8 @@ __global__ void tomb_kernel(DevAdj a, const uint32_t* fu, const uint8_t* ff, con
                             unsigned long long* dirty_rows) {
   const uint32_t F = *count;
   long long delta = 0;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x) {
-    const uint8_t f = ff[i];
-    if (!(f & vxh::kFInBase) || !(f & vxh::kFChanged)) continue;
-    if (((f & vxh::kFAdd) != 0) != (mode == 1)) continue;
-    const uint64_t p = fpos[i];
-    const uint32_t u = fu[i];
-    if (f & vxh::kFAdd) {
-      a.col[p] &= kIdMask;
-      atomicSub(&a.tcnt[u], 1u);
-      --delta;
-    } else {
-      a.col[p] |= kTomb;
-      atomicAdd(&a.tcnt[u], 1u);
-      ++delta;
-    }
-    mark_dirty(a.dirty, u, dirty_rows);
-  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
+    delta += gdev::tomb_arc(a, fu[i], ff[i], fpos[i], mode, dirty_rows);
   delta = vxb::warp_sum(delta);
   if ((threadIdx.x & 31) == 0 && delta) atomicAdd(tombs, (unsigned long long)delta);
 }
@@ -870,6 +790,24 @@ static int reserve_arena(Graph* g, Adjacency& a, size_t arcs, int* need_consolid
     return 0;
   }
   return grow_arena(a, need, g->stream);
+}
+
+// Arena room for a whole update stream whose batches insert at most
+// `entries` delta entries in total (the sum of the per-batch bounds):
+// consolidates first when the bound passes the limit; *fits = 0 when even
+// the consolidated graph cannot take it in one go.
+int graph_reserve_stream(Graph* g, uint64_t entries, int* fits) {
+  *fits = 1;
+  Adjacency& a = g->adj[0];
+  if (a.arena_bound + entries + 8 > g->arena_limit_entries || a.arena_bound + entries + 8 >= 0xFFFFFFF0ull) {
+    if (int rc = graph_consolidate(g)) return rc;
+    if (a.arena_bound + entries + 8 > g->arena_limit_entries || a.arena_bound + entries + 8 >= 0xFFFFFFF0ull) {
+      *fits = 0;
+      return 0;
+    }
+  }
+  if (a.arena_bound + entries + 8 > a.arena_cap) return grow_arena(a, a.arena_bound + entries + 8, g->stream);
+  return 0;
 }
 
 static int scan_count(Graph* g, const uint32_t* flag, uint32_t* pos, size_t m, uint32_t* total) {

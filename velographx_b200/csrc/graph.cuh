@@ -108,6 +108,7 @@ int graph_commit_batch(Graph* g);
 int graph_commit_removals(Graph* g);
 int graph_commit_insertions(Graph* g);
 int graph_consolidate(Graph* g);
+int graph_reserve_stream(Graph* g, uint64_t entries, int* fits);
 // One-launch canonicalisation of the staged batch in a thread-block cluster
 // (sort, last-op-wins dedupe, compaction, classification); *done = false when
 // the batch exceeds one cluster's capacity.

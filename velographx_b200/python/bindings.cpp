@@ -256,6 +256,35 @@ PYBIND11_MODULE(_velographx, m) {
              detail::check(vx_bfs_reached_arcs(x.handle(), &a));
              return a;
            })
+      .def("apply_stream",
+           [](IncrementalBFS& x, const u32_array& s, const u32_array& d, const u8_array& a,
+              const py::array_t<std::uint64_t, py::array::c_style | py::array::forcecast>& offsets, bool digests,
+              bool stats) {
+             Arrays y(s, d, a);
+             if (offsets.ndim() != 1 || offsets.shape(0) < 1) throw std::invalid_argument("offsets: 1-D, >= 1 entry");
+             const std::size_t nb = static_cast<std::size_t>(offsets.shape(0)) - 1;
+             if (offsets.data()[nb] > y.n) throw std::invalid_argument("offsets exceed the op arrays");
+             py::array_t<std::uint64_t> dg(digests ? nb : 0);
+             py::array_t<std::uint32_t> st(stats ? 4 * nb : 0);
+             std::uint64_t* pd = digests ? dg.mutable_data() : nullptr;
+             std::uint32_t* ps = stats ? st.mutable_data() : nullptr;
+             {
+               py::gil_scoped_release release;
+               detail::check(vx_bfs_apply_stream(x.handle(), y.src.data(), y.dst.data(), y.add.data(), offsets.data(),
+                                                 nb, pd, ps));
+             }
+             x.mark_stale();
+             if (stats) st.resize({static_cast<py::ssize_t>(nb), static_cast<py::ssize_t>(4)});
+             return py::make_tuple(dg, st);
+           },
+           py::arg("src"), py::arg("dst"), py::arg("add"), py::arg("offsets"), py::arg("digests") = false,
+           py::arg("stats") = false)
+      .def("digest",
+           [](IncrementalBFS& x) {
+             std::uint64_t d = 0;
+             detail::check(vx_bfs_digest(x.handle(), &d));
+             return d;
+           })
       .def("phase_trace",
            [](IncrementalBFS& x) {
              std::uint64_t t[32] = {};

@@ -5,16 +5,18 @@
                deletions drawn from the edges nearest the root (the ones whose
                endpoints have the smallest distances) -- deep subtree
                invalidation and repair.
-``lognormal``  R-MAT scale 20 with update batches of lognormal sizes (median
-               500 ops, sigma 2, clipped to [1, 200000]; 80% insertions),
-               applied one batch at a time through the public API, each
-               batch's host arrays copied in and the stream synchronised per
-               batch.
+``lognormal``  R-MAT scale 20 with 1,000 update batches of lognormal sizes
+               (median 500 ops, sigma 2, clipped to [1, 200000]; 80%
+               insertions): the plain path (one batch at a time through the
+               public API, host arrays copied in and the counters read back
+               per batch) against the batched path (the whole stream in one
+               apply_stream call), end to end from host arrays.
 
 Every run times batches with CUDA events on the graph's stream and checks the
 maintained distances against a fresh full BFS at regular batches.
 
   python -m velographx_b200.stream_bench --workload grid [--batches 500]
+  python -m velographx_b200.stream_bench --workload lognormal [--scale 20]
 """
 from __future__ import annotations
 
@@ -132,16 +134,90 @@ def grid(side: int = 4096, long_range: float = 0.001, batches: int = 500, ops: i
     return res
 
 
+def lognormal(scale: int = 20, batches: int = 1000, median: float = 500.0, sigma: float = 2.0,
+              insert_fraction: float = 0.8, seed: int = 33, check_batches: int = 200) -> dict:
+    """Batched stream (one apply_stream call: upload, stream-wide
+    canonicalisation, one persistent launch) against the plain path
+    (apply_arrays + a counter read-back per batch) on replicas of one graph."""
+    import torch
+
+    V = 1 << scale
+    edges = w.rmat_edges(scale, 16, seed=seed)
+    root = w.max_degree_root(edges, V)
+    sizes = w.lognormal_sizes(batches, median=median, sigma=sigma, lo=1, hi=200_000, seed=seed + 1)
+    st = w.mixed_stream(edges, V, sizes, insert_fraction, seed=seed + 2)
+    off = st.offsets.astype(np.uint64)
+
+    def replica():
+        g = Graph(V, False)
+        g.bulk_load_edges(edges)
+        return g, IncrementalBFS(g, root)
+
+    out = {"workload": f"rmat{scale}-undirected-ef16-lognormal-batches-median{median:g}-sigma{sigma:g}-"
+                       f"{int(insert_fraction * 100)}pct-insert",
+           "vertices": V, "batches": batches, "ops": int(sizes.sum()), "median_ops": float(np.median(sizes)),
+           "max_ops": int(sizes.max())}
+    # plain: one batch at a time from host arrays, synchronised per batch
+    gp, bp = replica()
+    cs = torch.cuda.ExternalStream(gp.stream)
+    e0, e1 = _events()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(cs)
+    for t in range(batches):
+        bp.apply_arrays(*st.batch(t))
+        bp.stats()
+    e1.record(cs)
+    torch.cuda.synchronize()
+    out["plain"] = {"seconds": e0.elapsed_time(e1) * 1e-3, "wall_s": time.perf_counter() - t0}
+    out["plain"]["batches_per_s"] = batches / out["plain"]["seconds"]
+    # batched: the whole stream in one call, distances resident on the device at the end
+    gb, bb = replica()
+    cs = torch.cuda.ExternalStream(gb.stream)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0.record(cs)
+    bb.apply_stream(st.src, st.dst, st.add, off)
+    e1.record(cs)
+    torch.cuda.synchronize()
+    out["batched"] = {"seconds": e0.elapsed_time(e1) * 1e-3, "wall_s": time.perf_counter() - t0}
+    out["batched"]["batches_per_s"] = batches / out["batched"]["seconds"]
+    ph = bb.phase_trace()[21:27]
+    out["batched"]["phase_us_per_batch"] = dict(zip(
+        ["classify", "removals", "cascade", "insertions", "post_repair", "end_barrier"],
+        [round(x / 1e3 / batches, 2) for x in ph]))
+    out["speedup"] = out["batched"]["batches_per_s"] / out["plain"]["batches_per_s"]
+    out["exact_final"] = bool(np.array_equal(bp.distances_array(), bb.distances_array())
+                              and bp.reachable_count == bb.reachable_count)
+    # per-batch check on a prefix: digests of the stream path against the plain path
+    if check_batches:
+        k = min(check_batches, batches)
+        gc_, bc = replica()
+        gd, bd = replica()
+        digs, _ = bc.apply_stream(st.src, st.dst, st.add, off[: k + 1], digests=True)
+        ok = True
+        for t in range(k):
+            bd.apply_arrays(*st.batch(t))
+            ok = ok and int(digs[t]) == bd.digest()
+        out["exact_every_batch"] = {"batches": k, "exact": bool(ok)}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--workload", choices=["grid"], default="grid")
+    ap.add_argument("--workload", choices=["grid", "lognormal"], default="grid")
     ap.add_argument("--side", type=int, default=4096)
     ap.add_argument("--batches", type=int, default=500)
     ap.add_argument("--ops", type=int, default=1000)
     ap.add_argument("--check-every", type=int, default=50)
+    ap.add_argument("--scale", type=int, default=20)
+    ap.add_argument("--sigma", type=float, default=2.0)
     a = ap.parse_args()
     t0 = time.time()
-    res = grid(a.side, batches=a.batches, ops=a.ops, check_every=a.check_every)
+    if a.workload == "lognormal":
+        res = lognormal(a.scale, batches=a.batches if a.batches != 500 else 1000, sigma=a.sigma)
+    else:
+        res = grid(a.side, batches=a.batches, ops=a.ops, check_every=a.check_every)
     res["wall_s"] = time.time() - t0
     print(json.dumps(res), flush=True)
 
