@@ -154,6 +154,12 @@ int vx_bfs_digest(vx_bfs* b, uint64_t* out);
 /* Direction switch (alpha, beta) and grid-expanded row length of the full BFS.
  * No reference counterpart: the reference BFS is top-down only. */
 int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row);
+/* fused != 0 (default): an undirected batch's commit and repair run in one
+ * persistent launch after staging; 0: the per-phase path (a launch per commit
+ * step and for each half of the repair) -- the plain baseline the batched
+ * stream path is measured against.  Same results either way.  No reference
+ * counterpart. */
+int vx_bfs_set_fused(vx_bfs* b, int fused);
 
 /* ---- Multi-root BFS (up to 256 roots, one launch) ----------------------
  * For every root r, row r of the result equals BasicIncrementalBFS(g,

@@ -23,8 +23,6 @@ if not torch.cuda.is_available():
 import velographx_b200 as vx  # noqa: E402
 from velographx_b200 import workloads as w  # noqa: E402
 
-M64 = (1 << 64) - 1
-
 
 def mix64(z: np.ndarray) -> np.ndarray:
     """splitmix64 finaliser on uint64 arrays (wrapping arithmetic)."""
@@ -158,3 +156,25 @@ def test_stream_fallback_and_directed_loop():
             assert int(digs[t]) == digest(ob.distances()), (directed, t)
             assert bool(stats[t, 2]) == ob.last_used_full_recompute
         assert np.array_equal(b.distances_array(), ob.distances())
+
+
+def test_per_phase_and_fused_paths_agree():
+    V = 1 << 13
+    edges = w.rmat_edges(13, 8, seed=12)
+    root = w.max_degree_root(edges, V)
+    src, dst, add, off = messy_stream(edges, V, [50, 700, 3, 2500, 0, 90, 1200], 13, grow=20)
+    runs = []
+    for fused in (False, True):
+        g = vx.Graph(V, False)
+        g.bulk_load_edges(edges)
+        b = vx.IncrementalBFS(g, root)
+        b.set_fused(fused)
+        rec = []
+        for t in range(len(off) - 1):
+            lo, hi = int(off[t]), int(off[t + 1])
+            b.apply_arrays(src[lo:hi], dst[lo:hi], add[lo:hi])
+            s = b.stats()
+            rec.append((b.digest(), s["last_deletion_candidates"], s["last_used_full_recompute"],
+                        s["reachable_count"], g.edge_count_directed(), g.version))
+        runs.append(rec)
+    assert runs[0] == runs[1]

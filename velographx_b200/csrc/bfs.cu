@@ -1828,7 +1828,7 @@ int bfs_repair_staged(Bfs* b) {
   Graph* g = b->g;
   cudaStream_t s = g->stream;
   if (b->staged_ops == 0) return 0;
-  if (!g->directed) return repair_fused(b);
+  if (!g->directed && b->tune.fused) return repair_fused(b);
   const size_t V_pre = b->staged_V_pre, len_pre = b->staged_len_pre;
   const size_t V_post = g->V;
   // fallback limit: max(1, size_t(double(V) * fraction))  (bfs.hpp:225-226)

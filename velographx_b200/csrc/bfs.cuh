@@ -44,6 +44,7 @@ struct BfsTuning {
   float alpha = 14.0f;       // top-down -> bottom-up when m_f * alpha > m_u
   float beta = 24.0f;        // bottom-up -> top-down when n_f * beta < V (shrinking)
   uint32_t large_row = 1024; // rows this long are expanded by the whole grid
+  bool fused = true;         // undirected batches: one persistent launch after staging
 };
 
 // Device buffers of the batched stream path (kept between calls).

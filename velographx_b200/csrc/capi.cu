@@ -337,6 +337,12 @@ int vx_bfs_apply_stream(vx_bfs* b, const uint32_t* src, const uint32_t* dst, con
   return VX_OK;
 }
 
+int vx_bfs_set_fused(vx_bfs* b, int fused) {
+  if (!b) return fail(VX_ERR_INVALID, "null argument");
+  b->b->tune.fused = fused != 0;
+  return VX_OK;
+}
+
 int vx_bfs_digest(vx_bfs* b, uint64_t* out) {
   if (!b || !out) return fail(VX_ERR_INVALID, "null argument");
   return vxh::bfs_digest(b->b, out);

@@ -279,6 +279,7 @@ PYBIND11_MODULE(_velographx, m) {
            },
            py::arg("src"), py::arg("dst"), py::arg("add"), py::arg("offsets"), py::arg("digests") = false,
            py::arg("stats") = false)
+      .def("set_fused", [](IncrementalBFS& x, bool fused) { detail::check(vx_bfs_set_fused(x.handle(), fused)); })
       .def("digest",
            [](IncrementalBFS& x) {
              std::uint64_t d = 0;

@@ -157,20 +157,26 @@ def lognormal(scale: int = 20, batches: int = 1000, median: float = 500.0, sigma
                        f"{int(insert_fraction * 100)}pct-insert",
            "vertices": V, "batches": batches, "ops": int(sizes.sum()), "median_ops": float(np.median(sizes)),
            "max_ops": int(sizes.max())}
-    # plain: one batch at a time from host arrays, synchronised per batch
-    gp, bp = replica()
-    cs = torch.cuda.ExternalStream(gp.stream)
+    # plain: one batch at a time from host arrays, synchronised per batch --
+    # the per-phase path (a launch per commit step and repair half) and the
+    # fused one (canonicalisation + one persistent launch per batch)
     e0, e1 = _events()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e0.record(cs)
-    for t in range(batches):
-        bp.apply_arrays(*st.batch(t))
-        bp.stats()
-    e1.record(cs)
-    torch.cuda.synchronize()
-    out["plain"] = {"seconds": e0.elapsed_time(e1) * 1e-3, "wall_s": time.perf_counter() - t0}
-    out["plain"]["batches_per_s"] = batches / out["plain"]["seconds"]
+    for name, fused in (("plain", False), ("plain_fused", True)):
+        gp, bp = replica()
+        bp.set_fused(fused)
+        cs = torch.cuda.ExternalStream(gp.stream)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record(cs)
+        for t in range(batches):
+            bp.apply_arrays(*st.batch(t))
+            bp.stats()
+        e1.record(cs)
+        torch.cuda.synchronize()
+        out[name] = {"seconds": e0.elapsed_time(e1) * 1e-3, "wall_s": time.perf_counter() - t0}
+        out[name]["batches_per_s"] = batches / out[name]["seconds"]
+        if fused:
+            bp_fused = bp
     # batched: the whole stream in one call, distances resident on the device at the end
     gb, bb = replica()
     cs = torch.cuda.ExternalStream(gb.stream)
@@ -187,14 +193,17 @@ def lognormal(scale: int = 20, batches: int = 1000, median: float = 500.0, sigma
         ["classify", "removals", "cascade", "insertions", "post_repair", "end_barrier"],
         [round(x / 1e3 / batches, 2) for x in ph]))
     out["speedup"] = out["batched"]["batches_per_s"] / out["plain"]["batches_per_s"]
+    out["speedup_vs_fused"] = out["batched"]["batches_per_s"] / out["plain_fused"]["batches_per_s"]
     out["exact_final"] = bool(np.array_equal(bp.distances_array(), bb.distances_array())
-                              and bp.reachable_count == bb.reachable_count)
+                              and bp.reachable_count == bb.reachable_count
+                              and np.array_equal(bp_fused.distances_array(), bb.distances_array()))
     # per-batch check on a prefix: digests of the stream path against the plain path
     if check_batches:
         k = min(check_batches, batches)
         gc_, bc = replica()
         gd, bd = replica()
         digs, _ = bc.apply_stream(st.src, st.dst, st.add, off[: k + 1], digests=True)
+        bd.set_fused(False)  # checked against the per-phase path
         ok = True
         for t in range(k):
             bd.apply_arrays(*st.batch(t))
