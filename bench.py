@@ -9,8 +9,12 @@ insertions, 30% deletions of loaded edges).  One step = one update batch:
 Graph.apply + IncrementalBFS repair (device-resident batch for `value`; host
 batch through the public API with the counters read back for `e2e`).
 Besides the headline, the run reports direction-optimising full BFS from 64
-roots (GTEPS and the HBM roofline of the BFS kernel), per-batch exactness
-against a fresh full BFS, and the reference's CPU path on the host cores.
+roots (GTEPS and the HBM roofline of the BFS kernel), multi-root BFS of 64
+and 256 roots, per-batch exactness against a fresh full BFS, the reference's
+CPU path on the host cores, and (under "streams") two further update
+streams measured end to end: R-MAT scale 20 with 1,000 lognormal-sized
+batches (the batched stream path against the plain one-batch-at-a-time
+path) and a 4096 x 4096 lattice with near-root deletions.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -49,6 +53,7 @@ def parse():
     p.add_argument("--check-batches", type=int, default=8)
     p.add_argument("--cpu-seconds", type=float, default=20.0, help="bound of the CPU-baseline sample")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-extras", action="store_true", help="skip the lognormal and grid stream measurements")
     p.add_argument("--seed", type=int, default=22)
     p.add_argument("--alpha", type=float, default=None, help="fix the direction switch (skips the autotune sweep)")
     p.add_argument("--beta", type=float, default=None)
@@ -169,20 +174,16 @@ def run_b200(args, rank, world, local):
     import torch
 
     torch.cuda.set_device(local)
+    from velographx_b200 import replicas
+
     dist = None
     if world > 1:
-        import datetime
-
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        replicas.init("nccl", timeout_s=120.0)
 
     def barrier_max(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, device="cuda")
 
     def barrier():
         if dist is not None:
@@ -380,6 +381,16 @@ def run_b200(args, rank, world, local):
                         "full": st["last_used_full_recompute"]},
         "clocks": clocks.summary(),
     }
+    if world == 1 and not args.no_extras:
+        # the other stream configurations, end to end (not part of the timed region above)
+        from velographx_b200 import stream_bench as sbm
+
+        del b
+        torch.cuda.synchronize()
+        line["streams"] = {
+            "lognormal_rmat20": sbm.lognormal(20, batches=1000, check_batches=100),
+            "grid4096_near_root": sbm.grid(4096, batches=500, check_every=100),
+        }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(args, V, edges, roots, stream)
     if dist is not None:
