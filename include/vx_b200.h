@@ -151,6 +151,14 @@ int vx_bfs_apply_stream(vx_bfs* b, const uint32_t* src, const uint32_t* dst, con
  * 0x9E3779B97F4A7C15, then the two xor-shift-multiply rounds and the final
  * xor-shift of Steele et al.).  No reference counterpart (verification). */
 int vx_bfs_digest(vx_bfs* b, uint64_t* out);
+/* Device memory reserved ahead of an update stream, so that no batch
+ * allocates (an allocation synchronises the device): batch buffers for
+ * batches of up to max_batch_ops ops and delta-arena room for total_ops more
+ * ops.  No reference counterpart. */
+int vx_graph_reserve(vx_graph* g, size_t max_batch_ops, size_t total_ops);
+/* The batched stream path's buffers for streams of up to `ops` ops in
+ * `batches` batches, the largest max_batch_ops ops.  No reference counterpart. */
+int vx_bfs_reserve_stream(vx_bfs* b, size_t ops, size_t batches, size_t max_batch_ops);
 /* Direction switch (alpha, beta) and grid-expanded row length of the full BFS.
  * No reference counterpart: the reference BFS is top-down only. */
 int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row);

@@ -343,6 +343,20 @@ int vx_bfs_set_fused(vx_bfs* b, int fused) {
   return VX_OK;
 }
 
+int vx_graph_reserve(vx_graph* g, size_t max_batch_ops, size_t total_ops) {
+  if (!g) return fail(VX_ERR_INVALID, "null argument");
+  if (int rc = g->g->batch.ensure(max_batch_ops)) return rc;
+  int fits = 0;
+  const int arcs_per_op = g->g->directed ? 1 : 2;  // in the out adjacency
+  if (int rc = vxh::graph_reserve_stream(g->g, 8ull * arcs_per_op * total_ops + 8, &fits)) return rc;
+  return VX_OK;  // past the arena limit the stream consolidates as it goes
+}
+
+int vx_bfs_reserve_stream(vx_bfs* b, size_t ops, size_t batches, size_t max_batch_ops) {
+  if (!b) return fail(VX_ERR_INVALID, "null argument");
+  return b->b->sb.ensure(ops, batches, 2 * std::max<size_t>(max_batch_ops, 1));
+}
+
 int vx_bfs_digest(vx_bfs* b, uint64_t* out) {
   if (!b || !out) return fail(VX_ERR_INVALID, "null argument");
   return vxh::bfs_digest(b->b, out);

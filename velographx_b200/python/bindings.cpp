@@ -181,6 +181,11 @@ PYBIND11_MODULE(_velographx, m) {
                                                  reinterpret_cast<const std::uint32_t*>(d),
                                                  reinterpret_cast<const std::uint8_t*>(a), n, vertex_count_after));
            })
+      .def("reserve",
+           [](DynamicGraph& g, std::size_t max_batch_ops, std::size_t total_ops) {
+             detail::check(vx_graph_reserve(g.handle(), max_batch_ops, total_ops));
+           },
+           py::arg("max_batch_ops"), py::arg("total_ops") = 0)
       .def_property_readonly("stream",
                              [](DynamicGraph& g) {
                                void* s = nullptr;
@@ -279,6 +284,11 @@ PYBIND11_MODULE(_velographx, m) {
            },
            py::arg("src"), py::arg("dst"), py::arg("add"), py::arg("offsets"), py::arg("digests") = false,
            py::arg("stats") = false)
+      .def("reserve_stream",
+           [](IncrementalBFS& x, std::size_t ops, std::size_t batches, std::size_t max_batch_ops) {
+             detail::check(vx_bfs_reserve_stream(x.handle(), ops, batches, max_batch_ops));
+           },
+           py::arg("ops"), py::arg("batches"), py::arg("max_batch_ops"))
       .def("set_fused", [](IncrementalBFS& x, bool fused) { detail::check(vx_bfs_set_fused(x.handle(), fused)); })
       .def("digest",
            [](IncrementalBFS& x) {
