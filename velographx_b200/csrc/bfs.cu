@@ -994,6 +994,10 @@ __device__ bool cascade(const Params& p, RepairSmem& sm, LbStage& lb, uint32_t n
     drain(p, sm, w);
     if (!sync_grid(p)) return false;
   }
+  if (gtid() == 0) {  // the drain statistics of the phase trace
+    p.c->rtrace[7] = ld_cg(p.rq_tail);
+    for (int k = 0; k < 6; ++k) p.c->rtrace[9 + k] = __ldcg(&p.rq_stat[k]);
+  }
   return true;
 }
 
@@ -1010,11 +1014,7 @@ __device__ void repair_pre(const Params& p, RepairSmem& sm, LbStage& lb) {
   if (ncand == 0) return;
   if (!cascade(p, sm, lb, ncand)) return;
   stamp(p, 2);
-  if (gtid() == 0) {
-    c->affected = ld_cg(&c->a_n);
-    c->rtrace[7] = ld_cg(p.rq_tail);
-    for (int k = 0; k < 6; ++k) c->rtrace[9 + k] = __ldcg(&p.rq_stat[k]);
-  }
+  if (gtid() == 0) c->affected = ld_cg(&c->a_n);
   reset_ring(p);  // for the post-batch kernel
 }
 
@@ -1759,7 +1759,7 @@ int bfs_recompute(Bfs* b) {
   return launch(b, p, kModeFull);
 }
 
-int bfs_stage(Bfs* b, size_t n, size_t vertex_bound) {
+int bfs_stage(Bfs* b, size_t n, size_t vertex_bound, bool classify) {
   Graph* g = b->g;
   cudaStream_t s = g->stream;
   // last_* counters reset on every apply (bfs.hpp:30-33)
@@ -1770,7 +1770,8 @@ int bfs_stage(Bfs* b, size_t n, size_t vertex_bound) {
   if (n == 0) return 0;
   VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->cand_n, 0, 3 * sizeof(uint32_t), s));
   VX_CUDA_TRY(cudaMemsetAsync(b->ctr->rtrace, 0, sizeof(b->ctr->rtrace), s));
-  if (int rc = graph_stage_batch(g, n, vertex_bound)) return rc;
+  b->staged_classified = classify;
+  if (int rc = graph_stage_batch(g, n, vertex_bound, classify)) return rc;
   if (int rc = ensure_capacity(b, std::max<size_t>(g->V, 1))) return rc;
   return ensure_ring(b);
 }
@@ -1814,7 +1815,7 @@ static int repair_fused(Bfs* b) {
   sa.V0 = (uint32_t)b->staged_V_pre;
   sa.len0 = (uint32_t)b->staged_len_pre;
   sa.v_single = (uint32_t)g->V;
-  sa.classified = 1;
+  sa.classified = b->staged_classified ? 1u : 0u;
   Params p = make_params(b, (uint32_t)g->V, (uint32_t)g->V);
   if (int rc = launch_stream(b, p, sa)) return rc;
   g->adj[0].arena_bound += 8ull * m + 8;  // the bound the staging reserved for
@@ -1863,7 +1864,9 @@ int bfs_full_staged(Bfs* b) {
 }
 
 int bfs_apply_staged(Bfs* b, size_t n, size_t vertex_bound) {
-  if (int rc = bfs_stage(b, n, vertex_bound)) return rc;
+  // the fused repair classifies the arcs itself; the per-phase path needs them classified
+  const bool fused = !b->g->directed && b->tune.fused;
+  if (int rc = bfs_stage(b, n, vertex_bound, !fused)) return rc;
   return bfs_repair_staged(b);
 }
 

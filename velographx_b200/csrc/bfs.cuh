@@ -91,6 +91,7 @@ struct Bfs {
   uint32_t* barrier = nullptr;          // grid barrier words (vxb::kBarrierWords)
   float* features = nullptr;            // selector features of the staged batch
   size_t staged_ops = 0, staged_V_pre = 0, staged_len_pre = 0;  // batch staged by bfs_stage
+  bool staged_classified = true;
   BfsTuning tune;
   int grid = 0;
   int stream_grid = 0;
@@ -105,7 +106,7 @@ int bfs_recompute(Bfs* b);
 // bfs_repair_staged (the reference's apply) or bfs_full_staged (graph apply +
 // recompute, the explicit full arm of the reference's selector harness).
 int bfs_apply_staged(Bfs* b, size_t n, size_t vertex_bound);
-int bfs_stage(Bfs* b, size_t n, size_t vertex_bound);
+int bfs_stage(Bfs* b, size_t n, size_t vertex_bound, bool classify = true);
 int bfs_repair_staged(Bfs* b);
 int bfs_full_staged(Bfs* b);
 int bfs_sync(Bfs* b);  // copies counters to hctr (synchronises the stream)

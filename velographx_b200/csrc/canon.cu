@@ -26,9 +26,12 @@ namespace {
 
 constexpr int kThreads = 1024;
 constexpr int kDigits = 256;
-constexpr int kMaxCluster = 8;
-// Two tile shapes: 4 keys per thread spreads mid-size batches over more SMs,
-// 11 keys per thread holds the largest batch one cluster can take.
+constexpr int kMaxCluster = 8;     // portable cluster size (capacity of the largest tile)
+constexpr int kMaxClusterNP = 16;  // non-portable size for the small tiles
+// Tile shapes: 1 or 2 keys per thread spread small batches over up to 16
+// CTAs (each pass is bound by its synchronisation, not by the keys), 4 keys
+// per thread mid-size ones over 8, and 11 keys per thread hold the largest
+// batch one cluster can take.
 template <int ITEMS>
 struct Tile {
   static constexpr int kItems = ITEMS;
@@ -249,12 +252,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 size_t canon_cluster_capacity() { return (size_t)kMaxCluster * Tile<11>::kTile; }
 
 template <int ITEMS>
-static int launch_canon(Graph* g, size_t n, size_t m, int b, int sh, uint32_t bound) {
+static int launch_canon(Graph* g, size_t n, size_t m, int b, int sh, uint32_t bound, bool* launched) {
   using T = Tile<ITEMS>;
+  *launched = false;
   static bool attr = false;
   if (!attr) {
     VX_CUDA_TRY(cudaFuncSetAttribute(canon_cluster_kernel<ITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)T::kSmem));
+    VX_CUDA_TRY(cudaFuncSetAttribute(canon_cluster_kernel<ITEMS>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     attr = true;
   }
   const unsigned C = (unsigned)((m + T::kTile - 1) / T::kTile);
@@ -270,11 +275,24 @@ static int launch_canon(Graph* g, size_t n, size_t m, int b, int sh, uint32_t bo
   at[0].val.clusterDim.z = 1;
   cfg.attrs = at;
   cfg.numAttrs = 1;
+  if (C > (unsigned)kMaxCluster) {  // a non-portable size: only where the device can place it
+    static int fits[kMaxClusterNP + 1] = {};
+    if (!fits[C]) {
+      int clusters = 0;
+      fits[C] = cudaOccupancyMaxActiveClusters(&clusters, canon_cluster_kernel<ITEMS>, &cfg) == cudaSuccess &&
+                        clusters > 0
+                    ? 1
+                    : -1;
+      cudaGetLastError();
+    }
+    if (fits[C] < 0) return 0;
+  }
   const int passes = (2 * b + 7) / 8;
   BatchBuffers& B = g->batch;
   count_launch();
   VX_CUDA_TRY(cudaLaunchKernelEx(&cfg, canon_cluster_kernel<ITEMS>, B.src, B.dst, B.add, (uint32_t)n,
                                  (int)g->directed, b, sh, bound, passes, B.fu, B.fv, B.ff, g->ctr));
+  *launched = true;
   return 0;
 }
 
@@ -287,9 +305,16 @@ int canon_cluster(Graph* g, size_t n, int b, uint32_t bound, bool* done) {
   while (sbits < 32 && ((size_t)1 << sbits) < n) ++sbits;
   const int sh = sbits + 1;
   if (m == 0 || m > canon_cluster_capacity() || 2 * b + sh > 64) return 0;
-  *done = true;
-  if (m <= (size_t)kMaxCluster * Tile<4>::kTile) return launch_canon<4>(g, n, m, b, sh, bound);
-  return launch_canon<11>(g, n, m, b, sh, bound);
+  bool launched = false;
+  int rc = 0;
+  if (m <= (size_t)kMaxClusterNP * Tile<1>::kTile) rc = launch_canon<1>(g, n, m, b, sh, bound, &launched);
+  if (!rc && !launched && m <= (size_t)kMaxClusterNP * Tile<2>::kTile)
+    rc = launch_canon<2>(g, n, m, b, sh, bound, &launched);
+  if (!rc && !launched && m <= (size_t)kMaxCluster * Tile<4>::kTile)
+    rc = launch_canon<4>(g, n, m, b, sh, bound, &launched);
+  if (!rc && !launched) rc = launch_canon<11>(g, n, m, b, sh, bound, &launched);
+  *done = launched;
+  return rc;
 }
 
 }  // namespace vxh

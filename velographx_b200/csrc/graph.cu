@@ -814,7 +814,7 @@ static int scan_count(Graph* g, const uint32_t* flag, uint32_t* pos, size_t m, u
   return scan_exclusive_u32(flag, pos, m, total, g->scratch, g->stream);
 }
 
-int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound) {
+int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound, bool classify) {
   cudaStream_t s = g->stream;
   BatchBuffers& B = g->batch;
   g->batch_ops = n;
@@ -839,6 +839,7 @@ int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound) {
   bool done = false;
   if (int rc = canon_cluster(g, n, b, (uint32_t)g->V, &done)) return rc;
   if (done) {
+    if (!classify) return 0;
     vxh::count_launch();
     classify_kernel<<<grid_for(m), kBlock, 0, s>>>(devadj(g->adj[0]), B.fu, B.fv, B.ff, B.fpos,
                                                     &g->ctr->final_arcs);
@@ -858,6 +859,8 @@ int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound) {
   if (int rc = scan_count(g, B.flag, B.pos, m, &g->ctr->final_arcs)) return rc;
   vxh::count_launch();
   compact_final_kernel<<<grid_for(m), kBlock, 0, s>>>(keys, vals, B.flag, B.pos, m, b, B.fu, B.fv, B.ff);
+  VX_CUDA_TRY(cudaGetLastError());
+  if (!classify) return 0;
   vxh::count_launch();
   classify_kernel<<<grid_for(m), kBlock, 0, s>>>(devadj(g->adj[0]), B.fu, B.fv, B.ff, B.fpos,
                                                   &g->ctr->final_arcs);

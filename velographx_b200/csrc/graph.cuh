@@ -101,7 +101,8 @@ int graph_grow(Graph* g, size_t vertices);
 int graph_bulk_load(Graph* g, const uint32_t* d_uv, size_t n_edges);
 // Stage a batch already in g->batch.{src,dst,add}: canonicalise + classify on
 // the pre-batch graph.  vertex_bound bounds every non-self-loop id + 1.
-int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound);
+// classify = false leaves the arcs unclassified (a fused repair classifies them itself).
+int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound, bool classify = true);
 // Apply the staged batch to the device structure (after any pre-batch reads):
 // removals first (tombstones, delta removals), then insertions.
 int graph_commit_batch(Graph* g);
