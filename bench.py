@@ -194,6 +194,9 @@ def run_b200(args, rank, world, local):
     V, edges, roots, stream = workload(args)
     g = vx.Graph(V, False)
     g.bulk_load_edges(edges)
+    # device memory for every batch of the run reserved up front (no batch
+    # allocates, and so synchronises, inside a timed region)
+    g.reserve(args.batch_ops, args.batch_ops * stream.batches)
     cs = torch.cuda.ExternalStream(g.stream)
     A = g.edge_count_directed()
 

@@ -1124,12 +1124,20 @@ struct Relax {
 // affected vertices, a block-sized chunk of them at a time: min of dist + 1
 // over non-affected in-neighbours, folded per vertex in shared memory; each
 // finite one seeds the relaxation.
+constexpr uint32_t kBigBoundary = 4096;  // in-rows this long go to the grid-wide pass
+
 __device__ void boundary_seeds(const Params& p, RepairSmem& sm, LbStage& lb, uint32_t na, long long& reach) {
   const uint32_t per = min((uint32_t)kThreads, max(1u, (na + gridDim.x - 1) / gridDim.x));
   for (uint32_t i0 = blockIdx.x * per; i0 < na; i0 += gridDim.x * per) {
     const uint32_t k = min(per, na - i0);
     if (threadIdx.x < k) {
-      sm.sv[threadIdx.x] = p.lst_a[i0 + threadIdx.x];
+      uint32_t v = p.lst_a[i0 + threadIdx.x];
+      if (degree_of(p.g.in, v) > kBigBoundary) {  // a hub: the whole grid scans it after the barrier
+        p.tent[i0 + threadIdx.x] = kUnreachable;
+        p.big[atomicAdd(&p.c->big_b, 1u)] = i0 + threadIdx.x;
+        v = 0xFFFFFFFFu;  // no row in this pass
+      }
+      sm.sv[threadIdx.x] = v;
       sm.cnt[threadIdx.x] = kUnreachable;
     }
     __syncthreads();
@@ -1141,7 +1149,7 @@ __device__ void boundary_seeds(const Params& p, RepairSmem& sm, LbStage& lb, uin
     block_rows(p.g.in, sm.sv, k, lb, bmin);
     bool seed = false;
     uint32_t v = 0;
-    if (threadIdx.x < k) {
+    if (threadIdx.x < k && sm.sv[threadIdx.x] != 0xFFFFFFFFu) {
       v = sm.sv[threadIdx.x];
       const uint32_t best = sm.cnt[threadIdx.x];
       // by atomicMin: an inserted arc may lower v first
@@ -1149,6 +1157,42 @@ __device__ void boundary_seeds(const Params& p, RepairSmem& sm, LbStage& lb, uin
     }
     seed_relax(p, seed, v, reach);
     __syncthreads();
+  }
+}
+
+// Boundary distances of the hub entries p.big[0, nb) (indices into lst_a):
+// each hub gets its own group of nwarps / nb warps (at least one), which fold
+// 32-arc slices of its row into p.tent[i] by atomicMin, so many hubs are
+// scanned side by side; the rows' seeds are taken after a barrier.
+__device__ void grid_boundary_min(const Params& p, uint32_t nb) {
+  const DevAdj& a = p.g.in;
+  const int lane = threadIdx.x & 31;
+  const uint32_t W = nwarps(), w = gwarp();
+  const uint32_t G = max(1u, W / nb), R = W / G;  // warps per hub, hubs per round
+  if (w >= R * G) return;
+  for (uint32_t r = w / G; r < nb; r += R) {
+    const uint32_t i = p.big[r];
+    const uint32_t v = p.lst_a[i];
+    uint32_t best = kUnreachable;
+    uint64_t b, e;
+    vxb::base_range(a, v, b, e);
+    const uint2 dr = a.drow[v];
+    const uint64_t nbase = e - b, total = nbase + dr.y;
+    for (uint64_t k = (uint64_t)(w % G) * 32 + lane; k < total; k += (uint64_t)G * 32) {
+      uint32_t x;
+      if (k < nbase) {
+        x = a.col[b + k];
+        if (x & kTomb) continue;
+      } else {
+        x = a.darena[dr.x + (uint32_t)(k - nbase)];
+      }
+      if (x >= p.dist_len || test_bit(p.aff, x)) continue;
+      const uint32_t dx = p.dist[x];
+      if (dx != kUnreachable && dx + 1 < best) best = dx + 1;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = min(best, __shfl_xor_sync(FULL, best, o));
+    if (lane == 0 && best != kUnreachable) atomicMin(&p.tent[i], best);
   }
 }
 
@@ -1171,7 +1215,10 @@ __device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQ
   if (na > 0) {
     // invalidate the affected vertices (repair_affected, bfs.hpp:272-283)
     for (uint32_t i = gtid(); i < na; i += nthreads()) p.dist[p.lst_a[i]] = kUnreachable;
-    if (gtid() == 0) reach_add(p, -(long long)na);
+    if (gtid() == 0) {
+      reach_add(p, -(long long)na);
+      c->big_b = 0;
+    }
     if (!sync_grid(p)) return;
     stamp(p, 4);
     boundary_seeds(p, sm, lb, na, reach);
@@ -1193,6 +1240,25 @@ __device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQ
     seed_relax(p, lowered, v, reach);
   }
   if (!sync_grid(p)) return;
+  const uint32_t nbig = na ? ld_cg(&c->big_b) : 0u;
+  if (nbig) {
+    grid_boundary_min(p, nbig);
+    if (!sync_grid(p)) return;
+    for (uint32_t base = gwarp() * 32; base < nbig; base += nwarps() * 32) {
+      const uint32_t r = base + lane;
+      bool seed = false;
+      uint32_t v = 0;
+      if (r < nbig) {
+        const uint32_t i = p.big[r];
+        v = p.lst_a[i];
+        const uint32_t best = ld_cg(&p.tent[i]);
+        p.tent[i] = 0u;  // tent is all-zero between phases (the cascade's chunk counts)
+        if (best != kUnreachable) seed = lower(p, v, best, reach);
+      }
+      seed_relax(p, seed, v, reach);
+    }
+    if (!sync_grid(p)) return;
+  }
   stamp(p, 5);
   if (ld_cg(p.rq_tail)) {  // the relaxation runs only when a seed left work queued
     Relax w{&p, &lb, &reach};

@@ -26,6 +26,7 @@ struct BfsCounters {
   uint32_t cand_n;       // deletion candidates (distinct heads)
   uint32_t touched_n;    // vertices whose support word is non-zero (lst_t)
   uint32_t a_n;          // affected list length
+  uint32_t big_b;        // affected hubs whose boundary the whole grid computes
   unsigned long long scratch64;  // single-value readbacks
   // globaltimer stamps of the last repair: pre entry, after its seeds, after
   // its cascade; post entry, after the boundary distances, after its seeds,

@@ -490,7 +490,8 @@ int alloc_array(T** p, size_t n) {
 }
 
 int grow_arena(Adjacency& a, size_t need_entries, cudaStream_t s) {
-  size_t ncap = std::max<size_t>(a.arena_cap * 2, std::max<size_t>(need_entries, 1u << 20));
+  // grows 4x at a time: a growth copies the arena and synchronises the stream
+  size_t ncap = std::max<size_t>(a.arena_cap * 4, std::max<size_t>(need_entries, 1u << 22));
   if (ncap >= 0xFFFFFFFFull) ncap = 0xFFFFFFFFull - 1;
   if (ncap < need_entries) {
     set_error("delta arena would exceed 2^32 entries");
