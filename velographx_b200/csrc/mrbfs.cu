@@ -37,6 +37,7 @@ struct MrParams {
   uint32_t* touched; // bitmap
   uint32_t* q[3];    // rotating frontier queues
   uint32_t* tl;      // touched list of a push level
+  uint32_t* big;     // frontier rows of a push level that the whole grid expands
   uint32_t* dist;    // [K][V]
   MrCounters* c;
   uint32_t* bar;
@@ -93,6 +94,109 @@ struct PushVisit {
   }
 };
 
+constexpr uint32_t kMrHead = 8;       // in-arcs a lane pulls itself before its warp helps
+constexpr uint32_t kMrBigRow = 4096;  // push rows this long are expanded by the whole grid
+
+// Pull level: one warp per 32 vertices.  Each lane ORs the frontier words of
+// the first kMrHead in-neighbours of its vertex; the rest of a longer row is
+// read by the whole warp, 32 arcs per step, the words OR-reduced across the
+// warp, until every root has reached the vertex or the row ends.
+template <uint32_t W>
+__device__ void pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, uint32_t level, uint32_t* qn,
+                           uint32_t* qout) {
+  const DevAdj& a = p.g.in;
+  const int lane = threadIdx.x & 31;
+  for (uint32_t base = gwarp() * 32; base < p.V; base += nwarps() * 32) {
+    const uint32_t v = base + lane;
+    uint32_t vis[W], acc[W];
+    bool done = true;
+#pragma unroll
+    for (uint32_t w = 0; w < W; ++w) {
+      vis[w] = v < p.V ? p.vis[(size_t)v * W + w] : word_mask(p, w);
+      acc[w] = 0;
+      done = done && vis[w] == word_mask(p, w);
+    }
+    const bool todo = !done;
+    uint64_t b = 0, e = 0;
+    uint2 dr = make_uint2(0, 0);
+    if (todo) {
+      vxb::base_range(a, v, b, e);
+      dr = a.drow[v];
+    }
+    const uint32_t nb = (uint32_t)(e - b), total = nb + dr.y;
+    const uint32_t head = todo ? min(total, kMrHead) : 0u;
+    for (uint32_t j = 0; j < head && !done; ++j) {
+      uint32_t x;
+      if (j < nb) {
+        x = a.col[b + j];
+        if (x & kTomb) continue;
+      } else {
+        x = a.darena[dr.x + (j - nb)];
+      }
+      done = true;
+#pragma unroll
+      for (uint32_t w = 0; w < W; ++w) {
+        acc[w] |= fc[(size_t)x * W + w] & ~vis[w];
+        done = done && (vis[w] | acc[w]) == word_mask(p, w);
+      }
+    }
+    uint32_t longm = __ballot_sync(FULL, todo && !done && total > head);
+    while (longm) {
+      const int l = __ffs(longm) - 1;
+      longm &= longm - 1;
+      const uint64_t bb = __shfl_sync(FULL, b, l);
+      const uint32_t nbl = __shfl_sync(FULL, nb, l), tot = __shfl_sync(FULL, total, l);
+      const uint32_t dx = __shfl_sync(FULL, dr.x, l);
+      uint32_t vl[W], al[W];
+#pragma unroll
+      for (uint32_t w = 0; w < W; ++w) {
+        vl[w] = __shfl_sync(FULL, vis[w], l);
+        al[w] = __shfl_sync(FULL, acc[w], l);
+      }
+      bool full = false;
+      for (uint32_t k0 = kMrHead; k0 < tot && !full; k0 += 32) {
+        const uint32_t k = k0 + lane;
+        uint32_t add[W];
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w) add[w] = 0;
+        if (k < tot) {
+          uint32_t x = 0;
+          bool valid = true;
+          if (k < nbl) {
+            x = a.col[bb + k];
+            valid = !(x & kTomb);
+          } else {
+            x = a.darena[dx + (k - nbl)];
+          }
+          if (valid)
+#pragma unroll
+            for (uint32_t w = 0; w < W; ++w) add[w] = fc[(size_t)(x & kIdMask) * W + w];
+        }
+        full = true;
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w) {
+          al[w] |= __reduce_or_sync(FULL, add[w]) & ~vl[w];
+          full = full && (vl[w] | al[w]) == word_mask(p, w);
+        }
+      }
+      if (lane == l)
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w) acc[w] = al[w];
+    }
+    bool any = false;
+#pragma unroll
+    for (uint32_t w = 0; w < W; ++w) {
+      if (!todo || !acc[w]) continue;
+      any = true;
+      p.vis[(size_t)v * W + w] = vis[w] | acc[w];
+      fn[(size_t)v * W + w] = acc[w];
+      write_dists(p, v, w, acc[w], level + 1);
+    }
+    const uint32_t slot = vxb::warp_append(any, qn);
+    if (any) qout[slot] = v;
+  }
+}
+
 template <uint32_t W>
 __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
   MrCounters* c = p.c;
@@ -122,6 +226,7 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
     if (gtid() == 0) {
       c->qn[clr] = 0;
       c->tn = 0;
+      c->nbig = 0;
     }
     // frontier words of level-1 are no longer read: clear them for reuse
     for (uint32_t i = gtid(); i < prev_n * W; i += nthreads()) p.frn[clr][(size_t)p.q[clr][i / W] * W + i % W] = 0u;
@@ -130,47 +235,7 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
     if ((float)n_f > p.pull_frac * (float)p.V) {
       // pull: every vertex not reached by all roots ORs its in-neighbours'
       // frontier words, stopping once all roots reached it
-      const DevAdj& a = p.g.in;
-      for (uint32_t v = gtid(); v < p.V; v += nthreads()) {
-        uint32_t vis[W], acc[W];
-        bool full = true;
-#pragma unroll
-        for (uint32_t w = 0; w < W; ++w) {
-          vis[w] = p.vis[(size_t)v * W + w];
-          acc[w] = 0;
-          full = full && vis[w] == word_mask(p, w);
-        }
-        if (full) continue;
-        uint64_t b, e;
-        vxb::base_range(a, v, b, e);
-        const uint2 dr = a.drow[v];
-        const uint64_t nb = e - b;
-        for (uint64_t j = 0; j < nb + dr.y && !full; ++j) {
-          uint32_t x;
-          if (j < nb) {
-            x = a.col[b + j];
-            if (x & kTomb) continue;
-          } else {
-            x = a.darena[dr.x + (uint32_t)(j - nb)];
-          }
-          full = true;
-#pragma unroll
-          for (uint32_t w = 0; w < W; ++w) {
-            acc[w] |= fc[(size_t)x * W + w] & ~vis[w];
-            full = full && (vis[w] | acc[w]) == word_mask(p, w);
-          }
-        }
-        bool any = false;
-#pragma unroll
-        for (uint32_t w = 0; w < W; ++w) {
-          if (!acc[w]) continue;
-          any = true;
-          p.vis[(size_t)v * W + w] = vis[w] | acc[w];
-          fn[(size_t)v * W + w] = acc[w];
-          write_dists(p, v, w, acc[w], level + 1);
-        }
-        if (any) p.q[nx][atomicAdd(&c->qn[nx], 1u)] = v;
-      }
+      pull_level<W>(p, fc, fn, level, &c->qn[nx], p.q[nx]);
       if (!mr_sync(p)) return;
     } else {
       // push along the rows of the queued frontier vertices, one warp each
@@ -178,11 +243,35 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
       PushVisit<W> pv{&p, {}, &c->tn};
       for (uint32_t i = gwarp(); i < n_f; i += nwarps()) {
         const uint32_t u = p.q[cur][i];
+        if (degree_of(a, u) >= kMrBigRow) {  // a hub: the whole grid, after the barrier
+          if ((threadIdx.x & 31) == 0) p.big[atomicAdd(&c->nbig, 1u)] = u;
+          continue;
+        }
 #pragma unroll
         for (uint32_t w = 0; w < W; ++w) pv.fw[w] = fc[(size_t)u * W + w];
         warp_row(a, u, pv);
       }
       if (!mr_sync(p)) return;
+      const uint32_t nbig = __ldcg(&c->nbig);
+      for (uint32_t r = 0; r < nbig; ++r) {  // every warp takes 32-arc slices of each hub row
+        const uint32_t u = p.big[r];
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w) pv.fw[w] = fc[(size_t)u * W + w];
+        uint64_t b, e;
+        vxb::base_range(a, u, b, e);
+        for (uint64_t j0 = b + (uint64_t)gwarp() * 32; j0 < e; j0 += (uint64_t)nwarps() * 32) {
+          const uint64_t j = j0 + (threadIdx.x & 31);
+          const uint32_t x = j < e ? a.col[j] : kTomb;
+          pv(!(x & kTomb), x & kIdMask, u);
+        }
+        const uint2 dr = a.drow[u];
+        for (uint32_t j0 = dr.x + gwarp() * 32; j0 < dr.x + dr.y; j0 += nwarps() * 32) {
+          const uint32_t j = j0 + (threadIdx.x & 31);
+          const bool ok = j < dr.x + dr.y;
+          pv(ok, ok ? a.darena[j] : 0u, u);
+        }
+      }
+      if (nbig && !mr_sync(p)) return;
       const uint32_t nt = __ldcg(&c->tn);
       for (uint32_t i = gtid(); i < nt; i += nthreads()) {
         const uint32_t x = p.tl[i];
@@ -239,7 +328,8 @@ int mrbfs_create(MrBfs** out, Graph* g, const uint32_t* host_roots, size_t k) {
   const size_t vw = V * m->W;
   bool ok = cudaMalloc(&m->roots, k * 4) == cudaSuccess && cudaMalloc(&m->vis, vw * 4) == cudaSuccess &&
             cudaMalloc(&m->nxt, vw * 4) == cudaSuccess && cudaMalloc(&m->touched, ((V + 31) / 32) * 4) == cudaSuccess &&
-            cudaMalloc(&m->tl, V * 4) == cudaSuccess && cudaMalloc(&m->dist, V * k * 4) == cudaSuccess &&
+            cudaMalloc(&m->tl, V * 4) == cudaSuccess && cudaMalloc(&m->big, V * 4) == cudaSuccess &&
+            cudaMalloc(&m->dist, V * k * 4) == cudaSuccess &&
             cudaMalloc(&m->ctr, sizeof(MrCounters)) == cudaSuccess &&
             cudaMalloc(&m->barrier, vxb::kBarrierWords * 4) == cudaSuccess &&
             cudaMallocHost(&m->hctr, sizeof(MrCounters)) == cudaSuccess;
@@ -260,7 +350,7 @@ int mrbfs_create(MrBfs** out, Graph* g, const uint32_t* host_roots, size_t k) {
 void mrbfs_destroy(MrBfs* m) {
   if (!m) return;
   if (m->g && m->g->stream) cudaStreamSynchronize(m->g->stream);
-  void* ptrs[] = {m->roots, m->vis, m->nxt, m->touched, m->tl, m->dist, m->ctr, m->barrier,
+  void* ptrs[] = {m->roots, m->vis, m->nxt, m->touched, m->tl, m->big, m->dist, m->ctr, m->barrier,
                   m->frn[0], m->frn[1], m->frn[2], m->q[0], m->q[1], m->q[2]};
   for (void* p : ptrs) cudaFree(p);
   cudaFreeHost(m->hctr);
@@ -308,6 +398,7 @@ int mrbfs_run(MrBfs* m) {
   p.nxt = m->nxt;
   p.touched = m->touched;
   p.tl = m->tl;
+  p.big = m->big;
   p.dist = m->dist;
   p.c = m->ctr;
   p.bar = m->barrier;

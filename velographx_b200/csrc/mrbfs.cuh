@@ -13,6 +13,7 @@ constexpr uint32_t kMaxRoots = 256;
 struct MrCounters {
   uint32_t qn[3];   // rotating frontier queue lengths
   uint32_t tn;      // touched heads of a push level
+  uint32_t nbig;    // frontier rows of a push level long enough for the whole grid
   uint32_t levels;
   uint32_t err;
   unsigned long long arcs;  // reached-arc total (mrbfs_reached_arcs)
@@ -28,6 +29,7 @@ struct MrBfs {
   uint32_t* touched = nullptr;
   uint32_t* q[3] = {nullptr, nullptr, nullptr};
   uint32_t* tl = nullptr;
+  uint32_t* big = nullptr;  // hub rows of a push level
   uint32_t* dist = nullptr;  // [K][V]
   MrCounters* ctr = nullptr;
   MrCounters* hctr = nullptr;
