@@ -149,6 +149,59 @@ def grid(side: int = 4096, long_range: float = 0.001, batches: int = 500, ops: i
     return res
 
 
+def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int = 14) -> dict:
+    """Undirected R-MAT scale 14, full BFS from the max-degree vertex, then 100
+    batches of 64 uniform-random insertions: the plain path (one batch per
+    call, counters read back) and the batched path, with the distance digest
+    after every batch; returns the stream (for a check elsewhere) with the
+    timings."""
+    import torch
+
+    V = 1 << scale
+    edges = w.rmat_edges(scale, 16, seed=seed)
+    root = w.max_degree_root(edges, V)
+    rng = np.random.default_rng(seed + 1)
+    src = rng.integers(0, V, batches * ops, dtype=np.uint32)
+    dst = rng.integers(0, V, batches * ops, dtype=np.uint32)
+    add = np.ones(batches * ops, np.uint8)
+    st = pinned_stream(w.Stream(src, dst, add, np.arange(batches + 1, dtype=np.int64) * ops))
+    off = st.offsets.astype(np.uint64)
+    out = {"workload": f"rmat{scale}-undirected-ef16-{batches}x{ops}-insertions", "vertices": V, "root": int(root),
+           "batches": batches}
+    e0, e1 = _events()
+    g = Graph(V, False)
+    g.bulk_load_edges(edges)
+    g.reserve(ops, ops * batches)
+    b = IncrementalBFS(g, root)
+    cs = torch.cuda.ExternalStream(g.stream)
+    torch.cuda.synchronize()
+    e0.record(cs)
+    plain_digests = []
+    for t in range(batches):
+        b.apply_arrays(*st.batch(t))
+        b.stats()
+        plain_digests.append(b.digest())
+    e1.record(cs)
+    torch.cuda.synchronize()
+    out["plain"] = {"batches_per_s": batches / (e0.elapsed_time(e1) * 1e-3)}
+    g2 = Graph(V, False)
+    g2.bulk_load_edges(edges)
+    g2.reserve(ops, ops * batches)
+    b2 = IncrementalBFS(g2, root)
+    b2.reserve_stream(batches * ops, batches, ops)
+    cs2 = torch.cuda.ExternalStream(g2.stream)
+    torch.cuda.synchronize()
+    e0.record(cs2)
+    digs, _ = b2.apply_stream(st.src, st.dst, st.add, off, digests=True)
+    e1.record(cs2)
+    torch.cuda.synchronize()
+    out["batched"] = {"batches_per_s": batches / (e0.elapsed_time(e1) * 1e-3)}
+    out["digests"] = [int(x) for x in digs]
+    out["plain_equals_batched"] = out["digests"] == [int(x) for x in plain_digests]
+    out["_stream"] = (edges, st, root)
+    return out
+
+
 def lognormal(scale: int = 20, batches: int = 1000, median: float = 500.0, sigma: float = 2.0,
               insert_fraction: float = 0.8, seed: int = 33, check_batches: int = 200) -> dict:
     """Batched stream (one apply_stream call: upload, stream-wide
