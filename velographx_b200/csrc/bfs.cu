@@ -104,12 +104,16 @@ struct TdVisit {
     const uint32_t bit = 1u << (x & 31);
     if (valid) {
       const uint32_t w = p->vis[x >> 5];
-      if (!(w & bit)) claim = !(atomicOr(&p->vis[x >> 5], bit) & bit);
+      if (!(w & bit)) {
+        // the row length is loaded before the claim, so both are in flight together
+        const uint64_t deg = want_deg ? degree_of(p->g.out, x) : 0ull;
+        claim = !(atomicOr(&p->vis[x >> 5], bit) & bit);
+        if (claim) mloc += deg;
+      }
     }
     if (claim) {
       p->dist[x] = level + 1;
       atomicOr(&fbn[x >> 5], bit);
-      if (want_deg) mloc += degree_of(p->g.out, x);
     }
     bq_push(*bq, claim, x, cnt_n, qout);
   }
@@ -351,12 +355,17 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
   if (threadIdx.x == 0) bq.cnt = 0;
   const uint32_t V = p.V;
   const uint32_t words = (V + 31) >> 5;
-  for (uint32_t i = gtid(); i < V; i += nthreads()) p.dist[i] = kUnreachable;
+  // one pass sets every vertex unreached and the source at level 0 (bits
+  // past V count as visited, so bottom-up never scans them)
+  const uint32_t s = p.source;
+  const bool has_source = s < V;
+  for (uint32_t i = gtid(); i < V; i += nthreads()) p.dist[i] = i == s ? 0u : kUnreachable;
   for (uint32_t i = gtid(); i < words; i += nthreads()) {
-    // bits past V count as visited so bottom-up never scans them
     const uint32_t lo = i * 32;
-    p.vis[i] = (lo + 32 <= V) ? 0u : (FULL << (V - lo));
-    p.fb[0][i] = p.fb[1][i] = p.fb[2][i] = 0u;
+    const uint32_t sbit = has_source && i == (s >> 5) ? 1u << (s & 31) : 0u;
+    p.vis[i] = ((lo + 32 <= V) ? 0u : (FULL << (V - lo))) | sbit;
+    p.fb[0][i] = sbit;
+    p.fb[1][i] = p.fb[2][i] = 0u;
   }
   if (gtid() == 0) {
     for (int k = 0; k < 3; ++k) {
@@ -364,38 +373,32 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
       c->lvl_big[k] = 0;
       c->lvl_m[k] = 0;
     }
-  }
-  if (!sync_grid(p)) return;
-  if (p.source >= V) {
-    if (gtid() == 0) {
+    if (has_source) {
+      p.q[0][0] = s;
+      c->lvl_n[0] = 1;
+      c->lvl_m[0] = degree_of(p.g.out, s);
+    } else {
       c->reachable = 0;
       c->levels = 0;
       c->arcs = 0;
     }
-    return;
   }
-  if (gtid() == 0) {
-    const uint32_t s = p.source;
-    p.dist[s] = 0;
-    p.vis[s >> 5] |= 1u << (s & 31);
-    p.fb[0][s >> 5] |= 1u << (s & 31);
-    p.q[0][0] = s;
-    c->lvl_n[0] = 1;
-    c->lvl_m[0] = degree_of(p.g.out, s);
-  }
-  if (!sync_grid(p)) return;
-  unsigned long long m_visited = 0, reached = 0;
+  if (!sync_grid(p) || !has_source) return;
+  unsigned long long m_visited = 0;
+  uint32_t reached = 0;
   bool bottom_up = false, left_bu = false;
   uint32_t prev_n = 0;
   uint32_t level = 0;
+  // the frontier size and arc count of the current level, read once after the
+  // barrier that ends the level before it
+  uint32_t n_f = ld_cg(&c->lvl_n[0]);
+  unsigned long long m_f = __ldcg(&c->lvl_m[0]);
   for (;; ++level) {
     if (level > V + 1) {
       if (gtid() == 0) atomicOr(&c->err, vxb::kErrLoopBound);
       break;
     }
     const int cur = level % 3, nxt = (level + 1) % 3, clr = (level + 2) % 3;
-    const uint32_t n_f = ld_cg(&c->lvl_n[cur]);
-    const unsigned long long m_f = __ldcg(&c->lvl_m[cur]);
     if (n_f == 0) break;
     reached += n_f;
     m_visited += m_f;
@@ -415,11 +418,19 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
         p.trace[2 * level + 1] = (unsigned long long)n_f | ((unsigned long long)bottom_up << 63);
       }
     }
-    // clear the frontier bitmap of level-1 through its queue
-    for (uint32_t i = gtid(); i < prev_n; i += nthreads()) p.fb[clr][p.q[clr][i] >> 5] = 0u;
+    // clear the frontier bitmap of level-1: through its queue when it was
+    // small, else word by word (plain stores, no dependent queue loads)
+    if ((unsigned long long)prev_n * 8 < words) {
+      for (uint32_t i = gtid(); i < prev_n; i += nthreads()) p.fb[clr][p.q[clr][i] >> 5] = 0u;
+    } else {
+      for (uint32_t i = gtid(); i < words; i += nthreads()) p.fb[clr][i] = 0u;
+    }
     if (bottom_up) {
       bu_level(p, level, p.fb[cur], p.fb[nxt], p.q[nxt], &c->lvl_n[nxt], bq);
       if (!sync_grid(p)) return;
+      prev_n = n_f;
+      n_f = ld_cg(&c->lvl_n[nxt]);
+      m_f = __ldcg(&c->lvl_m[nxt]);
     } else {
       TdVisit t{&p, level, p.q[nxt], p.fb[nxt], &c->lvl_n[nxt], !left_bu, 0ull, &bq};
       if (n_f <= kLbMax) td_level_lb(p, t, p.q[cur], n_f, lbst);
@@ -427,15 +438,20 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
       t.flush(&c->lvl_m[nxt]);
       bq_flush(bq, &c->lvl_n[nxt], p.q[nxt]);
       if (!sync_grid(p)) return;
+      // three independent loads: the next level's figures stand unless hub rows remain
+      prev_n = n_f;
       const uint32_t nbig = ld_cg(&c->lvl_big[cur]);
+      n_f = ld_cg(&c->lvl_n[nxt]);
+      m_f = __ldcg(&c->lvl_m[nxt]);
       if (nbig) {
         grid_rows(p.g.out, p.big, nbig, t);
         t.flush(&c->lvl_m[nxt]);
         bq_flush(bq, &c->lvl_n[nxt], p.q[nxt]);
         if (!sync_grid(p)) return;
+        n_f = ld_cg(&c->lvl_n[nxt]);
+        m_f = __ldcg(&c->lvl_m[nxt]);
       }
     }
-    prev_n = n_f;
   }
   if (gtid() == 0) {
     c->reachable = reached;

@@ -27,13 +27,13 @@ constexpr uint32_t kTomb = 0x80000000u;
 constexpr uint32_t kIdMask = 0x7FFFFFFFu;
 constexpr uint32_t kMaxVertices = 0x7FFFFFFFu;  // ids must leave bit 31 free
 
-// Device error word bits (VX_DEVERR_* in vx_b200.h mirror these).
+// Device error word bits (reported as VX_ERR_DEVICE, with the word in the
+// message, by the next synchronising call).
 constexpr uint32_t kErrBarrierTimeout = 1u << 0;
 constexpr uint32_t kErrLoopBound = 1u << 1;
 constexpr uint32_t kErrArenaOverflow = 1u << 2;
 constexpr uint32_t kErrBadVertex = 1u << 3;
 constexpr uint32_t kErrDrainTimeout = 1u << 4;  // a repair work ring stopped draining
-constexpr uint32_t kErrQueueOverflow = 1u << 4;
 
 struct DevAdj {
   const uint64_t* off;  // [Vb + 1]
@@ -119,49 +119,33 @@ __device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t 
   return lo;
 }
 
-// Grid-wide barrier for cooperative (co-resident) launches, two levels deep:
-// blocks arrive on one of kBarrierGroups counters (each on its own 128-byte
-// line), the last arrival of a group arrives on the top counter, and the last
-// group releases everyone by bumping the generation word.  bar layout (u32):
-// [0] generation, [32 * (1 + g)] group g, [32 * (1 + kBarrierGroups)] top;
-// kBarrierWords words, zeroed at setup.  The wait is bounded: after
-// kBarrierSpinLimit polls a block records kErrBarrierTimeout in *err and
+// Grid-wide barrier for cooperative (co-resident) launches on one arrival
+// word.  Block 0 adds 2^31 - (nblocks - 1) and every other block adds 1, so
+// the word's low 31 bits return to zero and its top bit flips exactly when
+// the last block of a barrier arrives; each block waits until the top bit
+// differs from the one its own arrival returned.  The critical path after the
+// last arrival is that one atomic and the pollers' next load, with no separate
+// release step.  bar[0] is the word (kBarrierWords words, zeroed at setup:
+// the low bits must be zero when a barrier starts).  The wait is bounded:
+// after kBarrierSpinLimit polls a block records kErrBarrierTimeout in *err and
 // proceeds, so a broken launch ends instead of hanging the device.
-constexpr uint32_t kBarrierGroups = 16;
-constexpr uint32_t kBarrierWords = 32 * (kBarrierGroups + 2);
+constexpr uint32_t kBarrierWords = 32;
 constexpr uint32_t kBarrierSpinLimit = 1u << 22;
 
 __device__ __forceinline__ void grid_barrier(uint32_t* bar, uint32_t nblocks, uint32_t* err) {
   __syncthreads();
   if (threadIdx.x == 0) {
-    volatile uint32_t* vgen = bar;
-    const uint32_t gen = *vgen;
+    const uint32_t inc = blockIdx.x == 0 ? 0x80000000u - (nblocks - 1u) : 1u;
     __threadfence();
-    const uint32_t g = blockIdx.x % kBarrierGroups;
-    const uint32_t gsize = nblocks / kBarrierGroups + (g < nblocks % kBarrierGroups ? 1u : 0u);
-    const uint32_t ngroups = nblocks < kBarrierGroups ? nblocks : kBarrierGroups;
-    uint32_t* gc = bar + 32 * (1 + g);
-    uint32_t* top = bar + 32 * (1 + kBarrierGroups);
-    bool release = false;
-    if (atomicAdd(gc, 1u) == gsize - 1) {
-      atomicExch(gc, 0u);
-      if (atomicAdd(top, 1u) == ngroups - 1) {
-        atomicExch(top, 0u);
-        release = true;
+    const uint32_t old = atomicAdd(bar, inc);
+    volatile uint32_t* v = bar;
+    uint32_t spins = 0;
+    while (((*v ^ old) & 0x80000000u) == 0u) {
+      if (++spins > kBarrierSpinLimit) {
+        atomicOr(err, kErrBarrierTimeout);
+        break;
       }
-    }
-    if (release) {
-      __threadfence();
-      atomicAdd(bar, 1u);
-    } else {
-      uint32_t spins = 0;
-      while (*vgen == gen) {
-        if (++spins > kBarrierSpinLimit) {
-          atomicOr(err, kErrBarrierTimeout);
-          break;
-        }
-        if (spins > 64) __nanosleep(spins < 1024 ? 32 : 256);
-      }
+      if (spins > 64) __nanosleep(spins < 1024 ? 32 : 256);
     }
     __threadfence();
   }
