@@ -275,6 +275,14 @@ def run_b200(args, rank, world, local):
         marcs = mr.reached_arcs()
         multiroot[str(k)] = {"ms": ms, "ms_runs": [round(x, 3) for x in runs],
                              "gteps": marcs / 2 / (ms * 1e-3) / 1e9, "levels": mr.levels}
+        if k == 64:  # rows of the last run against single-root full BFS (untimed)
+            d = mr.distances_array()
+            rows = (0, 21, 42, 63)
+            multiroot[str(k)]["rows_equal_single_root"] = {
+                "rows": list(rows),
+                "exact": all(np.array_equal(d[r], vx.IncrementalBFS(g, int(rr[r])).distances_array())
+                             for r in rows)}
+            del d
         del mr
 
     # ---- update stream, device-resident batches (value) ----

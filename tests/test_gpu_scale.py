@@ -145,6 +145,25 @@ def test_multiroot_matches_single_root(scale, directed, k):
         assert np.array_equal(got[r], exp), f"root index {r}"
 
 
+@pytest.mark.parametrize("scale,k", [(18, 64), (16, 256)])
+def test_multiroot_with_hub_rows_repeated_runs(scale, k):
+    """Graphs whose hubs (rows of >= 4096 arcs) go through the grid-wide push
+    pass; three runs over the same buffers must each equal the oracle."""
+    V = 1 << scale
+    e = w.rmat_edges(scale, seed=40 + scale)
+    g = vx.Graph(V, False)
+    g.bulk_load_edges(e)
+    roots = w.non_isolated_roots(e, V, k, seed=scale)
+    csr = oracle_csr(e, V, False)
+    exp = np.stack([oracle_bfs(e, V, int(r), False, csr) for r in roots.tolist()])
+    m = vx.MultiRootBFS(g, roots)
+    for run in range(3):
+        m.run()
+        got = m.distances_array()
+        bad = [r for r in range(k) if not np.array_equal(got[r], exp[r])]
+        assert not bad, f"run {run}: rows {bad[:8]} differ"
+
+
 def test_multiroot_on_updated_graph():
     """Tombstoned base arcs and delta rows are traversed like the logical graph."""
     V = 1 << 12
@@ -164,3 +183,6 @@ def test_multiroot_on_updated_graph():
     for r, root in enumerate(roots.tolist()):
         ob = OracleBFS(og, root)
         assert np.array_equal(got[r], ob.distances()), r
+    # a second run over the same buffers gives the same rows
+    m.run()
+    assert np.array_equal(m.distances_array(), got)

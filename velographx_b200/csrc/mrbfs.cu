@@ -223,13 +223,18 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
     const int cur = level % 3, nx = (level + 1) % 3, clr = (level + 2) % 3;
     const uint32_t n_f = __ldcg(&c->qn[cur]);
     if (n_f == 0) break;
-    if (gtid() == 0) {
+    if (gtid() == 0) {  // counters of level+2: no block uses them before the next barrier
       c->qn[clr] = 0;
-      c->tn = 0;
-      c->nbig = 0;
+      c->tn[clr] = 0;
+      c->nbig[clr] = 0;
     }
-    // frontier words of level-1 are no longer read: clear them for reuse
-    for (uint32_t i = gtid(); i < prev_n * W; i += nthreads()) p.frn[clr][(size_t)p.q[clr][i / W] * W + i % W] = 0u;
+    // frontier words of level-1 are no longer read: clear them for reuse,
+    // through its queue when it was small, else all of them with plain stores
+    if ((unsigned long long)prev_n * 8 < p.V) {
+      for (uint32_t i = gtid(); i < prev_n * W; i += nthreads()) p.frn[clr][(size_t)p.q[clr][i / W] * W + i % W] = 0u;
+    } else {
+      for (size_t i = gtid(); i < (size_t)p.V * W; i += nthreads()) p.frn[clr][i] = 0u;
+    }
     const uint32_t* fc = p.frn[cur];
     uint32_t* fn = p.frn[nx];
     if ((float)n_f > p.pull_frac * (float)p.V) {
@@ -240,11 +245,11 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
     } else {
       // push along the rows of the queued frontier vertices, one warp each
       const DevAdj& a = p.g.out;
-      PushVisit<W> pv{&p, {}, &c->tn};
+      PushVisit<W> pv{&p, {}, &c->tn[cur]};
       for (uint32_t i = gwarp(); i < n_f; i += nwarps()) {
         const uint32_t u = p.q[cur][i];
         if (degree_of(a, u) >= kMrBigRow) {  // a hub: the whole grid, after the barrier
-          if ((threadIdx.x & 31) == 0) p.big[atomicAdd(&c->nbig, 1u)] = u;
+          if ((threadIdx.x & 31) == 0) p.big[atomicAdd(&c->nbig[cur], 1u)] = u;
           continue;
         }
 #pragma unroll
@@ -252,7 +257,7 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
         warp_row(a, u, pv);
       }
       if (!mr_sync(p)) return;
-      const uint32_t nbig = __ldcg(&c->nbig);
+      const uint32_t nbig = __ldcg(&c->nbig[cur]);
       for (uint32_t r = 0; r < nbig; ++r) {  // every warp takes 32-arc slices of each hub row
         const uint32_t u = p.big[r];
 #pragma unroll
@@ -272,7 +277,7 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
         }
       }
       if (nbig && !mr_sync(p)) return;
-      const uint32_t nt = __ldcg(&c->tn);
+      const uint32_t nt = __ldcg(&c->tn[cur]);
       for (uint32_t i = gtid(); i < nt; i += nthreads()) {
         const uint32_t x = p.tl[i];
         bool any = false;

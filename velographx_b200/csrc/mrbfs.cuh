@@ -11,9 +11,12 @@ namespace vxh {
 constexpr uint32_t kMaxRoots = 256;
 
 struct MrCounters {
-  uint32_t qn[3];   // rotating frontier queue lengths
-  uint32_t tn;      // touched heads of a push level
-  uint32_t nbig;    // frontier rows of a push level long enough for the whole grid
+  // Per-level counters rotate over three slots (level % 3); a level's slots
+  // are cleared two levels ahead, so no block can clear a count that another
+  // block has already started for the current level.
+  uint32_t qn[3];    // frontier queue lengths
+  uint32_t tn[3];    // touched heads of a push level
+  uint32_t nbig[3];  // frontier rows of a push level long enough for the whole grid
   uint32_t levels;
   uint32_t err;
   unsigned long long arcs;  // reached-arc total (mrbfs_reached_arcs)
