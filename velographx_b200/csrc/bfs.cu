@@ -762,7 +762,51 @@ __device__ __forceinline__ void request_check(const Params& p, bool pred, uint32
   ring_push(p, push, x);
 }
 
-// check(x), whole warp.
+// First position k in [lo, hi) of x's in-row (base part [b, b + nb), delta
+// part from darena[dx]) whose tail y survives, sits at distance d - 1 and is
+// not affected; whole warp, warp-uniform result.  Each step covers 128 arcs:
+// every lane issues its four column loads, then the four distance and
+// affected-bit loads, so a step costs two dependent round trips however many
+// of its arcs are needed.
+__device__ __forceinline__ bool find_parent(const Params& p, const DevAdj& a, uint64_t b, uint32_t nb, uint32_t dx,
+                                            uint32_t lo, uint32_t hi, uint32_t d, uint32_t& kw, uint32_t& yw) {
+  const int lane = threadIdx.x & 31;
+  for (uint32_t k0 = lo; k0 < hi; k0 += 128) {
+    uint32_t y[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const uint32_t k = k0 + 32 * j + lane;
+      y[j] = kTomb;  // no arc
+      if (k < hi) y[j] = k < nb ? a.col[b + k] : a.darena[dx + (k - nb)];
+    }
+    uint32_t dy[4], aw[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const bool live = !(y[j] & kTomb) && y[j] < p.dist_len;
+      dy[j] = live ? p.dist[y[j]] : kUnreachable;
+      aw[j] = live ? __ldcg(&p.aff[y[j] >> 5]) : 0u;
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const bool ok = dy[j] != kUnreachable && dy[j] + 1 == d && !((aw[j] >> (y[j] & 31)) & 1u);
+      const uint32_t ball = __ballot_sync(FULL, ok);
+      if (ball) {
+        const int f = __ffs(ball) - 1;
+        kw = k0 + 32 * j + (uint32_t)f;
+        yw = __shfl_sync(FULL, y[j], f);
+        return true;
+      }
+    }
+  }
+  return false;
+}
+
+// check(x), whole warp.  The scan resumes at the position saved in sw[x]:
+// affectedness only grows and distances are fixed during the cascade, so an
+// arc that failed once fails again.  In-rows longer than kChunk arcs are
+// scanned in place over their first chunk only; when it holds no witness the
+// rest goes to a chunked pass (chunk_check), and the saved position kChunk
+// tells later checks to go straight to a new pass.
 __device__ void check_vertex(const Params& p, uint32_t x) {
   const DevAdj& a = p.g.in;
   const int lane = threadIdx.x & 31;
@@ -774,45 +818,12 @@ __device__ void check_vertex(const Params& p, uint32_t x) {
   vxb::base_range(a, x, b, e);
   const uint2 dr = a.drow[x];
   const uint32_t nb = (uint32_t)(e - b), total = nb + dr.y;
-  if (total > kChunk) {
-    // long in-row: one chunk-check item per kChunk arcs, scanned by many warps;
-    // tent[x] counts the chunks of the pass in flight.  A request that finds a
-    // pass in flight is covered by it: the pass clears tent[x] before it
-    // verifies its final witness.
-    const uint32_t K = (total + kChunk - 1) / kChunk;
-    bool start = false;
-    if (lane == 0) start = atomicCAS(&p.tent[x], 0u, K) == 0u;
-    start = __shfl_sync(FULL, start, 0);
-    if (start)
-      for (uint32_t c0 = 0; c0 < K; c0 += 32)
-        ring_push(p, c0 + lane < K, kChunkCheckBit | ((unsigned long long)(c0 + lane) << 32) | x);
-    return;
-  }
+  const uint32_t lim = min(total, kChunk);
   uint32_t k0 = (uint32_t)__ldcg(&p.sw[x]);
   bool resolved = false;
-  while (k0 < total && !resolved) {
-    const uint32_t k = k0 + lane;
-    bool ok = false;
-    uint32_t y = 0;
-    if (k < total) {
-      bool valid = true;
-      if (k < nb) {
-        y = a.col[b + k];
-        valid = !(y & kTomb);
-        y &= kIdMask;
-      } else {
-        y = a.darena[dr.x + (k - nb)];
-      }
-      ok = valid && y < p.dist_len && p.dist[y] + 1 == d && !test_bit_cg(p.aff, y);
-    }
-    const uint32_t ball = __ballot_sync(FULL, ok);
-    if (!ball) {
-      k0 += 32;
-      continue;
-    }
-    const int f = __ffs(ball) - 1;
-    const uint32_t yw = __shfl_sync(FULL, y, f);
-    const uint32_t kw = k0 + (uint32_t)f;
+  uint32_t kw = 0, yw = 0;
+  while (k0 < lim && !resolved) {
+    if (!find_parent(p, a, b, nb, dr.x, k0, lim, d, kw, yw)) break;
     bool still = false;
     if (lane == 0) {
       __stcg(&p.sw[x], kSwTouched | ((unsigned long long)(yw + 1) << 32) | kw);
@@ -822,21 +833,39 @@ __device__ void check_vertex(const Params& p, uint32_t x) {
     resolved = __shfl_sync(FULL, still, 0);
     k0 = kw + 1;  // the witness turned affected meanwhile: scan on past it
   }
-  if (!resolved) {
-    bool push = false;
+  if (resolved) return;
+  if (total > kChunk) {
+    // the rest of a long in-row: one chunk-check item per kChunk arcs past the
+    // first, scanned by many warps; tent[x] counts the chunks of the pass in
+    // flight.  A request that finds a pass in flight is covered by it: the
+    // pass clears tent[x] before it verifies its final witness.
+    const uint32_t K = (total + kChunk - 1) / kChunk - 1;
+    bool start = false;
     if (lane == 0) {
-      __stcg(&p.sw[x], kSwTouched | (unsigned long long)total);
-      push = mark_affected(p, x);
+      __stcg(&p.sw[x], kSwTouched | (unsigned long long)kChunk);
+      start = atomicCAS(&p.tent[x], 0u, K) == 0u;
     }
-    ring_push(p, push, (unsigned long long)(x | kKindBit));
+    start = __shfl_sync(FULL, start, 0);
+    if (start)
+      for (uint32_t c0 = 0; c0 < K; c0 += 32)
+        ring_push(p, c0 + lane < K, kChunkCheckBit | ((unsigned long long)(c0 + lane + 1) << 32) | x);
+    return;
   }
+  bool push = false;
+  if (lane == 0) {
+    __stcg(&p.sw[x], kSwTouched | (unsigned long long)total);
+    push = mark_affected(p, x);
+  }
+  ring_push(p, push, (unsigned long long)(x | kKindBit));
 }
 
-// One chunk of a long check (whole warp): scan [c * kChunk, (c + 1) * kChunk)
-// of x's in-row for a surviving, non-affected parent, unless another chunk
-// found one already (kFoundBit in tent[x]).  The last chunk of the pass clears
-// tent[x], then either verifies the recorded witness (asking for a new check
-// if it turned affected) or, when no chunk found one, marks x affected.
+// One chunk c >= 1 of a long check (whole warp): scan [c * kChunk,
+// (c + 1) * kChunk) of x's in-row for a surviving, non-affected parent, unless
+// another chunk found one already (kFoundBit in tent[x]).  The last chunk of
+// the pass clears tent[x], then either verifies the recorded witness (asking
+// for a new check if it turned affected) or, when no chunk found one, marks x
+// affected.  Witnesses are recorded with the saved position kChunk (the first
+// chunk is known to hold none).
 constexpr uint32_t kFoundBit = 0x80000000u;
 
 __device__ void chunk_check(const Params& p, uint32_t x, uint32_t c) {
@@ -847,41 +876,21 @@ __device__ void chunk_check(const Params& p, uint32_t x, uint32_t c) {
   vxb::base_range(a, x, b, e);
   const uint2 dr = a.drow[x];
   const uint32_t nb = (uint32_t)(e - b), total = nb + dr.y;
-  const uint32_t lo = c * kChunk, hi = min(total, lo + kChunk);
-  uint32_t k0 = lo;
+  const uint32_t hi = min(total, (c + 1) * kChunk);
+  uint32_t k0 = c * kChunk;
   bool found = (ld_cg(&p.tent[x]) & kFoundBit) != 0u;
+  uint32_t kw = 0, yw = 0;
   while (k0 < hi && !found) {
-    const uint32_t k = k0 + lane;
-    bool ok = false;
-    uint32_t y = 0;
-    if (k < hi) {
-      bool valid = true;
-      if (k < nb) {
-        y = a.col[b + k];
-        valid = !(y & kTomb);
-        y &= kIdMask;
-      } else {
-        y = a.darena[dr.x + (k - nb)];
-      }
-      ok = valid && y < p.dist_len && p.dist[y] + 1 == d && !test_bit_cg(p.aff, y);
-    }
-    const uint32_t ball = __ballot_sync(FULL, ok);
-    if (!ball) {
-      k0 += 32;
-      if (((k0 - lo) & 127) == 0) found = (ld_cg(&p.tent[x]) & kFoundBit) != 0u;  // one load per warp
-      continue;
-    }
-    const int f = __ffs(ball) - 1;
-    const uint32_t yw = __shfl_sync(FULL, y, f);
+    if (!find_parent(p, a, b, nb, dr.x, k0, hi, d, kw, yw)) break;
     bool good = false;
     if (lane == 0) {
-      __stcg(&p.sw[x], kSwTouched | ((unsigned long long)(yw + 1) << 32));
+      __stcg(&p.sw[x], kSwTouched | ((unsigned long long)(yw + 1) << 32) | kChunk);
       __threadfence();
       good = !test_bit_cg(p.aff, yw);
       if (good) atomicOr(&p.tent[x], kFoundBit);
     }
     found = __shfl_sync(FULL, good, 0);
-    k0 += (uint32_t)f + 1;
+    k0 = kw + 1;
   }
   bool recheck = false, aff = false;
   if (lane == 0) {
