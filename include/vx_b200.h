@@ -10,7 +10,9 @@
  *   - Every function returns an int status: VX_OK (0) or a negative VX_ERR_*.
  *     vx_last_error() returns the message of the calling thread's last error.
  *   - Host-pointer variants copy their inputs; *_device variants take device
- *     pointers on the current CUDA device and enqueue on the graph's stream.
+ *     pointers on the current CUDA device and enqueue on the graph's stream,
+ *     which reads the arrays in place: they must stay unchanged until that
+ *     stream has run the call's work.
  *   - Objects are single-threaded, like the reference classes
  *     (include/velographx/storage/dynamic_graph.hpp, incremental/bfs.hpp).
  *   - Vertex ids are uint32 and must be below 2^31 (bit 31 marks deleted base

@@ -1470,8 +1470,10 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
       tmark = now;
     }
   };
-  if (gtid() == 0)
+  if (gtid() == 0) {  // stamps and drain statistics are written by this thread only
     for (int k = 0; k < 6; ++k) c->stream_ns[k] = 0;
+    for (int k = 0; k < (int)(sizeof(c->rtrace) / sizeof(c->rtrace[0])); ++k) c->rtrace[k] = 0;
+  }
   for (uint32_t bi = 0; bi < s.nb; ++bi) {
     const uint32_t off = s.boff ? s.boff[bi] : 0u, F = s.bcnt[bi];
     const uint32_t Vpre = bi ? s.vpost[bi - 1] : s.V0, lpre = bi ? s.vpost[bi - 1] : s.len0;
@@ -1853,14 +1855,16 @@ int bfs_recompute(Bfs* b) {
 int bfs_stage(Bfs* b, size_t n, size_t vertex_bound, bool classify) {
   Graph* g = b->g;
   cudaStream_t s = g->stream;
-  // last_* counters reset on every apply (bfs.hpp:30-33)
-  VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->candidates, 0, 4 * sizeof(uint32_t), s));
   b->staged_ops = n;
   b->staged_V_pre = g->V;
   b->staged_len_pre = b->dist_len;
-  if (n == 0) return 0;
-  VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->cand_n, 0, 3 * sizeof(uint32_t), s));
-  VX_CUDA_TRY(cudaMemsetAsync(b->ctr->rtrace, 0, sizeof(b->ctr->rtrace), s));
+  if (n == 0) {  // last_* counters reset on every apply (bfs.hpp:30-33)
+    VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->candidates, 0, 4 * sizeof(uint32_t), s));
+    return 0;
+  }
+  // a non-empty batch resets them (and the repair lists) in whichever path
+  // consumes it: the fused launch in its first phase, the per-phase and full
+  // paths on the host before their kernels
   b->staged_classified = classify;
   if (int rc = graph_stage_batch(g, n, vertex_bound, classify)) return rc;
   if (int rc = ensure_capacity(b, std::max<size_t>(g->V, 1))) return rc;
@@ -1921,6 +1925,9 @@ int bfs_repair_staged(Bfs* b) {
   cudaStream_t s = g->stream;
   if (b->staged_ops == 0) return 0;
   if (!g->directed && b->tune.fused) return repair_fused(b);
+  VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->candidates, 0, 4 * sizeof(uint32_t), s));
+  VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->cand_n, 0, 3 * sizeof(uint32_t), s));
+  VX_CUDA_TRY(cudaMemsetAsync(b->ctr->rtrace, 0, sizeof(b->ctr->rtrace), s));
   const size_t V_pre = b->staged_V_pre, len_pre = b->staged_len_pre;
   const size_t V_post = g->V;
   // fallback limit: max(1, size_t(double(V) * fraction))  (bfs.hpp:225-226)
@@ -1951,6 +1958,7 @@ int bfs_full_staged(Bfs* b) {
   if (b->staged_ops == 0) return 0;
   if (int rc = graph_commit_batch(b->g)) return rc;
   b->staged_ops = 0;
+  VX_CUDA_TRY(cudaMemsetAsync(b->ctr->rtrace, 0, sizeof(b->ctr->rtrace), b->g->stream));
   return bfs_recompute(b);
 }
 

@@ -290,7 +290,7 @@ static int launch_canon(Graph* g, size_t n, size_t m, int b, int sh, uint32_t bo
   const int passes = (2 * b + 7) / 8;
   BatchBuffers& B = g->batch;
   count_launch();
-  VX_CUDA_TRY(cudaLaunchKernelEx(&cfg, canon_cluster_kernel<ITEMS>, B.src, B.dst, B.add, (uint32_t)n,
+  VX_CUDA_TRY(cudaLaunchKernelEx(&cfg, canon_cluster_kernel<ITEMS>, B.in_src, B.in_dst, B.in_add, (uint32_t)n,
                                  (int)g->directed, b, sh, bound, passes, B.fu, B.fv, B.ff, g->ctr));
   *launched = true;
   return 0;

@@ -67,16 +67,19 @@ int upload_batch(vxh::Graph* g, const uint32_t* src, const uint32_t* dst, const 
   VX_CUDA_TRY(cudaMemcpyAsync(g->batch.src, src, n * 4, cudaMemcpyHostToDevice, s));
   VX_CUDA_TRY(cudaMemcpyAsync(g->batch.dst, dst, n * 4, cudaMemcpyHostToDevice, s));
   VX_CUDA_TRY(cudaMemcpyAsync(g->batch.add, add, n, cudaMemcpyHostToDevice, s));
+  g->batch.in_src = g->batch.src;
+  g->batch.in_dst = g->batch.dst;
+  g->batch.in_add = g->batch.add;
   *v_after = vmax;
   return 0;
 }
 
+// A device batch is read in place by the staging kernels (stream-ordered).
 int stage_device_batch(vxh::Graph* g, const uint32_t* d_src, const uint32_t* d_dst, const uint8_t* d_add, size_t n) {
   if (int rc = g->batch.ensure(n)) return rc;
-  cudaStream_t s = g->stream;
-  VX_CUDA_TRY(cudaMemcpyAsync(g->batch.src, d_src, n * 4, cudaMemcpyDeviceToDevice, s));
-  VX_CUDA_TRY(cudaMemcpyAsync(g->batch.dst, d_dst, n * 4, cudaMemcpyDeviceToDevice, s));
-  VX_CUDA_TRY(cudaMemcpyAsync(g->batch.add, d_add, n, cudaMemcpyDeviceToDevice, s));
+  g->batch.in_src = d_src;
+  g->batch.in_dst = d_dst;
+  g->batch.in_add = d_add;
   return 0;
 }
 

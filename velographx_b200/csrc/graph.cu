@@ -834,9 +834,11 @@ int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound, bool classify) {
       if (int rc = reserve_arena(g, g->adj[d], m, &consolidate)) return rc;
   }
   if (int rc = graph_grow(g, std::max<size_t>(g->V, vertex_bound))) return rc;
-  VX_CUDA_TRY(cudaMemsetAsync(&g->ctr->final_arcs, 0, 5 * sizeof(uint32_t), s));
   const int b = bits_for(std::max<size_t>(g->V, 2));
-  if (n == 0) return 0;
+  if (n == 0) {  // a non-empty batch's staging sets these counts itself
+    VX_CUDA_TRY(cudaMemsetAsync(&g->ctr->final_arcs, 0, 5 * sizeof(uint32_t), s));
+    return 0;
+  }
   bool done = false;
   if (int rc = canon_cluster(g, n, b, (uint32_t)g->V, &done)) return rc;
   if (done) {
@@ -848,7 +850,7 @@ int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound, bool classify) {
     return 0;
   }
   vxh::count_launch();
-  expand_ops_kernel<<<grid_for(n), kBlock, 0, s>>>(B.src, B.dst, B.add, n, g->directed, b, (uint32_t)g->V,
+  expand_ops_kernel<<<grid_for(n), kBlock, 0, s>>>(B.in_src, B.in_dst, B.in_add, n, g->directed, b, (uint32_t)g->V,
                                                     B.keys, B.vals, g->ctr);
   VX_CUDA_TRY(cudaGetLastError());
   bool in_alt = false;

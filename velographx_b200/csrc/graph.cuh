@@ -53,6 +53,11 @@ struct BatchBuffers {
   uint32_t* src = nullptr;
   uint32_t* dst = nullptr;
   uint8_t* add = nullptr;
+  // the op arrays the next staging reads: src/dst/add after a host upload, or
+  // the caller's own device arrays (read in place)
+  const uint32_t* in_src = nullptr;
+  const uint32_t* in_dst = nullptr;
+  const uint8_t* in_add = nullptr;
   uint64_t* keys = nullptr;
   uint64_t* keys_alt = nullptr;
   uint32_t* vals = nullptr;

@@ -39,12 +39,55 @@ __device__ __forceinline__ uint32_t merged_at(uint32_t k, const uint32_t* A, uin
   return (j >= nB || (i < nA && A[i] < B[j])) ? A[i] : B[j];
 }
 
+// Merges of a short list (nB <= 32, the usual run of one row in a batch):
+// lane j holds B[j] and its final index slot_j = lower_bound(A, B[j]) + j,
+// found once by parallel binary searches.  Output k is then B[j] where
+// k == slot_j, else A[k - t] with t the number of slots below k (a register
+// scan over the lanes), so each 32 outputs cost one load instead of a
+// co-rank search each.
+__device__ __forceinline__ uint32_t short_merge_slot(const uint32_t* A, uint32_t nA, uint32_t nB, uint32_t bv) {
+  const uint32_t lane = threadIdx.x & 31;
+  return lane < nB ? vxb::lower_bound_u32(A, 0, nA, bv) + lane : 0xFFFFFFFFu;
+}
+
+// Whole warp: whether output k is one of B (then *bval) and, if not, the
+// number of B slots below k.
+__device__ __forceinline__ bool short_merge_pick(uint32_t k, uint32_t slot, uint32_t bv, uint32_t nB, uint32_t& t,
+                                                 uint32_t& bval) {
+  bool hit = false;
+  t = 0;
+  for (uint32_t j = 0; j < nB; ++j) {
+    const uint32_t sj = __shfl_sync(0xFFFFFFFFu, slot, j);
+    const uint32_t bj = __shfl_sync(0xFFFFFFFFu, bv, j);
+    t += sj < k;
+    if (sj == k) {
+      hit = true;
+      bval = bj;
+    }
+  }
+  return hit;
+}
+
 // Warp-cooperative merge of sorted B[0..nB) into sorted A[0..nA) where A has
 // room for nA + nB entries.  Output chunks are produced from the back; every
 // output k only reads A at positions <= k, so no unread input is overwritten.
 __device__ inline void warp_merge_inplace(uint32_t* A, uint32_t nA, const uint32_t* B, uint32_t nB) {
   const int lane = threadIdx.x & 31;
   const uint32_t total = nA + nB;
+  if (nB <= 32) {
+    const uint32_t bv = (uint32_t)lane < nB ? B[lane] : 0u;
+    const uint32_t slot = short_merge_slot(A, nA, nB, bv);
+    for (int64_t top = total; top > 0; top -= 32) {
+      const int64_t k = top - 32 + lane;
+      uint32_t t = 0, val = 0;
+      const bool hit = short_merge_pick(k < 0 ? 0xFFFFFFFFu : (uint32_t)k, slot, bv, nB, t, val);
+      if (k >= 0 && !hit) val = A[k - t];
+      __syncwarp();
+      if (k >= 0) A[k] = val;
+      __syncwarp();
+    }
+    return;
+  }
   for (int64_t top = total; top > 0; top -= 32) {
     const int64_t k = top - 32 + lane;
     uint32_t val = 0;
@@ -57,6 +100,17 @@ __device__ inline void warp_merge_inplace(uint32_t* A, uint32_t nA, const uint32
 
 __device__ inline void warp_merge_to(uint32_t* out, const uint32_t* A, uint32_t nA, const uint32_t* B, uint32_t nB) {
   const int lane = threadIdx.x & 31;
+  if (nB <= 32) {
+    const uint32_t bv = (uint32_t)lane < nB ? B[lane] : 0u;
+    const uint32_t slot = short_merge_slot(A, nA, nB, bv);
+    for (uint32_t k0 = 0; k0 < nA + nB; k0 += 32) {
+      const uint32_t k = k0 + lane;
+      uint32_t t = 0, val = 0;
+      const bool hit = short_merge_pick(k, slot, bv, nB, t, val);
+      if (k < nA + nB) out[k] = hit ? val : A[k - t];
+    }
+    return;
+  }
   for (uint32_t k = lane; k < nA + nB; k += 32) out[k] = merged_at(k, A, nA, B, nB);
 }
 
