@@ -287,16 +287,34 @@ __device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, u
   const DevAdj& a = p.g.in;
   const int lane = threadIdx.x & 31;
   const uint32_t words = (p.V + 31) >> 5;
-  for (uint32_t w = gwarp(); w < words; w += nwarps()) {
-    const uint32_t visw = p.vis[w];
-    if (visw == FULL) continue;
+  // software pipeline over the warp's words: the next word's visited bits
+  // and row bounds are loaded while the current word is scanned
+  uint32_t w = gwarp();
+  uint32_t nvis = 0;
+  uint64_t nbv = 0, nev = 0;
+  uint2 ndr = make_uint2(0, 0);
+  auto fetch = [&](uint32_t ww) {
+    const uint32_t vv = ww * 32 + lane;
+    nvis = ww < words ? p.vis[ww] : FULL;
+    nbv = nev = 0;
+    ndr = make_uint2(0, 0);
+    if (ww < words && vv < p.V) {
+      vxb::base_range(a, vv, nbv, nev);
+      ndr = a.drow[vv];
+    }
+  };
+  fetch(w);
+  for (; w < words; w += nwarps()) {
     const uint32_t v = w * 32 + lane;
+    const uint32_t visw = nvis;
+    uint64_t b = nbv, e = nev;
+    uint2 dr = ndr;
+    fetch(w + nwarps());
+    if (visw == FULL) continue;
     const bool todo = !((visw >> lane) & 1u);
-    uint64_t b = 0, e = 0;
-    uint2 dr = make_uint2(0, 0);
-    if (todo) {
-      vxb::base_range(a, v, b, e);
-      dr = a.drow[v];
+    if (!todo) {
+      b = e = 0;
+      dr = make_uint2(0, 0);
     }
     const uint32_t nb = (uint32_t)(e - b), total = nb + dr.y;
     bool found = false;

@@ -149,12 +149,13 @@ def grid(side: int = 4096, long_range: float = 0.001, batches: int = 500, ops: i
     return res
 
 
-def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int = 14) -> dict:
+def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int = 14, repeats: int = 3) -> dict:
     """Undirected R-MAT scale 14, full BFS from the max-degree vertex, then 100
     batches of 64 uniform-random insertions: the plain path (one batch per
     call, counters read back) and the batched path, with the distance digest
-    after every batch; returns the stream (for a check elsewhere) with the
-    timings."""
+    after every batch, each on fresh replicas `repeats` times (the median is
+    reported: a 100-batch run lasts only milliseconds); returns the stream
+    (for a check elsewhere) with the timings."""
     import torch
 
     V = 1 << scale
@@ -169,35 +170,41 @@ def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int 
     out = {"workload": f"rmat{scale}-undirected-ef16-{batches}x{ops}-insertions", "vertices": V, "root": int(root),
            "batches": batches}
     e0, e1 = _events()
-    g = Graph(V, False)
-    g.bulk_load_edges(edges)
-    g.reserve(ops, ops * batches)
-    b = IncrementalBFS(g, root)
-    cs = torch.cuda.ExternalStream(g.stream)
-    torch.cuda.synchronize()
-    e0.record(cs)
-    plain_digests = []
-    for t in range(batches):
-        b.apply_arrays(*st.batch(t))
-        b.stats()
-        plain_digests.append(b.digest())
-    e1.record(cs)
-    torch.cuda.synchronize()
-    out["plain"] = {"batches_per_s": batches / (e0.elapsed_time(e1) * 1e-3)}
-    g2 = Graph(V, False)
-    g2.bulk_load_edges(edges)
-    g2.reserve(ops, ops * batches)
-    b2 = IncrementalBFS(g2, root)
-    b2.reserve_stream(batches * ops, batches, ops)
-    cs2 = torch.cuda.ExternalStream(g2.stream)
-    torch.cuda.synchronize()
-    e0.record(cs2)
-    digs, _ = b2.apply_stream(st.src, st.dst, st.add, off, digests=True)
-    e1.record(cs2)
-    torch.cuda.synchronize()
-    out["batched"] = {"batches_per_s": batches / (e0.elapsed_time(e1) * 1e-3)}
+    plain_runs, batched_runs, same = [], [], True
+    for _ in range(repeats):
+        g = Graph(V, False)
+        g.bulk_load_edges(edges)
+        g.reserve(ops, ops * batches)
+        b = IncrementalBFS(g, root)
+        cs = torch.cuda.ExternalStream(g.stream)
+        torch.cuda.synchronize()
+        e0.record(cs)
+        plain_digests = []
+        for t in range(batches):
+            b.apply_arrays(*st.batch(t))
+            b.stats()
+            plain_digests.append(b.digest())
+        e1.record(cs)
+        torch.cuda.synchronize()
+        plain_runs.append(batches / (e0.elapsed_time(e1) * 1e-3))
+        g2 = Graph(V, False)
+        g2.bulk_load_edges(edges)
+        g2.reserve(ops, ops * batches)
+        b2 = IncrementalBFS(g2, root)
+        b2.reserve_stream(batches * ops, batches, ops)
+        cs2 = torch.cuda.ExternalStream(g2.stream)
+        torch.cuda.synchronize()
+        e0.record(cs2)
+        digs, _ = b2.apply_stream(st.src, st.dst, st.add, off, digests=True)
+        e1.record(cs2)
+        torch.cuda.synchronize()
+        batched_runs.append(batches / (e0.elapsed_time(e1) * 1e-3))
+        same = same and [int(x) for x in digs] == [int(x) for x in plain_digests]
+        del b, g, b2, g2
+    out["plain"] = {"batches_per_s": float(np.median(plain_runs)), "runs": [round(x) for x in plain_runs]}
+    out["batched"] = {"batches_per_s": float(np.median(batched_runs)), "runs": [round(x) for x in batched_runs]}
     out["digests"] = [int(x) for x in digs]
-    out["plain_equals_batched"] = out["digests"] == [int(x) for x in plain_digests]
+    out["plain_equals_batched"] = bool(same)
     out["_stream"] = (edges, st, root)
     return out
 
