@@ -1382,7 +1382,7 @@ __device__ __forceinline__ bool delta_op(uint8_t f, bool insertion) {
 // Delta removals of one row run (whole warp): the row's sorted delta list
 // keeps every entry that is not a removal of the run (delta_remove_kernel of
 // the per-batch path, on the canonical arcs directly).
-__device__ void run_remove(vxb::DevAdj& a, const uint32_t* fv, const uint8_t* ff, uint32_t s, uint32_t e, uint32_t u,
+__device__ void run_remove(const vxb::DevAdj& a, const uint32_t* fv, const uint8_t* ff, uint32_t s, uint32_t e, uint32_t u,
                            GraphCounters* gc) {
   const int lane = threadIdx.x & 31;
   bool any = false;
@@ -1418,7 +1418,7 @@ __device__ void run_remove(vxb::DevAdj& a, const uint32_t* fv, const uint8_t* ff
 // compacted into scratch[s, s + nB) and merged into the row's delta list, in
 // place when its block has room, else into a new power-of-two arena block
 // (delta_insert_kernel of the per-batch path).
-__device__ void run_insert(vxb::DevAdj& a, const uint32_t* fv, const uint8_t* ff, uint32_t* scratch, uint32_t s,
+__device__ void run_insert(const vxb::DevAdj& a, const uint32_t* fv, const uint8_t* ff, uint32_t* scratch, uint32_t s,
                            uint32_t e, uint32_t u, GraphCounters* gc, unsigned long long arena_cap) {
   const int lane = threadIdx.x & 31;
   uint32_t nB = 0;
@@ -1459,21 +1459,105 @@ __device__ void run_insert(vxb::DevAdj& a, const uint32_t* fv, const uint8_t* ff
   }
 }
 
-// Every row run of the batch's canonical arcs [0, F): warp w takes arc
-// indices w, w + nwarps, ... and processes the run that starts at each (a
-// run start is an arc whose row differs from its predecessor's), so the runs
-// of a batch spread over all warps.
+// The row runs of the batch's canonical arcs [0, F): delta removals
+// (kInsert false) or insertions (true).  A run of one arc whose delta row
+// holds at most 7 arcs (8 for a removal) -- most runs of a batch -- is done by
+// one lane: the row's block (capacity >= 8, 8-aligned in the arena) is loaded
+// as two 16-byte words, edited in registers and stored back; a row without a
+// block gets 8 slots from one warp-aggregated arena allocation.  The other
+// runs are queued in shared memory and done by the block's warps (run_insert,
+// run_remove).  Arcs are dealt round-robin (arc i to block i mod gridDim), so
+// a small batch still spreads over every block.  Block-uniform.
 template <bool kInsert>
-__device__ void for_each_run(const Params& p, const StreamArgs& s, uint32_t off, uint32_t F) {
-  vxb::DevAdj a = p.g.out;
+__device__ void commit_runs(const Params& p, const StreamArgs& s, uint32_t off, uint32_t F, RepairSmem& sm) {
+  const vxb::DevAdj& a = p.g.out;
   const uint32_t* fu = s.fu + off;
   const uint32_t* fv = s.fv + off;
   const uint8_t* ff = s.ff + off;
-  for (uint32_t i = gwarp(); i < F; i += nwarps()) {
-    if (i > 0 && fu[i] == fu[i - 1]) continue;  // same load on every lane: warp-uniform
-    const uint32_t en = run_end(fu, i, F);
-    if (kInsert) run_insert(a, fv, ff, s.scratch, i, en, fu[i], s.gc, s.arena_cap);
-    else run_remove(a, fv, ff, i, en, fu[i], s.gc);
+  const int lane = threadIdx.x & 31;
+  const uint32_t per_round = gridDim.x * kThreads;
+  for (uint32_t r0 = 0; r0 < F; r0 += per_round) {
+    if (threadIdx.x == 0) sm.nsv = 0;
+    __syncthreads();
+    const uint32_t i = r0 + threadIdx.x * gridDim.x + blockIdx.x;
+    bool job = false, queue = false, need_block = false;
+    uint32_t u = 0, v = 0;
+    uint2 row = make_uint2(0, 0);
+    if (i < F) {
+      u = fu[i];
+      if (i == 0 || fu[i - 1] != u) {
+        if (i + 1 < F && fu[i + 1] == u) {
+          queue = true;  // a run of several arcs
+        } else if (delta_op(ff[i], kInsert)) {
+          v = fv[i];
+          row = a.drow[u];
+          if (kInsert ? row.y < 8u : row.y <= 8u) {
+            job = true;
+            need_block = kInsert && a.dcap[u] == 0u;  // no block yet (then the row is empty)
+          } else {
+            queue = true;
+          }
+        }
+      }
+    }
+    const uint32_t nm = __ballot_sync(FULL, need_block);
+    uint32_t base_off = row.x;
+    if (nm) {
+      const int leader = __ffs(nm) - 1;
+      unsigned long long b0 = 0;
+      if (lane == leader) b0 = atomicAdd(&s.gc->arena_top[0], 8ull * (unsigned long long)__popc(nm));
+      b0 = __shfl_sync(FULL, b0, leader);
+      const unsigned long long o = b0 + 8ull * __popc(nm & vxb::lanemask_lt());
+      if (need_block) {
+        if (o + 8 > s.arena_cap) {
+          atomicOr(&s.gc->err, vxb::kErrArenaOverflow);
+          job = false;
+        } else {
+          base_off = (uint32_t)o;
+        }
+      }
+    }
+    long long dlive = 0;
+    unsigned long long dirtied = 0;
+    if (job) {
+      uint32_t x[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (row.y) {
+        const uint4* src = reinterpret_cast<const uint4*>(a.darena + row.x);
+        const uint4 q0 = src[0], q1 = src[1];
+        x[0] = q0.x, x[1] = q0.y, x[2] = q0.z, x[3] = q0.w;
+        x[4] = q1.x, x[5] = q1.y, x[6] = q1.z, x[7] = q1.w;
+      }
+      // output k: an insertion takes x[k] below the new arc's position, the arc
+      // at it and x[k - 1] above; a removal takes x[k] below the arc, x[k + 1] from it on
+      uint32_t pos = 0;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) pos += ((uint32_t)k < row.y && x[k] < v) ? 1u : 0u;
+      auto out = [&](int k) -> uint32_t {
+        if (kInsert) return (uint32_t)k < pos ? x[k] : ((uint32_t)k == pos ? v : x[k > 0 ? k - 1 : 0]);
+        return (uint32_t)k < pos ? x[k] : x[k < 7 ? k + 1 : 7];
+      };
+      uint4* dst = reinterpret_cast<uint4*>(a.darena + base_off);
+      dst[0] = make_uint4(out(0), out(1), out(2), out(3));
+      dst[1] = make_uint4(out(4), out(5), out(6), out(7));
+      dlive = kInsert ? 1 : -1;
+      a.drow[u] = make_uint2(base_off, kInsert ? row.y + 1 : row.y - 1);
+      if (need_block) a.dcap[u] = 8u;
+      const uint32_t bit = 1u << (u & 31);
+      dirtied = (atomicOr(&a.dirty[u >> 5], bit) & bit) ? 0ull : 1ull;
+    }
+    dlive = vxb::warp_sum(dlive);
+    dirtied = vxb::warp_sum(dirtied);
+    if (lane == 0 && dlive) atomicAdd(&s.gc->delta_live[0], (unsigned long long)dlive);
+    if (lane == 0 && dirtied) atomicAdd(&s.gc->dirty_rows[0], dirtied);
+    if (queue) sm.sv[atomicAdd(&sm.nsv, 1u)] = i;
+    __syncthreads();
+    const uint32_t nq = sm.nsv;
+    for (uint32_t k = threadIdx.x >> 5; k < nq; k += kThreads / 32) {
+      const uint32_t st = sm.sv[k], en = run_end(fu, st, F);
+      if (kInsert) run_insert(a, fv, ff, s.scratch, st, en, fu[st], s.gc, s.arena_cap);
+      else run_remove(a, fv, ff, st, en, fu[st], s.gc);
+    }
+    __syncthreads();  // the list is rebuilt by the next round
   }
 }
 
@@ -1529,7 +1613,7 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
     if (!sync_grid(p)) return;
     phase(0);
     // B: delta removals; deletion candidates registered
-    for_each_run<false>(q, s, off, F);
+    commit_runs<false>(q, s, off, F, sm);
     register_candidates(q);
     if (!sync_grid(p)) return;
     phase(1);
@@ -1554,7 +1638,7 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
       if (lane == 0 && tombs) atomicAdd(&s.gc->tombs[0], (unsigned long long)tombs);
       for (uint32_t v = lpre + gtid(); v < Vpost; v += nthreads()) p.dist[v] = kUnreachable;
     }
-    for_each_run<true>(q, s, off, F);
+    commit_runs<true>(q, s, off, F, sm);
     if (!sync_grid(p)) return;
     phase(3);
     // E: the post-batch repair (or the fallback full BFS) on the new graph
