@@ -1596,18 +1596,23 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
     stamp(q, 0);
     // A: classification against the pre-batch graph; tombstone the deleted base arcs
     {
-      vxb::DevAdj a = p.g.out;
+      // arcs dealt round-robin over the blocks (arc i to block i mod gridDim),
+      // so a small batch's searches spread over every SM
+      const vxb::DevAdj& a = p.g.out;
       long long tombs = 0;
-      for (uint32_t i = gtid(); i < F; i += nthreads()) {
+      uint32_t dirtied = 0;
+      for (uint32_t i = threadIdx.x * gridDim.x + blockIdx.x; i < F; i += nthreads()) {
         uint8_t f = s.ff[off + i];
         if (!s.classified) {
           f = gdev::classify_arc(a, s.fu[off + i], s.fv[off + i], f, s.fpos[off + i]);
           s.ff[off + i] = f;
         }
-        tombs += gdev::tomb_arc(a, s.fu[off + i], f, s.fpos[off + i], 0, &s.gc->dirty_rows[0]);
+        tombs += gdev::tomb_arc(a, s.fu[off + i], f, s.fpos[off + i], 0, dirtied);
       }
       tombs = vxb::warp_sum(tombs);
+      dirtied = vxb::warp_sum(dirtied);
       if (lane == 0 && tombs) atomicAdd(&s.gc->tombs[0], (unsigned long long)tombs);
+      if (lane == 0 && dirtied) atomicAdd(&s.gc->dirty_rows[0], (unsigned long long)dirtied);
       if (s.digest && bi > 0) digest_pass(p.dist, lpre, &s.digest[bi - 1]);
     }
     if (!sync_grid(p)) return;
@@ -1630,12 +1635,15 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
     stamp(q, 2);
     // D: revive re-added base arcs, delta insertions; new vertices start unreachable
     {
-      vxb::DevAdj a = p.g.out;
+      const vxb::DevAdj& a = p.g.out;
       long long tombs = 0;
-      for (uint32_t i = gtid(); i < F; i += nthreads())
-        tombs += gdev::tomb_arc(a, s.fu[off + i], s.ff[off + i], s.fpos[off + i], 1, &s.gc->dirty_rows[0]);
+      uint32_t dirtied = 0;
+      for (uint32_t i = threadIdx.x * gridDim.x + blockIdx.x; i < F; i += nthreads())
+        tombs += gdev::tomb_arc(a, s.fu[off + i], s.ff[off + i], s.fpos[off + i], 1, dirtied);
       tombs = vxb::warp_sum(tombs);
+      dirtied = vxb::warp_sum(dirtied);
       if (lane == 0 && tombs) atomicAdd(&s.gc->tombs[0], (unsigned long long)tombs);
+      if (lane == 0 && dirtied) atomicAdd(&s.gc->dirty_rows[0], (unsigned long long)dirtied);
       for (uint32_t v = lpre + gtid(); v < Vpost; v += nthreads()) p.dist[v] = kUnreachable;
     }
     commit_runs<true>(q, s, off, F, sm);

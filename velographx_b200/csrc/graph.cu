@@ -192,10 +192,13 @@ __global__ void tomb_kernel(DevAdj a, const uint32_t* fu, const uint8_t* ff, con
                             unsigned long long* dirty_rows) {
   const uint32_t F = *count;
   long long delta = 0;
+  uint32_t dirtied = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < F; i += gridDim.x * blockDim.x)
-    delta += gdev::tomb_arc(a, fu[i], ff[i], fpos[i], mode, dirty_rows);
+    delta += gdev::tomb_arc(a, fu[i], ff[i], fpos[i], mode, dirtied);
   delta = vxb::warp_sum(delta);
+  dirtied = vxb::warp_sum(dirtied);
   if ((threadIdx.x & 31) == 0 && delta) atomicAdd(tombs, (unsigned long long)delta);
+  if ((threadIdx.x & 31) == 0 && dirtied) atomicAdd(dirty_rows, (unsigned long long)dirtied);
 }
 
 // mode 0: delta removals (state present -> absent, arc not in base)

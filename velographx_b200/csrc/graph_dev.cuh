@@ -120,6 +120,13 @@ __device__ __forceinline__ void mark_dirty(uint32_t* dirty, uint32_t u, unsigned
   if (!(old & bit)) atomicAdd(counter, 1ull);
 }
 
+// Marks row u dirty; 1 when this call dirtied it (for a caller that counts
+// newly dirtied rows itself, once per warp).
+__device__ __forceinline__ uint32_t mark_dirty_count(uint32_t* dirty, uint32_t u) {
+  const uint32_t bit = 1u << (u & 31);
+  return (atomicOr(&dirty[u >> 5], bit) & bit) ? 0u : 1u;
+}
+
 // Pre-batch state of canonical arc (u, v) whose desired state is bit 0 of
 // `add`: in the base CSR (position in fpos, live unless tombstoned) or in the
 // row's sorted delta list; flags kFInBase / kFCur / kFChanged.
@@ -145,9 +152,10 @@ __device__ __forceinline__ uint8_t classify_arc(const DevAdj& a, uint32_t u, uin
 }
 
 // mode 0 tombstones a base arc the batch deletes, mode 1 revives one it
-// re-adds; returns the change of the tombstone count.
-__device__ __forceinline__ long long tomb_arc(DevAdj& a, uint32_t u, uint8_t f, uint64_t p, int mode,
-                                              unsigned long long* dirty_rows) {
+// re-adds; returns the change of the tombstone count and adds the row to
+// `dirtied` when this call dirtied it (callers sum both per warp).
+__device__ __forceinline__ long long tomb_arc(const DevAdj& a, uint32_t u, uint8_t f, uint64_t p, int mode,
+                                              uint32_t& dirtied) {
   if (!(f & kFInBase) || !(f & kFChanged)) return 0;
   if (((f & kFAdd) != 0) != (mode == 1)) return 0;
   long long delta;
@@ -160,7 +168,7 @@ __device__ __forceinline__ long long tomb_arc(DevAdj& a, uint32_t u, uint8_t f, 
     atomicAdd(&a.tcnt[u], 1u);
     delta = 1;
   }
-  mark_dirty(a.dirty, u, dirty_rows);
+  dirtied += mark_dirty_count(a.dirty, u);
   return delta;
 }
 
