@@ -766,18 +766,28 @@ __device__ __forceinline__ bool mark_affected(const Params& p, uint32_t v) {
 }
 
 // Warp-uniform: request a check of x where pred holds (first touch is recorded
-// in sw and in the touched list; a pending request is not repeated).
-__device__ __forceinline__ void request_check(const Params& p, bool pred, uint32_t x, uint32_t* first_count) {
+// in sw and in the touched list; a pending request is not repeated).  The
+// touched-list and ring reservations are one atomic each, both in flight
+// before either result is used.
+__device__ __forceinline__ void request_check(const Params& p, bool pred, uint32_t x) {
   bool first = false, push = false;
   if (pred) {
     first = !(atomicOr(&p.sw[x], kSwTouched) & kSwTouched);
     const uint32_t bit = 1u << (x & 31);
     push = !(atomicOr(&p.inq[1][x >> 5], bit) & bit);
   }
-  const uint32_t slot = vxb::warp_append(first, &p.c->touched_n);
-  if (first) p.lst_t[slot] = x;
-  if (first_count) vxb::warp_append(first, first_count);
-  ring_push(p, push, x);
+  const uint32_t mf = __ballot_sync(FULL, first), mp = __ballot_sync(FULL, push);
+  if (!(mf | mp)) return;
+  const int lane = threadIdx.x & 31;
+  const int lf = mf ? __ffs(mf) - 1 : 0, lp = mp ? __ffs(mp) - 1 : 0;
+  uint32_t bf = 0, bp = 0;
+  if (mf && lane == lf) bf = atomicAdd(&p.c->touched_n, (uint32_t)__popc(mf));
+  if (mp && lane == lp) bp = atomicAdd(p.rq_tail, (uint32_t)__popc(mp));
+  bf = __shfl_sync(FULL, bf, lf);
+  bp = __shfl_sync(FULL, bp, lp);
+  const uint32_t lt = vxb::lanemask_lt();
+  if (first) p.lst_t[bf + __popc(mf & lt)] = x;
+  if (push) __stcg(&p.ring[(bp + __popc(mp & lt)) & p.ring_mask], (unsigned long long)x);
 }
 
 // First position k in [lo, hi) of x's in-row (base part [b, b + nb), delta
@@ -828,13 +838,15 @@ __device__ __forceinline__ bool find_parent(const Params& p, const DevAdj& a, ui
 __device__ void check_vertex(const Params& p, uint32_t x) {
   const DevAdj& a = p.g.in;
   const int lane = threadIdx.x & 31;
-  if (lane == 0) atomicAnd(&p.inq[1][x >> 5], ~(1u << (x & 31)));
-  __syncwarp();
-  __threadfence();  // the request bit is clear before the state is read
+  // x's distance and row bounds do not change during the cascade: they load
+  // together with the clearing of the request bit
   const uint32_t d = p.dist[x];
   uint64_t b, e;
   vxb::base_range(a, x, b, e);
   const uint2 dr = a.drow[x];
+  if (lane == 0) atomicAnd(&p.inq[1][x >> 5], ~(1u << (x & 31)));
+  __syncwarp();
+  __threadfence();  // the request bit is clear before the state (witness, affected bits) is read
   const uint32_t nb = (uint32_t)(e - b), total = nb + dr.y;
   const uint32_t lim = min(total, kChunk);
   uint32_t k0 = (uint32_t)__ldcg(&p.sw[x]);
@@ -925,7 +937,7 @@ __device__ void chunk_check(const Params& p, uint32_t x, uint32_t c) {
       }
     }
   }
-  request_check(p, recheck, x, nullptr);
+  request_check(p, recheck, x);
   ring_push(p, aff, (unsigned long long)(x | kKindBit));
 }
 
@@ -976,12 +988,13 @@ struct Cascade {
       __syncthreads();
       auto expand = [&](bool valid, uint32_t x, uint32_t j) {
         bool need = false;
-        if (valid && x < P.dist_len && P.dist[x] == sm.d[j] + 1) {
+        if (valid && x < P.dist_len) {  // both loads in flight together
+          const uint32_t dx = P.dist[x];
           const unsigned long long w = __ldcg(&P.sw[x]);
           const uint32_t wit = (uint32_t)(w >> 32) & 0x7FFFFFFFu;
-          need = !(w & kSwTouched) || wit == item_vertex(sm.ex[j]) + 1;
+          need = dx == sm.d[j] + 1 && (!(w & kSwTouched) || wit == item_vertex(sm.ex[j]) + 1);
         }
-        request_check(P, need, x, nullptr);
+        request_check(P, need, x);
       };
       block_rows(P.g.out, sm.ex, nex, *lb, expand, &P);
     }

@@ -98,25 +98,41 @@ __device__ __forceinline__ uint32_t warp_append(bool pred, uint32_t* count) {
   return pred ? base + __popc(mask & lanemask_lt()) : 0xFFFFFFFFu;
 }
 
-// Lower bound of x among the low 31 bits of a sorted base row.
-__device__ __forceinline__ uint64_t lower_bound_masked(const uint32_t* a, uint64_t lo, uint64_t hi,
-                                                       uint32_t x) {
-  while (lo < hi) {
-    const uint64_t mid = lo + ((hi - lo) >> 1);
-    if ((a[mid] & kIdMask) < x) lo = mid + 1;
-    else hi = mid;
+// Lower bounds in sorted rows, 8-ary: while more than 8 candidates remain, a
+// step reads 7 evenly spaced pivots at once (one dependent round trip) and
+// keeps the eighth of the range that holds the answer; the last <= 8 entries
+// are read together and counted.  A hub row of 2^17 arcs takes 6 dependent
+// round trips where a binary search takes 17.  key(v) is the compared value
+// of an entry (the low 31 bits for base rows, whose bit 31 is the tombstone).
+template <class I, class K>
+__device__ __forceinline__ I lower_bound_8ary(const uint32_t* a, I lo, I hi, uint32_t x, K key) {
+  while (hi - lo > 8) {
+    const I step = (hi - lo) / 8;
+    uint32_t pv[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) pv[k] = key(a[lo + step * (I)(k + 1)]);
+    uint32_t below = 0;  // pivots below x; they are sorted, so these are the first ones
+#pragma unroll
+    for (int k = 0; k < 7; ++k) below += pv[k] < x ? 1u : 0u;
+    const I nhi = below < 7 ? lo + step * (I)(below + 1) : hi;
+    lo = below ? lo + step * (I)below + 1 : lo;
+    hi = nhi;
   }
-  return lo;
+  uint32_t tail[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) tail[k] = lo + (I)k < hi ? key(a[lo + (I)k]) : 0xFFFFFFFFu;
+  I n = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) n += (lo + (I)k < hi && tail[k] < x) ? (I)1 : (I)0;
+  return lo + n;
 }
 
-__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t lo, uint32_t hi,
-                                                    uint32_t x) {
-  while (lo < hi) {
-    const uint32_t mid = lo + ((hi - lo) >> 1);
-    if (a[mid] < x) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo;
+__device__ __forceinline__ uint64_t lower_bound_masked(const uint32_t* a, uint64_t lo, uint64_t hi, uint32_t x) {
+  return lower_bound_8ary<uint64_t>(a, lo, hi, x, [](uint32_t v) { return v & kIdMask; });
+}
+
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t* a, uint32_t lo, uint32_t hi, uint32_t x) {
+  return lower_bound_8ary<uint32_t>(a, lo, hi, x, [](uint32_t v) { return v; });
 }
 
 // Grid-wide barrier for cooperative (co-resident) launches on one arrival
