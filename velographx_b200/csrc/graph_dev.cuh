@@ -41,7 +41,7 @@ __device__ __forceinline__ uint32_t merged_at(uint32_t k, const uint32_t* A, uin
 
 // Merges of a short list (nB <= 32, the usual run of one row in a batch):
 // lane j holds B[j] and its final index slot_j = lower_bound(A, B[j]) + j,
-// found once by parallel binary searches.  Output k is then B[j] where
+// found once by parallel row searches.  Output k is then B[j] where
 // k == slot_j, else A[k - t] with t the number of slots below k (a register
 // scan over the lanes), so each 32 outputs cost one load instead of a
 // co-rank search each.
