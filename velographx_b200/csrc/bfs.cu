@@ -1800,15 +1800,20 @@ static int ensure_capacity(Bfs* b, size_t V) {
   const size_t words = (c + 31) / 32 + 1;
   cudaStream_t s = b->g->stream;
   VX_CUDA_TRY(cudaStreamSynchronize(s));
+  // fills and copies go on the graph's (non-blocking) stream, ahead of the
+  // kernels that use the new buffers; the old buffers are freed once the
+  // stream has finished copying out of them
+  std::vector<uint32_t*> old;
   auto realloc_copy = [&](uint32_t** p, size_t n_new, size_t n_old, int fill) -> int {
     uint32_t* q = nullptr;
     if (cudaMalloc(&q, n_new * sizeof(uint32_t)) != cudaSuccess) {
       set_error("BFS allocation of %zu bytes failed", n_new * 4);
       return -4;
     }
-    if (cudaMemset(q, fill, n_new * sizeof(uint32_t)) != cudaSuccess) return -3;
-    if (*p && n_old) cudaMemcpy(q, *p, n_old * sizeof(uint32_t), cudaMemcpyDeviceToDevice);
-    cudaFree(*p);
+    if (cudaMemsetAsync(q, fill, n_new * sizeof(uint32_t), s) != cudaSuccess) return -3;
+    if (*p && n_old && cudaMemcpyAsync(q, *p, n_old * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      return -3;
+    if (*p) old.push_back(*p);
     *p = q;
     return 0;
   };
@@ -1828,7 +1833,10 @@ static int ensure_capacity(Bfs* b, size_t V) {
   rc |= realloc_copy(&b->lst_a, c, 0, 0);
   rc |= realloc_copy(&b->lst_t, c, 0, 0);
   rc |= realloc_copy(&b->tent, c, 0, 0);
+  const cudaError_t e = cudaStreamSynchronize(s);
+  for (uint32_t* p : old) cudaFree(p);
   if (rc) return -4;
+  VX_CUDA_TRY(e);
   b->cap = c;
   return 0;
 }
@@ -1851,7 +1859,10 @@ static int ensure_ring(Bfs* b) {
     set_error("BFS work ring allocation of %zu bytes failed", slots * 8);
     return -4;
   }
-  VX_CUDA_TRY(cudaMemset(b->ring, 0xFF, slots * sizeof(unsigned long long)));
+  // on the graph's stream, so the first launch that drains the ring sees every
+  // slot empty (the graph's stream is non-blocking: a legacy-stream memset
+  // would not be ordered before it)
+  VX_CUDA_TRY(cudaMemsetAsync(b->ring, 0xFF, slots * sizeof(unsigned long long), b->g->stream));
   b->ring_slots = slots;
   return 0;
 }

@@ -137,7 +137,11 @@ int vx_graph_bulk_load(vx_graph* g, const uint32_t* uv, size_t n) {
   uint32_t* d = nullptr;
   if (cudaMalloc(&d, std::max<size_t>(n, 1) * 8) != cudaSuccess) return fail(VX_ERR_NOMEM, "bulk load upload");
   int rc = VX_OK;
-  if (n && cudaMemcpy(d, uv, n * 8, cudaMemcpyHostToDevice) != cudaSuccess) rc = fail(VX_ERR_CUDA, "bulk copy");
+  // on the graph's own (non-blocking) stream: a plain cudaMemcpy from pageable
+  // memory may return before its DMA lands and is not ordered before the load
+  // kernels on that stream
+  if (n && cudaMemcpyAsync(d, uv, n * 8, cudaMemcpyHostToDevice, g->g->stream) != cudaSuccess)
+    rc = fail(VX_ERR_CUDA, "bulk copy");
   if (!rc) rc = vxh::graph_bulk_load(g->g, d, n);
   cudaFree(d);
   return rc;

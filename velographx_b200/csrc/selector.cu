@@ -340,10 +340,13 @@ int selector_create(Selector** out, uint64_t seed) {
   for (int i = oW1; i < oB1; ++i) h[i] = next() * std::sqrt(6.f / kIn);
   for (int i = oW2; i < oB2; ++i) h[i] = next() * std::sqrt(6.f / kH);
   for (int i = oW3; i < oB3; ++i) h[i] = next() * std::sqrt(3.f / kH);
-  const cudaError_t e = cudaMemcpy(s->params, h, kSelParams * 4, cudaMemcpyHostToDevice);
+  // uploads and fills go on the selector's (non-blocking) stream, ahead of its
+  // kernels; the copy from pageable memory is staged before this returns
+  cudaError_t e = cudaMemcpyAsync(s->params, h, kSelParams * 4, cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->adam_m, 0, kSelParams * 4, s->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->adam_v, 0, kSelParams * 4, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
   delete[] h;
-  cudaMemset(s->adam_m, 0, kSelParams * 4);
-  cudaMemset(s->adam_v, 0, kSelParams * 4);
   if (e != cudaSuccess) {
     set_error("selector initialisation failed");
     selector_destroy(s);
@@ -364,12 +367,13 @@ void selector_destroy(Selector* s) {
   delete s;
 }
 
-static int upload(const void* host, size_t bytes, void** dev) {
+// Device copy of a host array, ordered on `stream` before the kernels that read it.
+static int upload(const void* host, size_t bytes, void** dev, cudaStream_t stream) {
   if (cudaMalloc(dev, bytes ? bytes : 4) != cudaSuccess) {
     set_error("selector staging allocation failed");
     return -4;
   }
-  if (bytes && host) VX_CUDA_TRY(cudaMemcpy(*dev, host, bytes, cudaMemcpyHostToDevice));
+  if (bytes && host) VX_CUDA_TRY(cudaMemcpyAsync(*dev, host, bytes, cudaMemcpyHostToDevice, stream));
   return 0;
 }
 
@@ -380,9 +384,9 @@ int selector_train(Selector* s, const float* X, const float* Y, size_t n, uint32
     return -1;
   }
   void *dx = nullptr, *dy = nullptr, *perm = nullptr;
-  int rc = upload(X, n * kIn * 4, &dx);
-  if (!rc) rc = upload(Y, n * kOut * 4, &dy);
-  if (!rc) rc = upload(nullptr, n * 4, &perm);
+  int rc = upload(X, n * kIn * 4, &dx, s->stream);
+  if (!rc) rc = upload(Y, n * kOut * 4, &dy, s->stream);
+  if (!rc) rc = upload(nullptr, n * 4, &perm, s->stream);
   if (!rc) {
     static bool attr = false;
     if (!attr) {
@@ -414,9 +418,9 @@ int selector_gradients(Selector* s, const float* X, const float* Y, size_t n, fl
   uint32_t idx[kMaxBatch];
   for (size_t i = 0; i < n; ++i) idx[i] = (uint32_t)i;
   void *dx = nullptr, *dy = nullptr, *di = nullptr;
-  int rc = upload(X, n * kIn * 4, &dx);
-  if (!rc) rc = upload(Y, n * kOut * 4, &dy);
-  if (!rc) rc = upload(idx, n * 4, &di);
+  int rc = upload(X, n * kIn * 4, &dx, s->stream);
+  if (!rc) rc = upload(Y, n * kOut * 4, &dy, s->stream);
+  if (!rc) rc = upload(idx, n * 4, &di, s->stream);
   if (!rc) {
     static bool attr = false;
     if (!attr) {
@@ -442,8 +446,8 @@ int selector_gradients(Selector* s, const float* X, const float* Y, size_t n, fl
 
 int selector_predict(Selector* s, const float* X, size_t n, float* Y) {
   void *dx = nullptr, *dy = nullptr;
-  int rc = upload(X, n * kIn * 4, &dx);
-  if (!rc) rc = upload(nullptr, n * kOut * 4, &dy);
+  int rc = upload(X, n * kIn * 4, &dx, s->stream);
+  if (!rc) rc = upload(nullptr, n * kOut * 4, &dy, s->stream);
   if (!rc && n) {
     count_launch();
     const unsigned blocks = (unsigned)std::min<size_t>((n + 7) / 8, 1024);
@@ -461,14 +465,16 @@ int selector_predict(Selector* s, const float* X, size_t n, float* Y) {
 }
 
 int selector_set_params(Selector* s, const float* p) {
-  VX_CUDA_TRY(cudaMemcpy(s->params, p, kSelParams * 4, cudaMemcpyHostToDevice));
-  VX_CUDA_TRY(cudaMemset(s->adam_m, 0, kSelParams * 4));
-  VX_CUDA_TRY(cudaMemset(s->adam_v, 0, kSelParams * 4));
+  VX_CUDA_TRY(cudaMemcpyAsync(s->params, p, kSelParams * 4, cudaMemcpyHostToDevice, s->stream));
+  VX_CUDA_TRY(cudaMemsetAsync(s->adam_m, 0, kSelParams * 4, s->stream));
+  VX_CUDA_TRY(cudaMemsetAsync(s->adam_v, 0, kSelParams * 4, s->stream));
+  VX_CUDA_TRY(cudaStreamSynchronize(s->stream));
   return 0;
 }
 
 int selector_get_params(Selector* s, float* p) {
-  VX_CUDA_TRY(cudaMemcpy(p, s->params, kSelParams * 4, cudaMemcpyDeviceToHost));
+  VX_CUDA_TRY(cudaMemcpyAsync(p, s->params, kSelParams * 4, cudaMemcpyDeviceToHost, s->stream));
+  VX_CUDA_TRY(cudaStreamSynchronize(s->stream));
   return 0;
 }
 
