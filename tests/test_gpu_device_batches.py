@@ -89,6 +89,25 @@ def test_graph_only_device_batches():
             assert sorted(gd.neighbors(u)) == sorted(gh.neighbors(u)), (t, u)
 
 
+def test_repeated_bulk_loads_size_the_graph_exactly():
+    """Host edge lists are uploaded on the graph's own stream: graph after graph
+    in one process (device memory reused between them), the vertex count after
+    a bulk load is max id + 1 and the arc count is the loaded one."""
+    base = w.rmat_edges(13, 8, seed=12)
+    e = base[base[:, 0] != base[:, 1]]
+    expect_arcs = np.unique(np.concatenate([e[:, 0].astype(np.uint64) << 32 | e[:, 1],
+                                            e[:, 1].astype(np.uint64) << 32 | e[:, 0]])).size
+    V = 1 << 13
+    for t in range(12):
+        edges = base.copy()  # a fresh host array each time
+        g = vx.Graph(V if t % 2 else 16, False)
+        g.bulk_load_edges(edges)
+        assert g.vertex_count == max(V if t % 2 else 16, int(e.max()) + 1), t
+        assert g.edge_count_directed() == expect_arcs, t
+        b = vx.IncrementalBFS(g, 0)
+        assert b.distances_array().size == g.vertex_count, t
+
+
 def test_device_batch_vertex_bound_is_checked():
     g = vx.Graph(16, False)
     b = vx.IncrementalBFS(g, 0)
