@@ -790,6 +790,25 @@ __device__ __forceinline__ void request_check(const Params& p, bool pred, uint32
   if (push) __stcg(&p.ring[(bp + __popc(mp & lt)) & p.ring_mask], (unsigned long long)x);
 }
 
+// expand(y) for a newly affected y at distance dy, applied to one arc (y, x)
+// of y's out-row (warp-uniform): x gets a check if it sits at dy + 1 and its
+// witness is y or no check has touched it yet.
+constexpr uint32_t kInlineExpand = 64;  // out-rows this short are expanded by the warp that marked y
+struct ExpandChildren {
+  const Params* p;
+  uint32_t y, dy;
+  __device__ __forceinline__ void operator()(bool valid, uint32_t x, uint32_t) {
+    bool need = false;
+    if (valid && x < p->dist_len) {
+      const uint32_t dx = p->dist[x];
+      const unsigned long long w = __ldcg(&p->sw[x]);
+      const uint32_t wit = (uint32_t)(w >> 32) & 0x7FFFFFFFu;
+      need = dx == dy + 1 && (!(w & kSwTouched) || wit == y + 1);
+    }
+    request_check(*p, need, x);
+  }
+};
+
 // First position k in [lo, hi) of x's in-row (base part [b, b + nb), delta
 // part from darena[dx]) whose tail y survives, sits at distance d - 1 and is
 // not affected; whole warp, warp-uniform result.  Each step covers 128 arcs:
@@ -881,12 +900,27 @@ __device__ void check_vertex(const Params& p, uint32_t x) {
         ring_push(p, c0 + lane < K, kChunkCheckBit | ((unsigned long long)(c0 + lane + 1) << 32) | x);
     return;
   }
-  bool push = false;
+  bool marked = false;
   if (lane == 0) {
     __stcg(&p.sw[x], kSwTouched | (unsigned long long)total);
-    push = mark_affected(p, x);
+    marked = mark_affected(p, x);
   }
-  ring_push(p, push, (unsigned long long)(x | kKindBit));
+  marked = __shfl_sync(FULL, marked, 0);
+  bool inlined = false;
+  if (marked) {
+    // a short out-row is expanded here instead of through one more ring round;
+    // every lane fences after the affected bit (set and fenced by lane 0)
+    // before it reads a child's witness, as the expanding block does after
+    // claiming an expand item
+    __syncwarp();
+    __threadfence();
+    if (degree_of(p.g.out, x) <= kInlineExpand) {
+      ExpandChildren ec{&p, x, d};
+      warp_row(p.g.out, x, ec);
+      inlined = true;
+    }
+  }
+  ring_push(p, marked && !inlined && lane == 0, (unsigned long long)(x | kKindBit));
 }
 
 // One chunk c >= 1 of a long check (whole warp): scan [c * kChunk,
