@@ -61,7 +61,7 @@ def parse():
 
 
 def workload(args):
-    from velographx_b200 import workloads as w
+    import workloads as w
 
     V = 1 << args.scale
     edges = w.rmat_edges(args.scale, args.edge_factor, seed=args.seed)
@@ -73,7 +73,7 @@ def workload(args):
 
 def vx_roots(roots, k, V, edges, args):
     """k seeded non-isolated roots (the first len(roots) are the single-root ones)."""
-    from velographx_b200 import workloads as w
+    import workloads as w
 
     if k <= len(roots):
         return roots[:k]
@@ -398,7 +398,7 @@ def run_b200(args, rank, world, local):
     }
     if world == 1 and not args.no_extras:
         # the other stream configurations, end to end (not part of the timed region above)
-        from velographx_b200 import stream_bench as sbm
+        from workloads import streams as sbm
 
         del b
         torch.cuda.synchronize()

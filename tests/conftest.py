@@ -16,9 +16,9 @@ def pytest_configure(config):
 @pytest.fixture(scope="session", autouse=True)
 def _oracle_built():
     """The oracle libraries are test infrastructure; build them if missing (CPU only)."""
-    lib = os.path.join(ROOT, "oracle", "liboracle.so")
-    if not os.path.exists(lib):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle")], check=True)
+    for sub, lib in (("oracle", "liboracle.so"), ("workloads", "libvxgen.so")):
+        if not os.path.exists(os.path.join(ROOT, sub, lib)):
+            subprocess.run(["make", "-s", "-C", os.path.join(ROOT, sub)], check=True)
 
 
 def gpu_available() -> bool:

@@ -223,7 +223,7 @@ def test_capi_direct_calls():
 def test_large_batches_use_the_multipass_path(directed):
     """Batches above one cluster's capacity (~90k arcs) take the multi-kernel
     sort path; results must be the same."""
-    from velographx_b200 import workloads as w
+    import workloads as w
 
     V = 1 << 15
     e = w.rmat_edges(15, seed=31)

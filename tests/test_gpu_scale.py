@@ -8,7 +8,7 @@ import pytest
 
 from oracle import OracleBFS, OracleGraph
 from oracle import load as load_oracle
-from velographx_b200 import workloads as w
+import workloads as w
 
 pytestmark = pytest.mark.gpu
 vx = pytest.importorskip("velographx_b200")

@@ -21,8 +21,9 @@ if not torch.cuda.is_available():
     pytest.skip("needs a CUDA device", allow_module_level=True)
 
 import velographx_b200 as vx  # noqa: E402
-from velographx_b200 import selector as sel  # noqa: E402
-from velographx_b200 import workloads as w  # noqa: E402
+from velographx_b200 import selector as sel
+from workloads import selector_study as study  # noqa: E402
+import workloads as w  # noqa: E402
 
 # fp32 accumulation over at most 64 samples x 64 hidden units
 GRAD_RTOL = 2e-4
@@ -161,11 +162,11 @@ def test_reduced_regime_study():
     edges = w.rmat_edges(14, 16, seed=21)
     root = w.max_degree_root(edges, V)
     sizes = np.tile([10, 300, 3000, 30000], 12)
-    rd = sel.collect("rmat14", edges, V, root, sizes, 0.75, seed=4)
+    rd = study.collect("rmat14", edges, V, root, sizes, 0.75, seed=4)
     assert rd.exact
     assert np.all(rd.t_repair > 0) and np.all(rd.t_full > 0)
     assert np.all(np.isfinite(rd.features))
-    rep = sel.evaluate([rd], train_fraction=0.3, epochs=200)
+    rep = study.evaluate([rd], train_fraction=0.3, epochs=200)
     for arm in ("mlp", "heuristic"):
         r = rep[arm]
         assert 0 <= r["wrong_arm_rate"] <= 1

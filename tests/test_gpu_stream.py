@@ -21,7 +21,7 @@ if not torch.cuda.is_available():
     pytest.skip("needs a CUDA device", allow_module_level=True)
 
 import velographx_b200 as vx  # noqa: E402
-from velographx_b200 import workloads as w  # noqa: E402
+import workloads as w  # noqa: E402
 
 
 def mix64(z: np.ndarray) -> np.ndarray:

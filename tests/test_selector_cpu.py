@@ -12,6 +12,7 @@ import pytest
 
 from oracle import selector_ref as ref
 from velographx_b200 import selector as sel
+from workloads import selector_study as study
 
 
 @pytest.mark.parametrize("vertices,reach", [(1000, 0.9), (1000, 0.1), (1000, 0.01), (1 << 20, 0.7)])
@@ -77,4 +78,4 @@ def test_shallow_parent_deletion_fraction_example():
     # 0-1 tree arc (d=1); 2-1 reversed tree arc at depth 2; 3-4 at depth 4 (too deep);
     # 4-3 reversed at depth 4; 1-6 not a tree arc; 5 unreachable; 0-6 an insertion;
     # 6-0 reversed tree arc at depth 1
-    assert sel.shallow_parent_deletion_fraction(src, dst, add, dist) == pytest.approx(3 / 8)
+    assert study.shallow_parent_deletion_fraction(src, dst, add, dist) == pytest.approx(3 / 8)

@@ -40,7 +40,7 @@ def entry_point():
 
 @pytest.mark.skipif(not torch.cuda.is_available(), reason="needs a CUDA device")
 def test_static_scratch_bfs_matches_regular_entry_point():
-    from velographx_b200 import workloads as w
+    import workloads as w
 
     V = 1 << 16
     edges = w.rmat_edges(16, seed=16)

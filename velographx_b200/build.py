@@ -50,8 +50,14 @@ def build_library(verbose_ptxas: bool = False) -> str:
             extra = ["-Xptxas", "-v"] if verbose_ptxas else []
             _run([NVCC] + NVCC_FLAGS + extra + ["-c", src, "-o", obj])
         objs.append(obj)
-    if _newer(LIB, objs):
+    # relink when an object changed or the set of sources did
+    manifest = os.path.join(BUILD, "objects.txt")
+    listing = "\n".join(objs)
+    old = open(manifest).read() if os.path.exists(manifest) else None
+    if _newer(LIB, objs) or old != listing:
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs)
+        with open(manifest, "w") as f:
+            f.write(listing)
     return LIB
 
 

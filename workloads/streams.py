@@ -16,8 +16,8 @@
 Every run times batches with CUDA events on the graph's stream and checks the
 maintained distances against a fresh full BFS at regular batches.
 
-  python -m velographx_b200.stream_bench --workload grid [--batches 500]
-  python -m velographx_b200.stream_bench --workload lognormal [--scale 20]
+  python -m workloads.streams --workload grid [--batches 500]
+  python -m workloads.streams --workload lognormal [--scale 20]
 """
 from __future__ import annotations
 
@@ -28,42 +28,14 @@ import time
 
 import numpy as np
 
-from . import Graph, IncrementalBFS
-from . import workloads as w
+import workloads as w
+from velographx_b200 import Graph, IncrementalBFS
 
 
 def _events():
     import torch
 
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-
-
-def near_root_stream(edges: np.ndarray, vertices: int, dist: np.ndarray, batches: int, ops: int,
-                     delete_fraction: float, seed: int) -> w.Stream:
-    """Batches of `ops` updates: round(ops * delete_fraction) deletions of edges
-    drawn at random from the 2x-sized pool of edges nearest the root (by the
-    larger endpoint distance), the rest uniform-random insertions; each batch
-    shuffled."""
-    rng = np.random.default_rng(seed)
-    e = edges[edges[:, 0] != edges[:, 1]]
-    nd = int(round(ops * delete_fraction))
-    total = nd * batches
-    key = np.maximum(dist[e[:, 0]].astype(np.uint64), dist[e[:, 1]].astype(np.uint64))
-    pool = np.argsort(key, kind="stable")[: min(e.shape[0], 2 * total)]
-    pick = rng.choice(pool, size=total, replace=total > pool.size)
-    ni = ops - nd
-    src = np.empty(batches * ops, np.uint32)
-    dst = np.empty(batches * ops, np.uint32)
-    add = np.empty(batches * ops, np.uint8)
-    for b in range(batches):
-        s = np.concatenate([e[pick[b * nd:(b + 1) * nd], 0], rng.integers(0, vertices, ni, dtype=np.uint32)])
-        d = np.concatenate([e[pick[b * nd:(b + 1) * nd], 1], rng.integers(0, vertices, ni, dtype=np.uint32)])
-        a = np.concatenate([np.zeros(nd, np.uint8), np.ones(ni, np.uint8)])
-        perm = rng.permutation(ops)
-        lo = b * ops
-        src[lo:lo + ops], dst[lo:lo + ops], add[lo:lo + ops] = s[perm], d[perm], a[perm]
-    offsets = np.arange(batches + 1, dtype=np.int64) * ops
-    return w.Stream(src, dst, add, offsets)
 
 
 def pinned_stream(st: w.Stream) -> w.Stream:
@@ -140,7 +112,7 @@ def grid(side: int = 4096, long_range: float = 0.001, batches: int = 500, ops: i
     e1.synchronize()
     full_ms = e0.elapsed_time(e1)
     levels = bfs.stats()["levels"]
-    stream = near_root_stream(edges, V, bfs.distances_array(), batches, ops, delete_fraction, seed + 1)
+    stream = w.near_root_stream(edges, V, bfs.distances_array(), batches, ops, delete_fraction, seed + 1)
     res = run_stream(g, bfs, root, stream, check_every)
     res.update({"workload": f"grid{side}x{side}+{long_range:g}-long-range-root0-{ops}-op-batches-"
                             f"{int(delete_fraction * 100)}pct-near-root-deletions",
