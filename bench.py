@@ -51,6 +51,8 @@ def parse():
     p.add_argument("--insert-fraction", type=float, default=0.7)
     p.add_argument("--roots", type=int, default=64)
     p.add_argument("--check-batches", type=int, default=8)
+    p.add_argument("--ref-batches", type=int, default=20,
+                   help="batches of each stream checked bit-exactly against the CPU reference after every batch")
     p.add_argument("--cpu-seconds", type=float, default=20.0, help="bound of the CPU-baseline sample")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-extras", action="store_true", help="skip the lognormal and grid stream measurements")
@@ -355,6 +357,21 @@ def run_b200(args, rank, world, local):
         exact = exact and same and b.reachable_count == fresh.reachable_count
         del fresh
 
+    # ---- the records of the first ref_batches batches on a fresh replica
+    # (untimed), for the per-batch comparison with the CPU reference ----
+    gpu_recs = []
+    if rank == 0 and world == 1 and not args.no_cpu and args.ref_batches:
+        from workloads.streams import record
+
+        gv = vx.Graph(V, False)
+        gv.bulk_load_edges(edges)
+        bv = vx.IncrementalBFS(gv, root)
+        bv.set_tuning(alpha, beta, 1024)
+        for i in range(min(args.ref_batches, stream.batches)):
+            bv.apply_arrays(*stream.batch(i))
+            gpu_recs.append(record(gv, bv))
+        del bv, gv
+
     hbm, hbm_kind = measured_hbm()
     traffic = profiled_traffic()
     line = {
@@ -403,17 +420,24 @@ def run_b200(args, rank, world, local):
         del b
         torch.cuda.synchronize()
         c1 = sbm.insertions_c1()
-        c1_edges, c1_stream, c1_root = c1.pop("_stream")
+        ln = sbm.lognormal(20, batches=1000, check_batches=100)
+        gr = sbm.grid(4096, batches=500, check_every=100, ref_batches=args.ref_batches)
+        line["streams"] = {"insertions_rmat14": c1, "lognormal_rmat20": ln, "grid4096_near_root": gr}
+        checks = {k: v.pop("_check", None) for k, v in line["streams"].items()}
+        roots20 = ln.pop("_roots", None)
         if rank == 0 and not args.no_cpu:
-            c1["cpu_baseline"] = c1_reference(c1_edges, c1_stream, c1_root, c1["digests"])
-        c1.pop("digests")
-        line["streams"] = {
-            "insertions_rmat14": c1,
-            "lognormal_rmat20": sbm.lognormal(20, batches=1000, check_batches=100),
-            "grid4096_near_root": sbm.grid(4096, batches=500, check_every=100),
-        }
+            for name, rec_samples in (("insertions_rmat14", 5), ("lognormal_rmat20", 2), ("grid4096_near_root", 1)):
+                if checks[name] is not None:
+                    ce, cst, croot, crecs = checks[name]
+                    line["streams"][name]["cpu_baseline"] = reference_check(
+                        ce, line["streams"][name]["vertices"], croot, cst, crecs, rec_samples)
+            if roots20 is not None:
+                ln["multiroot"]["cpu_baseline"] = reference_multiroot(checks["lognormal_rmat20"][0], roots20)
+        del checks
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(args, V, edges, roots, stream)
+        line["cpu_baseline"] = cpu_baseline(args, V, edges, roots, stream, gpu_recs)
+        line["exact_vs_reference"] = dict(line["cpu_baseline"].get("exact_vs_reference", {}))
+        line["host"] = host_info()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -446,54 +470,75 @@ def reference_stream(args, V, edges, root, stream, first, count, budget_s):
     return done, t
 
 
-def c1_reference(edges, stream, root, gpu_digests):
-    """The reference's IncrementalBFS::apply (oracle/_ref, one thread) on the
-    100 x 64-insertion stream; every batch's distances against the GPU's
-    digests (splitmix64 sum, as vx_bfs_digest)."""
-    from oracle import OracleBFS, OracleGraph, available
+def host_info() -> dict:
+    """The host's core count and CPU model (the CPU baseline runs there)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "cpu_model": model}
+
+
+def reference_check(edges, V, root, stream, gpu_recs, recompute_samples=1, budget_s=None):
+    """The reference's IncrementalBFS::apply (oracle/_ref, single-threaded, as
+    the reference path is) on the first len(gpu_recs) batches of the stream,
+    each batch's post-batch state compared with the GPU's record; then
+    recompute() timed recompute_samples times (the full arm of every batch)."""
+    from oracle import available
+    from oracle.replay import BatchRecord, Replay, mismatch
 
     if not available("reference"):
         return {"value": None, "unavailable": "oracle/_ref not built"}
-    V = 1 << 14
-    g = OracleGraph(V, False, "reference")
-    g.bulk_load_edges(edges)
-    b = OracleBFS(g, root)
-    t, exact = 0.0, True
-    for i in range(stream.batches):
-        s, d, a = stream.batch(i)
-        t0 = time.perf_counter()
-        b.apply(s, d, a)
-        t += time.perf_counter() - t0
-        dist = b.distances().astype(np.uint64)
-        v = np.arange(dist.size, dtype=np.uint64)
-        with np.errstate(over="ignore"):
-            z = (v << np.uint64(32)) | dist
-            z = z + np.uint64(0x9E3779B97F4A7C15)
-            z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
-            z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
-            z = z ^ (z >> np.uint64(31))
-            exact = exact and int(np.sum(z, dtype=np.uint64)) == gpu_digests[i]
-    return {"value": stream.batches / t, "unit": "batches/s", "cores": 1, "kind": "reference",
-            "sample": "IncrementalBFS::apply on all 100 batches (single-threaded)",
-            "exact_every_batch_vs_gpu": bool(exact)}
+    rp = Replay(edges, V, root, kind="reference")
+    t, n, bad = 0.0, 0, []
+    for i, rec in enumerate(gpu_recs):
+        t += rp.apply_timed(*stream.batch(i))
+        n += 1
+        why = mismatch(BatchRecord(*rec), rp.record(), V, rp.fraction)
+        if why:
+            bad.append(f"batch {i}: {why}")
+        if budget_s is not None and t > budget_s:
+            break
+    rec_s = [rp.recompute_timed() for _ in range(recompute_samples)]
+    return {"value": n / t if t > 0 else None, "unit": "batches/s", "cores": 1, "kind": "reference",
+            "sample": f"IncrementalBFS::apply on the first {n} batches of the same stream (single-threaded, as "
+                      f"the reference path is), each checked against the GPU",
+            "recompute_ms": float(np.median(rec_s)) * 1e3,
+            "recompute_sample": f"IncrementalBFS::recompute, {recompute_samples} run(s), single-threaded",
+            "exact_vs_reference": {"batches": n, "exact": not bad, "first_mismatch": bad[:1]}}
 
 
-def cpu_baseline(args, V, edges, roots, stream):
+def reference_multiroot(edges, roots):
+    """The reference's multicore path for many roots: thread-per-root
+    bfs_distances over all host cores (benchmarks/thread_scaling_bfs.cpp:78-108)."""
     from oracle import available, csr_multi_bfs
+
+    if not available("reference"):
+        return {"value": None, "unavailable": "oracle/_ref not built"}
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    _, arcs, _ = csr_multi_bfs(edges, roots, cores)
+    tb = time.perf_counter() - t0
+    return {"value": float(arcs.sum() / 2 / tb / 1e9), "unit": "GTEPS", "cores": cores, "kind": "reference",
+            "ms": tb * 1e3, "sample": f"thread-per-root bfs_distances over {len(roots)} roots on {cores} threads"}
+
+
+def cpu_baseline(args, V, edges, roots, stream, gpu_recs):
+    from oracle import available
 
     if not available("reference"):
         return {"value": None, "unit": "batches/s", "cores": 0, "kind": "reference",
                 "sample": "unavailable: oracle/_ref not built"}
-    n, t = reference_stream(args, V, edges, int(roots[0]), stream, 0, args.steps, args.cpu_seconds)
-    cores = os.cpu_count() or 1
-    out = {"value": n / t, "unit": "batches/s", "cores": 1, "kind": "reference",
-           "sample": f"IncrementalBFS::apply on the first {n} batches of the same stream (single-threaded, as the "
-                     f"reference path is)"}
-    t0 = time.perf_counter()
-    _, arcs, _ = csr_multi_bfs(edges, roots, cores)
-    tb = time.perf_counter() - t0
-    out["bfs_gteps"] = float(arcs.sum() / 2 / tb / 1e9)
-    out["bfs_sample"] = f"thread-per-root bfs_distances over {len(roots)} roots on {cores} threads"
+    out = reference_check(edges, V, int(roots[0]), stream, gpu_recs, recompute_samples=2,
+                          budget_s=args.cpu_seconds)
+    mr = reference_multiroot(edges, roots)
+    out["bfs_gteps"] = mr["value"]
+    out["bfs_sample"] = mr["sample"]
     return out
 
 
@@ -518,6 +563,7 @@ def run_reference(args, rank, world):
         "cpu_baseline": {"value": value, "unit": "batches/s", "cores": 1, "kind": "reference",
                          "sample": f"IncrementalBFS::apply, batches {w}..{w + n - 1} of the stream"},
         "e2e": {"value": value, "unit": "batches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "host": host_info(),
     }), flush=True)
 
 

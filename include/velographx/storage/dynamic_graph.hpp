@@ -8,6 +8,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <span>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -99,6 +100,9 @@ class DynamicGraph {
     return d != 0;
   }
 
+  // :493-500 -- grows the vertex count; the version is unchanged
+  void ensure_vertex(VertexId v) { detail::check(vx_graph_ensure_vertex(g_, v)); }
+
   void bulk_load_edges(const std::vector<std::pair<VertexId, VertexId>>& edges) {
     std::vector<std::uint32_t> uv(edges.size() * 2);
     for (std::size_t i = 0; i < edges.size(); ++i) {
@@ -137,6 +141,19 @@ class DynamicGraph {
     for (auto u : in_neighbors(v)) fn(u);
   }
 
+  // :573-581 -- the row as of the last consolidation.  The span points into a
+  // host copy owned by this object, valid until the next compact_*neighbors
+  // call in the same direction (the reference's points into its own storage,
+  // valid until the next mutation).
+  [[nodiscard]] std::span<const VertexId> compact_neighbors(VertexId u) const {
+    compact_row(u, false, compact_out_buf_);
+    return compact_out_buf_;
+  }
+  [[nodiscard]] std::span<const VertexId> compact_in_neighbors(VertexId v) const {
+    compact_row(v, true, compact_in_buf_);
+    return compact_in_buf_;
+  }
+
   [[nodiscard]] bool has_edge(VertexId u, VertexId v) const {
     int r = 0;
     detail::check(vx_graph_has_edge(g_, u, v, &r));
@@ -146,6 +163,23 @@ class DynamicGraph {
     std::size_t n = 0;
     detail::check(vx_graph_edge_count_directed(g_, &n));
     return n;
+  }
+  // :593-595
+  [[nodiscard]] std::size_t base_edge_count_directed() const {
+    std::size_t n = 0;
+    detail::check(vx_graph_base_edge_count_directed(g_, &n));
+    return n;
+  }
+  // :599-605 -- device bytes of the graph's storage
+  [[nodiscard]] std::size_t storage_bytes() const {
+    std::size_t n = 0;
+    detail::check(vx_graph_storage_bytes(g_, &n));
+    return n;
+  }
+  // :607-610
+  [[nodiscard]] double delta_ratio() const {
+    const std::size_t base = base_edge_count_directed();
+    return static_cast<double>(delta_edge_count()) / static_cast<double>(base > 1 ? base : 1);
   }
   [[nodiscard]] std::size_t delta_edge_count() const {
     std::size_t n = 0;
@@ -178,6 +212,13 @@ class DynamicGraph {
     if (n) detail::check(fn(g_, u, out.data(), n, &n));
     return out;
   }
+  void compact_row(VertexId u, bool in, std::vector<VertexId>& out) const {
+    std::size_t n = 0;
+    auto fn = in ? vx_graph_compact_in_neighbors : vx_graph_compact_neighbors;
+    detail::check(fn(g_, u, nullptr, 0, &n));
+    out.resize(n);
+    if (n) detail::check(fn(g_, u, out.data(), n, &n));
+  }
   std::pair<std::size_t, std::size_t> dirty() const {
     std::size_t o = 0, i = 0;
     detail::check(vx_graph_dirty_rows(g_, &o, &i));
@@ -185,6 +226,7 @@ class DynamicGraph {
   }
 
   vx_graph* g_ = nullptr;
+  mutable std::vector<VertexId> compact_out_buf_, compact_in_buf_;
 };
 
 }  // namespace velographx

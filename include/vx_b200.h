@@ -82,6 +82,19 @@ int vx_graph_apply_device(vx_graph* g, const uint32_t* d_src, const uint32_t* d_
  * ascending order, *n = full row length. */
 int vx_graph_neighbors(vx_graph* g, uint32_t u, uint32_t* out, size_t cap, size_t* n);
 int vx_graph_in_neighbors(vx_graph* g, uint32_t v, uint32_t* out, size_t cap, size_t* n);
+/* ensure_vertex(v) :493-500: grows the vertex count to v + 1 (never shrinks;
+ * the version is unchanged). */
+int vx_graph_ensure_vertex(vx_graph* g, uint32_t v);
+/* compact_neighbors(u) :573-576 / compact_in_neighbors(v) :578-581: the row as
+ * of the last consolidation (the base CSR row; arcs deleted since are still
+ * in it), ascending; writes up to cap ids, *n = full length. */
+int vx_graph_compact_neighbors(vx_graph* g, uint32_t u, uint32_t* out, size_t cap, size_t* n);
+int vx_graph_compact_in_neighbors(vx_graph* g, uint32_t v, uint32_t* out, size_t cap, size_t* n);
+/* base_edge_count_directed() :593-595: arcs of the compact representation. */
+int vx_graph_base_edge_count_directed(vx_graph* g, size_t* out);
+/* storage_bytes() :599-605: here the device bytes the graph's storage holds
+ * (its layout differs from the reference's host layout). */
+int vx_graph_storage_bytes(vx_graph* g, size_t* out);
 /* has_edge(u, v) :583-587 */
 int vx_graph_has_edge(vx_graph* g, uint32_t u, uint32_t v, int* out);
 /* edge_count_directed() :589-591, delta_edge_count() :597, is_compact() :569-571,
@@ -198,8 +211,11 @@ int vx_multiroot_bfs(vx_graph* g, const uint32_t* roots, size_t k, uint32_t* out
  * (their device memory is owned by another allocator, or they must not block
  * on the driver's allocator once running): the same direction-optimising BFS
  * as vx_bfs_recompute, on a CSR the caller holds in device memory (out- and
- * in-rows; pass the same arrays twice for an undirected graph; column ids
- * below 2^31), writing `vertices` distances to d_dist.  All other working
+ * in-rows; pass the same arrays twice for an undirected graph), writing
+ * `vertices` distances to d_dist.  Every column id must be below `vertices`
+ * (the kernel indexes d_dist and the scratch bitmaps by column id and does not
+ * check it) and rows must be free of duplicates; a source at or beyond
+ * `vertices` gives all-unreachable and *reachable = 0, as in the reference.  All other working
  * memory is one file-scope device array (~6.3 MB per GPU that loads the
  * library, held until exit), so at most 262,144 vertices (larger counts
  * return VX_ERR_RANGE).  Calls share that array: calls that overlap on the

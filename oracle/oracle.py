@@ -39,6 +39,10 @@ _SIGS = {
     "graph_dirty_in_count": (_sz, [_vp]),
     "graph_compact": (None, [_vp]),
     "graph_maybe_compact": (C.c_int, [_vp, C.c_double]),
+    "graph_ensure_vertex": (None, [_vp, C.c_uint32]),
+    "graph_base_edge_count_directed": (_sz, [_vp]),
+    "graph_compact_neighbors": (_sz, [_vp, C.c_uint32, _u32p, _sz]),
+    "graph_compact_in_neighbors": (_sz, [_vp, C.c_uint32, _u32p, _sz]),
     "bfs_create": (_vp, [_vp, C.c_uint32, C.c_double]),
     "bfs_destroy": (None, [_vp]),
     "bfs_recompute": (None, [_vp]),
@@ -144,6 +148,18 @@ class OracleGraph:
 
     def in_neighbors(self, v: int):
         return self._row(self.lib.graph_in_neighbors, v)
+
+    def compact_neighbors(self, u: int):
+        return self._row(self.lib.graph_compact_neighbors, u)
+
+    def compact_in_neighbors(self, v: int):
+        return self._row(self.lib.graph_compact_in_neighbors, v)
+
+    def ensure_vertex(self, v: int) -> None:
+        self.lib.graph_ensure_vertex(self.h, v)
+
+    def base_edge_count_directed(self) -> int:
+        return self.lib.graph_base_edge_count_directed(self.h)
 
     def has_edge(self, u: int, v: int) -> bool:
         return bool(self.lib.graph_has_edge(self.h, u, v))

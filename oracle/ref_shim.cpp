@@ -82,6 +82,24 @@ int vxr_graph_is_compact(void* g) { return static_cast<DynamicGraph*>(g)->is_com
 size_t vxr_graph_dirty_out_count(void* g) { return static_cast<DynamicGraph*>(g)->dirty_out_segment_count(); }
 size_t vxr_graph_dirty_in_count(void* g) { return static_cast<DynamicGraph*>(g)->dirty_in_segment_count(); }
 void vxr_graph_compact(void* g) { static_cast<DynamicGraph*>(g)->compact(); }
+void vxr_graph_ensure_vertex(void* g, uint32_t v) { static_cast<DynamicGraph*>(g)->ensure_vertex(v); }
+size_t vxr_graph_base_edge_count_directed(void* g) {
+  return static_cast<DynamicGraph*>(g)->base_edge_count_directed();
+}
+size_t vxr_graph_compact_neighbors(void* g, uint32_t u, uint32_t* out, size_t cap) {
+  auto* dg = static_cast<DynamicGraph*>(g);
+  if (u >= dg->vertex_count()) return 0;
+  auto row = dg->compact_neighbors(u);
+  if (out) std::memcpy(out, row.data(), std::min(cap, row.size()) * sizeof(uint32_t));
+  return row.size();
+}
+size_t vxr_graph_compact_in_neighbors(void* g, uint32_t v, uint32_t* out, size_t cap) {
+  auto* dg = static_cast<DynamicGraph*>(g);
+  if (v >= dg->vertex_count()) return 0;
+  auto row = dg->compact_in_neighbors(v);
+  if (out) std::memcpy(out, row.data(), std::min(cap, row.size()) * sizeof(uint32_t));
+  return row.size();
+}
 int vxr_graph_maybe_compact(void* g, double t) {
   return static_cast<DynamicGraph*>(g)->maybe_compact(t) ? 1 : 0;
 }

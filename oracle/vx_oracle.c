@@ -334,6 +334,26 @@ size_t vxo_graph_edge_count_directed(const vxo_graph* g) {
 
 size_t vxo_graph_delta_edge_count(const vxo_graph* g) { return g->delta_out.live; }
 
+/* base_edge_count_directed  dynamic_graph.hpp:593-595 */
+size_t vxo_graph_base_edge_count_directed(const vxo_graph* g) { return g->compact_out_edges; }
+
+/* ensure_vertex  dynamic_graph.hpp:493-500 (no version change) */
+void vxo_graph_ensure_vertex(vxo_graph* g, uint32_t v) { g_grow(g, (size_t)v + 1); }
+
+/* compact_neighbors / compact_in_neighbors  dynamic_graph.hpp:573-581: the
+ * base-or-patch row without the overlay */
+static size_t copy_row(const row_t* r, uint32_t* out, size_t cap) {
+  const size_t m = r->n < cap ? r->n : cap;
+  if (out && m) memcpy(out, r->v, m * sizeof(uint32_t));
+  return r->n;
+}
+size_t vxo_graph_compact_neighbors(const vxo_graph* g, uint32_t u, uint32_t* out, size_t cap) {
+  return u < g->V ? copy_row(&g->base_out[u], out, cap) : 0;
+}
+size_t vxo_graph_compact_in_neighbors(const vxo_graph* g, uint32_t v, uint32_t* out, size_t cap) {
+  return v < g->V ? copy_row(&g->base_in[v], out, cap) : 0;
+}
+
 int vxo_graph_is_compact(const vxo_graph* g) {
   return g->delta_out.live == 0 && g->delta_in.live == 0;
 }

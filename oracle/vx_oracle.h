@@ -49,6 +49,13 @@ int vxo_graph_is_compact(const vxo_graph* g);
 size_t vxo_graph_dirty_out_count(const vxo_graph* g);
 size_t vxo_graph_dirty_in_count(const vxo_graph* g);
 void vxo_graph_compact(vxo_graph* g);
+/* ensure_vertex  dynamic_graph.hpp:493-500 */
+void vxo_graph_ensure_vertex(vxo_graph* g, uint32_t v);
+/* base_edge_count_directed  dynamic_graph.hpp:593-595 */
+size_t vxo_graph_base_edge_count_directed(const vxo_graph* g);
+/* compact_neighbors / compact_in_neighbors  dynamic_graph.hpp:573-581 */
+size_t vxo_graph_compact_neighbors(const vxo_graph* g, uint32_t u, uint32_t* out, size_t cap);
+size_t vxo_graph_compact_in_neighbors(const vxo_graph* g, uint32_t v, uint32_t* out, size_t cap);
 int vxo_graph_maybe_compact(vxo_graph* g, double threshold);
 
 /* BasicIncrementalBFS(Graph&, VertexId, double)  bfs.hpp:18-21 */

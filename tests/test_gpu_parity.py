@@ -166,6 +166,56 @@ def test_gpu_matches_oracle_live(seed, directed):
                 assert g.in_neighbors(int(u)) == og.in_neighbors(int(u))
 
 
+@pytest.mark.parametrize("directed", [False, True])
+def test_boundary_members_match_oracle(directed):
+    """ensure_vertex, compact_neighbors / compact_in_neighbors,
+    base_edge_count_directed, delta_ratio and storage_bytes
+    (dynamic_graph.hpp:493-500, 573-610) against the oracle, with both graphs
+    consolidated at the same points; the BFS sees vertices added by
+    ensure_vertex exactly as the reference's apply does (bfs.hpp:72-74)."""
+    from oracle.replay import best_kind
+
+    kind = best_kind()
+    rng = np.random.default_rng(5 + directed)
+    V = 200
+    e = rng.integers(0, V, size=(700, 2), dtype=np.uint32)
+    og = OracleGraph(V, directed, kind)
+    og.bulk_load_edges(e)
+    ob = OracleBFS(og, 3, 0.35)
+    g = vx.Graph(V, directed)
+    g.bulk_load_edges(e)
+    b = vx.IncrementalBFS(g, 3, 0.35)
+    assert g.storage_bytes() > 0
+    for t in range(40):
+        if t % 7 == 3:
+            grow = g.vertex_count + int(rng.integers(1, 6))
+            g.ensure_vertex(grow)
+            og.ensure_vertex(grow)
+            assert g.vertex_count == og.vertex_count == grow + 1 and g.version == og.version
+        n = int(rng.integers(1, 120))
+        Vn = g.vertex_count
+        s = rng.integers(0, Vn, size=n, dtype=np.uint32)
+        d = rng.integers(0, Vn, size=n, dtype=np.uint32)
+        a = (rng.random(n) < 0.6).astype(np.uint8)
+        k = n // 3
+        pick = rng.integers(0, e.shape[0], size=k)
+        s[:k], d[:k], a[:k] = e[pick, 0], e[pick, 1], 0
+        ob.apply(s, d, a)
+        b.apply_arrays(s, d, a)
+        assert np.array_equal(b.distances_array(), ob.distances()), t
+        assert b.reachable_count == ob.reachable_count
+        if t % 9 == 8:
+            g.compact()
+            og.compact()
+        assert g.base_edge_count_directed() == og.base_edge_count_directed(), t
+        assert g.delta_edge_count() == og.delta_edge_count(), t
+        assert g.delta_ratio() == pytest.approx(g.delta_edge_count() / max(1, g.base_edge_count_directed()))
+        if t % 5 == 4:
+            for u in range(g.vertex_count):
+                assert g.compact_neighbors(u) == og.compact_neighbors(u), (t, u)
+                assert g.compact_in_neighbors(u) == og.compact_in_neighbors(u), (t, u)
+
+
 def test_loaders_and_errors():
     with pytest.raises(ValueError):
         vx.from_numpy_edges(np.zeros((3, 3), np.uint32))

@@ -87,6 +87,9 @@ def test_port_matches_reference_live(seed, directed):
         a = (rng.random(n) < 0.5).astype(np.uint8)
         for k in G:
             B[k].apply(s, d, a)
+        if t % 13 == 5:  # ensure_vertex between batches (dynamic_graph.hpp:493-500)
+            for k in G:
+                G[k].ensure_vertex(G[k].vertex_count + 2)
         if t % 11 == 0:
             for k in G:
                 G[k].maybe_compact(0.3) if t % 2 else G[k].compact()
@@ -98,8 +101,11 @@ def test_port_matches_reference_live(seed, directed):
                 gp.dirty_out_count(), gp.dirty_in_count()) == (
                 gr.vertex_count, gr.version, gr.edge_count_directed(), gr.delta_edge_count(), gr.is_compact(),
                 gr.dirty_out_count(), gr.dirty_in_count()), t
+        assert gp.base_edge_count_directed() == gr.base_edge_count_directed(), t
         for u in range(gp.vertex_count):
             assert gp.neighbors(u) == gr.neighbors(u) and gp.in_neighbors(u) == gr.in_neighbors(u)
+            assert gp.compact_neighbors(u) == gr.compact_neighbors(u), (t, u)
+            assert gp.compact_in_neighbors(u) == gr.compact_in_neighbors(u), (t, u)
 
 
 @pytest.mark.skipif(not available("reference"), reason="reference build (oracle/_ref) not present")

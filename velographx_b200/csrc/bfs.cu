@@ -19,6 +19,7 @@
 //              the affected vertices, then one asynchronous label-correcting
 //              relaxation from them and from the heads of inserted arcs.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <vector>
 
@@ -914,7 +915,8 @@ __device__ void check_vertex(const Params& p, uint32_t x) {
     // claiming an expand item
     __syncwarp();
     __threadfence();
-    if (degree_of(p.g.out, x) <= kInlineExpand) {
+    // past the fallback limit the block path drops expansions; so does this one
+    if (degree_of(p.g.out, x) <= kInlineExpand && !ld_cg(&p.c->fallback)) {
       ExpandChildren ec{&p, x, d};
       warp_row(p.g.out, x, ec);
       inlined = true;
@@ -2405,7 +2407,9 @@ static __device__ __align__(256) unsigned char vx_static_bfs_scratch[sizeof(vxh:
 
 namespace {
 constexpr int kStaticMaxDevices = 64;
-void* g_static_scratch_addr[kStaticMaxDevices];  // device address of the array, per device
+// device address of the array, per device; two host threads making their
+// first call on one device at once both look it up and store the same value
+std::atomic<void*> g_static_scratch_addr[kStaticMaxDevices];
 }  // namespace
 
 extern "C" int vx_bfs_csr_static(const uint64_t* d_out_offsets, const uint32_t* d_out_cols,
@@ -2428,17 +2432,17 @@ extern "C" int vx_bfs_csr_static(const uint64_t* d_out_offsets, const uint32_t* 
     vxh::set_error("vx_bfs_csr_static: device %d beyond the supported %d", dev, kStaticMaxDevices);
     return -2;
   }
-  if (!g_static_scratch_addr[dev]) {
+  void* addr = g_static_scratch_addr[dev].load(std::memory_order_acquire);
+  if (!addr) {
     // one-time set-up on this device (the device is current here)
-    void* ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&ptr, vx_static_bfs_scratch);
-    if (e != cudaSuccess || !ptr) {
+    const cudaError_t e = cudaGetSymbolAddress(&addr, vx_static_bfs_scratch);
+    if (e != cudaSuccess || !addr) {
       vxh::set_error("vx_bfs_csr_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
       return -3;
     }
-    g_static_scratch_addr[dev] = ptr;
+    g_static_scratch_addr[dev].store(addr, std::memory_order_release);
   }
-  StaticBfsScratch* sc = static_cast<StaticBfsScratch*>(g_static_scratch_addr[dev]);
+  StaticBfsScratch* sc = static_cast<StaticBfsScratch*>(addr);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // what must start at zero: counters, barrier words, the delta-row table
   VX_CUDA_TRY(cudaMemsetAsync(&sc->ctr, 0, sizeof(vxh::BfsCounters), s));

@@ -181,6 +181,35 @@ int vx_graph_in_neighbors(vx_graph* g, uint32_t v, uint32_t* out, size_t cap, si
   return vxh::graph_row(g->g, 1, v, out, cap, n);
 }
 
+int vx_graph_ensure_vertex(vx_graph* g, uint32_t v) {
+  if (!g) return fail(VX_ERR_INVALID, "null argument");
+  if ((size_t)v + 1 > vxb::kMaxVertices) return fail(VX_ERR_RANGE, "vertex id beyond the supported maximum (2^31 - 1)");
+  // grows the vertex count only; the version is unchanged (dynamic_graph.hpp:493-500)
+  return vxh::graph_grow(g->g, (size_t)v + 1);
+}
+
+int vx_graph_compact_neighbors(vx_graph* g, uint32_t u, uint32_t* out, size_t cap, size_t* n) {
+  if (!g || !n) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::graph_compact_row(g->g, 0, u, out, cap, n);
+}
+
+int vx_graph_compact_in_neighbors(vx_graph* g, uint32_t v, uint32_t* out, size_t cap, size_t* n) {
+  if (!g || !n) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::graph_compact_row(g->g, 1, v, out, cap, n);
+}
+
+int vx_graph_base_edge_count_directed(vx_graph* g, size_t* out) {
+  if (!g || !out) return fail(VX_ERR_INVALID, "null argument");
+  *out = (size_t)g->g->adj[0].A;
+  return VX_OK;
+}
+
+int vx_graph_storage_bytes(vx_graph* g, size_t* out) {
+  if (!g || !out) return fail(VX_ERR_INVALID, "null argument");
+  *out = vxh::graph_storage_bytes(g->g);
+  return VX_OK;
+}
+
 int vx_graph_has_edge(vx_graph* g, uint32_t u, uint32_t v, int* out) {
   if (!g || !out) return fail(VX_ERR_INVALID, "null argument");
   return vxh::graph_has_edge(g->g, u, v, out);

@@ -1061,6 +1061,38 @@ int graph_row(Graph* g, int dir, uint32_t u, uint32_t* host_out, size_t cap, siz
   return 0;
 }
 
+int graph_compact_row(Graph* g, int dir, uint32_t u, uint32_t* host_out, size_t cap, size_t* n) {
+  *n = 0;
+  Adjacency& a = dir == 0 ? g->adj[0] : g->in();
+  if (u >= g->V || u >= a.Vb) return 0;  // vertices added after the base build have empty base rows
+  cudaStream_t s = g->stream;
+  uint64_t* be = g->pinned_scalar;
+  VX_CUDA_TRY(cudaMemcpyAsync(be, a.off + u, 16, cudaMemcpyDeviceToHost, s));
+  VX_CUDA_TRY(cudaStreamSynchronize(s));
+  const size_t len = (size_t)(be[1] - be[0]);
+  if (host_out && cap && len) {
+    const size_t m = std::min(cap, len);
+    VX_CUDA_TRY(cudaMemcpyAsync(host_out, a.col + be[0], m * 4, cudaMemcpyDeviceToHost, s));
+    VX_CUDA_TRY(cudaStreamSynchronize(s));
+    // a tombstoned base arc is still part of the compact row (the overlay,
+    // not the base, records its deletion)
+    for (size_t i = 0; i < m; ++i) host_out[i] &= vxb::kIdMask;
+  }
+  *n = len;
+  return 0;
+}
+
+size_t graph_storage_bytes(const Graph* g) {
+  size_t bytes = sizeof(GraphCounters);
+  const int ndir = g->directed ? 2 : 1;
+  for (int d = 0; d < ndir; ++d) {
+    const Adjacency& a = g->adj[d];
+    bytes += a.off_cap * sizeof(uint64_t) + a.col_cap * sizeof(uint32_t) + a.arena_cap * sizeof(uint32_t);
+    bytes += g->Vcap * (sizeof(uint2) + 2 * sizeof(uint32_t)) + (g->Vcap + 31) / 32 * sizeof(uint32_t);
+  }
+  return bytes;
+}
+
 int graph_has_edge(Graph* g, uint32_t u, uint32_t v, int* out) {
   *out = 0;
   if (u >= g->V) return 0;

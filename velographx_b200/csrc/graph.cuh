@@ -126,6 +126,12 @@ int graph_maybe_compact(Graph* g, double threshold, int* compacted);
 int graph_sync_counters(Graph* g);  // copies counters to g->hctr (synchronises)
 int graph_row(Graph* g, int dir, uint32_t u, uint32_t* host_out, size_t cap, size_t* n);
 int graph_has_edge(Graph* g, uint32_t u, uint32_t v, int* out);
+// The compact row of u (compact_neighbors / compact_in_neighbors,
+// dynamic_graph.hpp:573-581): the base CSR row as of the last consolidation,
+// arcs deleted since then included; *n = its length.
+int graph_compact_row(Graph* g, int dir, uint32_t u, uint32_t* host_out, size_t cap, size_t* n);
+// Device bytes held by the graph's storage (storage_bytes, dynamic_graph.hpp:599-605).
+size_t graph_storage_bytes(const Graph* g);
 uint64_t graph_edge_count_directed(const Graph* g);  // needs synced counters
 
 }  // namespace vxh

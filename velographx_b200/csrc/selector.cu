@@ -373,7 +373,15 @@ static int upload(const void* host, size_t bytes, void** dev, cudaStream_t strea
     set_error("selector staging allocation failed");
     return -4;
   }
-  if (bytes && host) VX_CUDA_TRY(cudaMemcpyAsync(*dev, host, bytes, cudaMemcpyHostToDevice, stream));
+  if (bytes && host) {
+    const cudaError_t e = cudaMemcpyAsync(*dev, host, bytes, cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) {
+      set_error("selector staging copy failed: %s", cudaGetErrorString(e));
+      cudaFree(*dev);
+      *dev = nullptr;
+      return -3;
+    }
+  }
   return 0;
 }
 

@@ -153,6 +153,20 @@ PYBIND11_MODULE(_velographx, m) {
       .def_property_readonly("handle", [](DynamicGraph& g) { return reinterpret_cast<std::uintptr_t>(g.handle()); })
       .def("in_neighbors", &DynamicGraph::in_neighbors)
       .def("has_edge", &DynamicGraph::has_edge)
+      .def("ensure_vertex", &DynamicGraph::ensure_vertex)
+      .def("compact_neighbors",
+           [](const DynamicGraph& g, VertexId u) {
+             auto r = g.compact_neighbors(u);
+             return std::vector<VertexId>(r.begin(), r.end());
+           })
+      .def("compact_in_neighbors",
+           [](const DynamicGraph& g, VertexId v) {
+             auto r = g.compact_in_neighbors(v);
+             return std::vector<VertexId>(r.begin(), r.end());
+           })
+      .def("base_edge_count_directed", &DynamicGraph::base_edge_count_directed)
+      .def("storage_bytes", &DynamicGraph::storage_bytes)
+      .def("delta_ratio", &DynamicGraph::delta_ratio)
       .def("edge_count_directed", &DynamicGraph::edge_count_directed)
       .def("delta_edge_count", &DynamicGraph::delta_edge_count)
       .def("is_compact", &DynamicGraph::is_compact)

@@ -29,7 +29,7 @@ import time
 import numpy as np
 
 import workloads as w
-from velographx_b200 import Graph, IncrementalBFS
+from velographx_b200 import Graph, IncrementalBFS, MultiRootBFS
 
 
 def _events():
@@ -50,6 +50,20 @@ def pinned_stream(st: w.Stream) -> w.Stream:
     add = buf[8 * n: 9 * n]
     src[:], dst[:], add[:] = st.src, st.dst, st.add
     return w.Stream(src, dst, add, st.offsets)
+
+
+def record(g: Graph, b: IncrementalBFS) -> tuple:
+    """(digest, length, reachable, candidates, affected, full) of the current
+    post-batch state: what the CPU reference must reproduce after the batch."""
+    st = b.stats()
+    return (int(b.digest()), int(g.vertex_count), int(st["reachable_count"]), int(st["last_deletion_candidates"]),
+            int(st["last_affected_vertices"]), bool(st["last_used_full_recompute"]))
+
+
+def stream_records(digs, stats, V: int) -> list:
+    """The same records from apply_stream(digests=True, stats=True)."""
+    return [(int(digs[t]), V, int(stats[t, 3]), int(stats[t, 0]), int(stats[t, 1]), bool(stats[t, 2]))
+            for t in range(len(digs))]
 
 
 def run_stream(g: Graph, bfs: IncrementalBFS, root: int, stream: w.Stream, check_every: int) -> dict:
@@ -94,7 +108,10 @@ def run_stream(g: Graph, bfs: IncrementalBFS, root: int, stream: w.Stream, check
 
 
 def grid(side: int = 4096, long_range: float = 0.001, batches: int = 500, ops: int = 1000,
-         delete_fraction: float = 0.5, seed: int = 44, check_every: int = 50) -> dict:
+         delete_fraction: float = 0.5, seed: int = 44, check_every: int = 50, ref_batches: int = 20) -> dict:
+    """The lattice stream, device-resident batches timed per batch; then, on a
+    fresh replica, the records of the first ref_batches batches (returned
+    under "_check" for a comparison with the CPU reference)."""
     import torch
 
     edges = w.grid_edges(side, side, long_range, seed=seed)
@@ -118,6 +135,18 @@ def grid(side: int = 4096, long_range: float = 0.001, batches: int = 500, ops: i
                             f"{int(delete_fraction * 100)}pct-near-root-deletions",
                 "vertices": V, "arcs": int(g.edge_count_directed()), "full_bfs_ms": full_ms,
                 "full_bfs_levels": int(levels)})
+    del bfs, g
+    if ref_batches:
+        k = min(ref_batches, batches)
+        g = Graph(V, False)
+        g.bulk_load_edges(edges)
+        b = IncrementalBFS(g, root)
+        recs = []
+        for t in range(k):
+            b.apply_arrays(*stream.batch(t))
+            recs.append(record(g, b))
+        del b, g
+        res["_check"] = (edges, stream.prefix(k), root, recs)
     return res
 
 
@@ -151,7 +180,7 @@ def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int 
         cs = torch.cuda.ExternalStream(g.stream)
         torch.cuda.synchronize()
         e0.record(cs)
-        plain_digests = []
+        plain_digests, recs = [], []
         for t in range(batches):
             b.apply_arrays(*st.batch(t))
             b.stats()
@@ -173,16 +202,24 @@ def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int 
         batched_runs.append(batches / (e0.elapsed_time(e1) * 1e-3))
         same = same and [int(x) for x in digs] == [int(x) for x in plain_digests]
         del b, g, b2, g2
+    # the records of every batch, on one more replica (untimed)
+    g = Graph(V, False)
+    g.bulk_load_edges(edges)
+    b = IncrementalBFS(g, root)
+    for t in range(batches):
+        b.apply_arrays(*st.batch(t))
+        recs.append(record(g, b))
+    same = same and [r[0] for r in recs] == [int(x) for x in digs]
+    del b, g
     out["plain"] = {"batches_per_s": float(np.median(plain_runs)), "runs": [round(x) for x in plain_runs]}
     out["batched"] = {"batches_per_s": float(np.median(batched_runs)), "runs": [round(x) for x in batched_runs]}
-    out["digests"] = [int(x) for x in digs]
     out["plain_equals_batched"] = bool(same)
-    out["_stream"] = (edges, st, root)
+    out["_check"] = (edges, st, root, recs)
     return out
 
 
 def lognormal(scale: int = 20, batches: int = 1000, median: float = 500.0, sigma: float = 2.0,
-              insert_fraction: float = 0.8, seed: int = 33, check_batches: int = 200) -> dict:
+              insert_fraction: float = 0.8, seed: int = 33, check_batches: int = 200, multiroot: int = 256) -> dict:
     """Batched stream (one apply_stream call: upload, stream-wide
     canonicalisation, one persistent launch) against the plain path
     (apply_arrays + a counter read-back per batch) on replicas of one graph."""
@@ -265,13 +302,37 @@ def lognormal(scale: int = 20, batches: int = 1000, median: float = 500.0, sigma
         k = min(check_batches, batches)
         gc_, bc = replica()
         gd, bd = replica()
-        digs, _ = bc.apply_stream(st.src, st.dst, st.add, off[: k + 1], digests=True)
+        digs, stats = bc.apply_stream(st.src, st.dst, st.add, off[: k + 1], digests=True, stats=True)
+        recs = stream_records(digs, stats, V)
         bd.set_fused(False)  # checked against the per-phase path
         ok = True
         for t in range(k):
             bd.apply_arrays(*st.batch(t))
-            ok = ok and int(digs[t]) == bd.digest()
-        out["exact_every_batch"] = {"batches": k, "exact": bool(ok)}
+            ok = ok and record(gd, bd) == recs[t]
+        out["exact_every_batch"] = {"batches": k, "exact": bool(ok), "against": "per-phase plain path"}
+        out["_check"] = (edges, st.prefix(k), root, recs)
+        del bc, gc_, bd, gd
+    if multiroot:
+        # the configuration's 256 roots in one bit-parallel launch (median of three runs)
+        roots = w.non_isolated_roots(edges, V, multiroot, seed=seed + 3)
+        gm = Graph(V, False)
+        gm.bulk_load_edges(edges)
+        mr = MultiRootBFS(gm, roots)
+        mr.run()
+        cs = torch.cuda.ExternalStream(gm.stream)
+        runs = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            e0.record(cs)
+            mr.run()
+            e1.record(cs)
+            e1.synchronize()
+            runs.append(e0.elapsed_time(e1))
+        ms = float(np.median(runs))
+        out["multiroot"] = {"roots": int(roots.size), "ms": ms, "ms_runs": [round(x, 3) for x in runs],
+                            "gteps": mr.reached_arcs() / 2 / (ms * 1e-3) / 1e9, "levels": mr.levels}
+        out["_roots"] = roots
+        del mr, gm
     return out
 
 
