@@ -177,6 +177,11 @@ int vx_bfs_reserve_stream(vx_bfs* b, size_t ops, size_t batches, size_t max_batc
 /* Direction switch (alpha, beta) and grid-expanded row length of the full BFS.
  * No reference counterpart: the reference BFS is top-down only. */
 int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row);
+/* Thread blocks of the persistent update launch (fused single batch and
+ * batched stream): 0 (default) = every block that can be co-resident; fewer
+ * blocks shorten the grid barriers and the ring's termination for small
+ * batches.  Results are the same for every value.  No reference counterpart. */
+int vx_bfs_set_update_blocks(vx_bfs* b, uint32_t blocks);
 /* fused != 0 (default): an undirected batch's commit and repair run in one
  * persistent launch after staging; 0: the per-phase path (a launch per commit
  * step and for each half of the repair) -- the plain baseline the batched
@@ -216,7 +221,7 @@ int vx_multiroot_bfs(vx_graph* g, const uint32_t* roots, size_t k, uint32_t* out
  * (the kernel indexes d_dist and the scratch bitmaps by column id and does not
  * check it) and rows must be free of duplicates; a source at or beyond
  * `vertices` gives all-unreachable and *reachable = 0, as in the reference.  All other working
- * memory is one file-scope device array (~6.3 MB per GPU that loads the
+ * memory is one file-scope device array (~8.5 MB per GPU that loads the
  * library, held until exit), so at most 262,144 vertices (larger counts
  * return VX_ERR_RANGE).  Calls share that array: calls that overlap on the
  * GPU race, so issue them one at a time per device.  The first call on a

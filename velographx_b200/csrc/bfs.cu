@@ -54,6 +54,8 @@ struct Params {
   uint32_t* lst_a;
   uint32_t* lst_t;
   uint32_t* tent;
+  uint32_t* bul;      // bottom-up candidate lists A (bul[0, bul_half)) and B (bul[bul_half, 2 * bul_half))
+  uint32_t bul_half;
   unsigned long long* sw;  // support words of the pre-batch cascade (zero between batches)
   unsigned long long* ring;  // work ring of the repair phases (kSent between phases)
   uint32_t ring_mask;
@@ -279,40 +281,52 @@ __device__ void grid_rows(const DevAdj& a, const uint32_t* rows, uint32_t n, F& 
 
 constexpr uint32_t kBuHead = 8;  // arcs a lane scans itself before the warp helps
 
-// One warp per 32 unvisited-candidate vertices (a visited-bitmap word).  Each
-// lane scans the first kBuHead in-arcs of its row; the remainder of longer
-// rows is scanned by the whole warp 32 arcs at a time; every scan stops at the
-// first parent found in the frontier bitmap.
-__device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, uint32_t* fbn, uint32_t* qout,
-                         uint32_t* cnt_n, BlockQueue& bq) {
+// Bottom-up over a candidate list: lin[0, nin) holds the vertices that may
+// still be reached (unvisited when the list was made, in-degree > 0; the
+// first list is every such vertex, built by the full BFS's initialisation,
+// later ones the previous level's misses).  One warp per 32 entries: each
+// lane scans the first kBuHead in-arcs of its row, the rest of longer rows is
+// scanned by the whole warp 32 arcs at a time, every scan stops at the first
+// parent in the frontier bitmap.  Entries visited since the list was made are
+// skipped; entries that find no parent are appended to the next list (lout,
+// counter cnt_out whose value out_base corresponds to lout[0]), so isolated
+// vertices cost nothing and a later level scans only the remaining ones.
+// Entries are loaded two groups ahead and their visited words and row bounds
+// one group ahead, so those loads are in flight while a group is scanned.
+__device__ void bu_list_level(const Params& p, uint32_t level, const uint32_t* fbc, uint32_t* fbn, uint32_t* qout,
+                              uint32_t* cnt_n, BlockQueue& bq, const uint32_t* lin, uint32_t nin, uint32_t* lout,
+                              uint32_t* cnt_out, uint32_t out_base, BlockQueue& bqf) {
   const DevAdj& a = p.g.in;
   const int lane = threadIdx.x & 31;
-  const uint32_t words = (p.V + 31) >> 5;
-  // software pipeline over the warp's words: the next word's visited bits
-  // and row bounds are loaded while the current word is scanned
-  uint32_t w = gwarp();
-  uint32_t nvis = 0;
-  uint64_t nbv = 0, nev = 0;
-  uint2 ndr = make_uint2(0, 0);
-  auto fetch = [&](uint32_t ww) {
-    const uint32_t vv = ww * 32 + lane;
-    nvis = ww < words ? p.vis[ww] : FULL;
-    nbv = nev = 0;
-    ndr = make_uint2(0, 0);
-    if (ww < words && vv < p.V) {
-      vxb::base_range(a, vv, nbv, nev);
-      ndr = a.drow[vv];
+  const uint32_t step = nwarps() * 32;
+  uint32_t base = gwarp() * 32;
+  uint32_t v1 = base + step + lane < nin ? lin[base + step + lane] : kUnreachable;
+  uint32_t v0 = base + lane < nin ? lin[base + lane] : kUnreachable;
+  uint32_t vis0 = 0;
+  uint64_t b0 = 0, e0 = 0;
+  uint2 dr0 = make_uint2(0, 0);
+  if (v0 != kUnreachable) {
+    vis0 = p.vis[v0 >> 5];
+    vxb::base_range(a, v0, b0, e0);
+    dr0 = a.drow[v0];
+  }
+  for (; base < nin; base += step) {
+    const uint32_t v = v0, visw = vis0;
+    uint64_t b = b0, e = e0;
+    uint2 dr = dr0;
+    // advance the pipeline: row bounds of the next group, entries of the one after
+    v0 = v1;
+    vis0 = 0;
+    b0 = e0 = 0;
+    dr0 = make_uint2(0, 0);
+    if (v0 != kUnreachable) {
+      vis0 = p.vis[v0 >> 5];
+      vxb::base_range(a, v0, b0, e0);
+      dr0 = a.drow[v0];
     }
-  };
-  fetch(w);
-  for (; w < words; w += nwarps()) {
-    const uint32_t v = w * 32 + lane;
-    const uint32_t visw = nvis;
-    uint64_t b = nbv, e = nev;
-    uint2 dr = ndr;
-    fetch(w + nwarps());
-    if (visw == FULL) continue;
-    const bool todo = !((visw >> lane) & 1u);
+    const uint32_t i2 = base + 2 * step + lane;
+    v1 = i2 < nin ? lin[i2] : kUnreachable;
+    const bool todo = v != kUnreachable && !((visw >> (v & 31)) & 1u);
     if (!todo) {
       b = e = 0;
       dr = make_uint2(0, 0);
@@ -356,29 +370,56 @@ __device__ void bu_level(const Params& p, uint32_t level, const uint32_t* fbc, u
       }
       if (lane == l) found = hit_l;
     }
-    const uint32_t newly = __ballot_sync(FULL, found);
     if (found) p.dist[v] = level + 1;
-    if (lane == 0 && newly) {
-      p.vis[w] = visw | newly;
-      fbn[w] = newly;
+    // visited and next-frontier bits: OR-combined over runs of lanes on the
+    // same bitmap word (list entries come in ascending runs), one atomic per
+    // run; a word that recurs outside its run is ORed again, which is harmless
+    const uint32_t word = v >> 5;
+    uint32_t bits = found ? 1u << (v & 31) : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, bits, o);
+      const uint32_t wy = __shfl_up_sync(FULL, word, o);
+      if (lane >= o && wy == word) bits |= y;
+    }
+    const uint32_t wnext = __shfl_down_sync(FULL, word, 1);
+    if (bits && (lane == 31 || wnext != word)) {
+      atomicOr(&p.vis[word], bits);
+      atomicOr(&fbn[word], bits);
     }
     bq_push(bq, found, v, cnt_n, qout);
+    bq_push(bqf, todo && !found, v, cnt_out, lout, out_base);
   }
   bq_flush(bq, cnt_n, qout);
+  bq_flush(bqf, cnt_out, lout, out_base);
 }
 
 // ------------------------------------------------------------ full BFS --
 
-__device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
+// Precondition: c->bun[0] == c->bun[1] == 0 (set by the host before a
+// recompute launch, by repair_post before its fallback, by the allocation-free
+// entry's counter reset, and by the end of every full BFS).
+__device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst, BlockQueue& bqf) {
   BfsCounters* c = p.c;
-  if (threadIdx.x == 0) bq.cnt = 0;
+  if (threadIdx.x == 0) bq.cnt = bqf.cnt = 0;
   const uint32_t V = p.V;
   const uint32_t words = (V + 31) >> 5;
   // one pass sets every vertex unreached and the source at level 0 (bits
-  // past V count as visited, so bottom-up never scans them)
+  // past V count as visited, so bottom-up never scans them), and lists the
+  // bottom-up candidates: every vertex but the source with a nonempty in-row
+  // (isolated vertices never enter a bottom-up level)
   const uint32_t s = p.source;
   const bool has_source = s < V;
-  for (uint32_t i = gtid(); i < V; i += nthreads()) p.dist[i] = i == s ? 0u : kUnreachable;
+  for (uint32_t i0 = gwarp() * 32; i0 < V; i0 += nwarps() * 32) {
+    const uint32_t i = i0 + (threadIdx.x & 31);
+    bool cand = false;
+    if (i < V) {
+      p.dist[i] = i == s ? 0u : kUnreachable;
+      cand = has_source && i != s && degree_of(p.g.in, i) != 0u;
+    }
+    bq_push(bqf, cand, i, &c->bun[0], p.bul);
+  }
+  bq_flush(bqf, &c->bun[0], p.bul);
   for (uint32_t i = gtid(); i < words; i += nthreads()) {
     const uint32_t lo = i * 32;
     const uint32_t sbit = has_source && i == (s >> 5) ? 1u << (s & 31) : 0u;
@@ -412,6 +453,10 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
   // barrier that ends the level before it
   uint32_t n_f = ld_cg(&c->lvl_n[0]);
   unsigned long long m_f = __ldcg(&c->lvl_m[0]);
+  // bottom-up candidate lists: list k holds entries [lbase[k], ld(bun[k])) of
+  // its counter's range (counters are never reset during the BFS, so every
+  // block derives the same bases); the first bottom-up level reads list 0
+  uint32_t lin = 0, lbase[2] = {0u, 0u};  // the counters read 0 at entry (precondition)
   for (;; ++level) {
     if (level > V + 1) {
       if (gtid() == 0) atomicOr(&c->err, vxb::kErrLoopBound);
@@ -445,7 +490,14 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
       for (uint32_t i = gtid(); i < words; i += nthreads()) p.fb[clr][i] = 0u;
     }
     if (bottom_up) {
-      bu_level(p, level, p.fb[cur], p.fb[nxt], p.q[nxt], &c->lvl_n[nxt], bq);
+      const uint32_t lout = lin ^ 1u;
+      // list lout was last emptied when it was consumed, so its counter still
+      // reads lbase[lout]; at most nin entries are appended to it
+      const uint32_t nin = min(ld_cg(&c->bun[lin]) - lbase[lin], p.bul_half);
+      bu_list_level(p, level, p.fb[cur], p.fb[nxt], p.q[nxt], &c->lvl_n[nxt], bq, p.bul + lin * p.bul_half, nin,
+                    p.bul + lout * p.bul_half, &c->bun[lout], lbase[lout], bqf);
+      lbase[lin] += nin;  // consumed: its next contents start at the counter's current value
+      lin = lout;
       if (!sync_grid(p)) return;
       prev_n = n_f;
       n_f = ld_cg(&c->lvl_n[nxt]);
@@ -476,6 +528,9 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
     c->reachable = reached;
     c->levels = level;
     c->arcs = m_visited;
+    // every append of this BFS came before the barrier that ended its last
+    // level: the list counters are free again for the next one
+    c->bun[0] = c->bun[1] = 0u;
     if (p.trace && level < kTraceLevels) {
       p.trace[2 * level] = globaltimer();
       p.trace[2 * level + 1] = 0;
@@ -635,6 +690,15 @@ struct RepairSmem {
   uint32_t cnt[kThreads];    // chunk + 1 of a chunk-check sv item (0: plain check); boundary minima
   uint32_t d[kThreads];      // distance of each staged item
   uint32_t g0, n, stop, nsv, nex, fallback;
+};
+
+// The repair phases' shared memory and the full BFS's candidate-list queue
+// share one allocation: a full BFS (recompute, or the fallback of the
+// post-batch repair) runs while no repair phase is active, and every repair
+// phase sets the fields it reads before reading them.
+union RepairUnion {
+  RepairSmem sm;
+  BlockQueue bqf;
 };
 
 // Drains the ring; W::process(sm, n) handles sm.items[0, n) block-uniformly.
@@ -1288,13 +1352,14 @@ __device__ void grid_boundary_min(const Params& p, uint32_t nb) {
   }
 }
 
-__device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQueue& bq) {
+__device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQueue& bq, BlockQueue& bqf) {
   BfsCounters* c = p.c;
   const int lane = threadIdx.x & 31;
   if (ld_cg(&c->fallback)) {
+    if (gtid() == 0) c->bun[0] = c->bun[1] = 0u;  // the full BFS's precondition (after the barrier below)
     clear_workspace(p);
     if (!sync_grid(p)) return;
-    full_bfs(p, bq, lb);
+    full_bfs(p, bq, lb, bqf);
     if (gtid() == 0) c->full = 1;
     return;
   }
@@ -1610,7 +1675,8 @@ __device__ void commit_runs(const Params& p, const StreamArgs& s, uint32_t off, 
   }
 }
 
-__device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm, LbStage& lb, BlockQueue& bq) {
+__device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm, LbStage& lb, BlockQueue& bq,
+                                   BlockQueue& bqf) {
   BfsCounters* c = p.c;
   const int lane = threadIdx.x & 31;
   unsigned long long tmark = globaltimer();
@@ -1701,7 +1767,7 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
     // E: the post-batch repair (or the fallback full BFS) on the new graph
     q.V = Vpost;
     q.dist_len = Vpost;
-    repair_post(q, sm, lb, bq);
+    repair_post(q, sm, lb, bq, bqf);
     if (ld_cg(&c->err)) return;
     phase(4);
     // every block's counter updates are in before they are recorded, and
@@ -1721,17 +1787,17 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
 __global__ void __launch_bounds__(kThreads, 3) bfs_kernel(Params p, int mode) {
   __shared__ BlockQueue bq;
   __shared__ LbStage lb;
-  __shared__ RepairSmem sm;
-  if (mode == kModeFull) full_bfs(p, bq, lb);
-  else if (mode == kModePre) repair_pre(p, sm, lb);
-  else repair_post(p, sm, lb, bq);
+  __shared__ RepairUnion ru;
+  if (mode == kModeFull) full_bfs(p, bq, lb, ru.bqf);
+  else if (mode == kModePre) repair_pre(p, ru.sm, lb);
+  else repair_post(p, ru.sm, lb, bq, ru.bqf);
 }
 
 __global__ void __launch_bounds__(kThreads, 2) bfs_stream_kernel(Params p, StreamArgs s) {
   __shared__ BlockQueue bq;
   __shared__ LbStage lb;
-  __shared__ RepairSmem sm;
-  stream_kernel_body(p, s, sm, lb, bq);
+  __shared__ RepairUnion ru;
+  stream_kernel_body(p, s, ru.sm, lb, bq, ru.bqf);
 }
 
 // Stream canonicalisation: both arcs of every non-self-loop op keyed by
@@ -1869,6 +1935,7 @@ static int ensure_capacity(Bfs* b, size_t V) {
   rc |= realloc_copy(&b->lst_a, c, 0, 0);
   rc |= realloc_copy(&b->lst_t, c, 0, 0);
   rc |= realloc_copy(&b->tent, c, 0, 0);
+  rc |= realloc_copy(&b->bul, 2 * c, 0, 0);
   const cudaError_t e = cudaStreamSynchronize(s);
   for (uint32_t* p : old) cudaFree(p);
   if (rc) return -4;
@@ -1921,6 +1988,8 @@ static Params make_params(Bfs* b, uint32_t V, uint32_t dist_len) {
   p.lst_a = b->lst_a;
   p.lst_t = b->lst_t;
   p.tent = b->tent;
+  p.bul = b->bul;
+  p.bul_half = (uint32_t)b->cap;
   p.sw = reinterpret_cast<unsigned long long*>(b->sw);
   p.ring = b->ring;
   p.ring_mask = b->ring_slots ? (uint32_t)(b->ring_slots - 1) : 0u;
@@ -1995,7 +2064,7 @@ void bfs_destroy(Bfs* b) {
   if (!b) return;
   if (b->g && b->g->stream) cudaStreamSynchronize(b->g->stream);
   uint32_t* ptrs[] = {b->dist, b->vis, b->fb[0], b->fb[1], b->fb[2], b->q[0], b->q[1], b->q[2], b->big,
-                      b->lst_a, b->lst_t, b->tent, b->sw, b->aff, b->inq[0], b->inq[1]};
+                      b->lst_a, b->lst_t, b->tent, b->bul, b->sw, b->aff, b->inq[0], b->inq[1]};
   for (uint32_t* p : ptrs) cudaFree(p);
   cudaFree(b->ctr);
   cudaFree(b->trace);
@@ -2013,7 +2082,8 @@ int bfs_recompute(Bfs* b) {
   const size_t V = g->V;
   if (int rc = ensure_capacity(b, std::max<size_t>(V, 1))) return rc;
   b->dist_len = V;
-  VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->candidates, 0, 4 * sizeof(uint32_t), g->stream));
+  // last_* counters, and the full BFS's candidate-list counters (bun)
+  VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->candidates, 0, 6 * sizeof(uint32_t), g->stream));
   if (V == 0) {
     VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->reachable, 0, 8, g->stream));
     return 0;
@@ -2051,10 +2121,11 @@ static int launch_stream(Bfs* b, Params& p, StreamArgs& sa) {
     }
     b->stream_grid = per_sm * sm_count();
   }
-  p.nblocks = (uint32_t)b->stream_grid;
+  const uint32_t want = b->tune.update_blocks;
+  p.nblocks = want && want < (uint32_t)b->stream_grid ? want : (uint32_t)b->stream_grid;
   void* args[] = {&p, &sa};
   count_launch();
-  VX_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)bfs_stream_kernel, dim3(b->stream_grid), dim3(kThreads), args,
+  VX_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)bfs_stream_kernel, dim3(p.nblocks), dim3(kThreads), args,
                                           0, b->g->stream));
   return 0;
 }
@@ -2378,7 +2449,7 @@ int bfs_digest(Bfs* b, uint64_t* out) {
 // device array.  It allocates nothing.
 //
 // Limits and sharing: at most kStaticMaxVertices vertices; every GPU that
-// loads this library holds the array (about 6.3 MB) until the process exits;
+// loads this library holds the array (about 8.5 MB) until the process exits;
 // all calls share it and it keeps the last call's contents, so calls that
 // overlap on the GPU (different streams, different threads) race -- issue
 // them one at a time per device.  The first call on a device looks up the
@@ -2395,6 +2466,7 @@ struct StaticBfsScratch {
   uint32_t fb[3][kStaticWords];
   uint32_t q[3][kStaticMaxVertices];
   uint32_t big[kStaticMaxVertices];
+  uint32_t bul[2 * kStaticMaxVertices];  // the bottom-up candidate lists
   uint2 drow[kStaticMaxVertices];  // kept all-zero: a plain CSR has no delta rows
   BfsCounters ctr;
   uint32_t bar[vxb::kBarrierWords];
@@ -2473,6 +2545,8 @@ extern "C" int vx_bfs_csr_static(const uint64_t* d_out_offsets, const uint32_t* 
     p.q[k] = sc->q[k];
   }
   p.big = sc->big;
+  p.bul = sc->bul;
+  p.bul_half = vxh::kStaticMaxVertices;
   p.c = &sc->ctr;
   p.total_arcs = arcs;
   p.alpha = 14.0f;

@@ -17,6 +17,7 @@ struct BfsCounters {
   uint32_t affected;              // last_affected_vertices
   uint32_t full;                  // last_used_full_recompute
   uint32_t fallback;              // fixpoint exceeded the fallback limit
+  uint32_t bun[2];                // bottom-up candidate lists: entries appended in this BFS (zero at its start)
   uint32_t err;
   // per-level counters of the persistent loops (3-way rotation)
   uint32_t lvl_n[3];
@@ -46,6 +47,7 @@ struct BfsTuning {
   float beta = 24.0f;        // bottom-up -> top-down when n_f * beta < V (shrinking)
   uint32_t large_row = 1024; // rows this long are expanded by the whole grid
   bool fused = true;         // undirected batches: one persistent launch after staging
+  uint32_t update_blocks = 0;  // blocks of the update launch (0: every co-resident block)
 };
 
 // Device buffers of the batched stream path (kept between calls).
@@ -80,6 +82,7 @@ struct Bfs {
   uint32_t* lst_a = nullptr;  // affected list
   uint32_t* lst_t = nullptr;  // touched (lost > 0) list
   uint32_t* tent = nullptr;   // boundary seed distance of each affected entry
+  uint32_t* bul = nullptr;    // two bottom-up candidate lists of cap entries each (full BFS)
   uint32_t* sw = nullptr;     // 64-bit support words, as pairs of u32 (zero between batches)
   unsigned long long* ring = nullptr;  // work ring of the repair phases (ring_slots, a power of two)
   size_t ring_slots = 0;

@@ -408,6 +408,12 @@ int vx_bfs_level_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n) {
   return vxh::bfs_level_trace(b->b, reinterpret_cast<unsigned long long*>(out), cap, n);
 }
 
+int vx_bfs_set_update_blocks(vx_bfs* b, uint32_t blocks) {
+  if (!b) return fail(VX_ERR_INVALID, "null argument");
+  b->b->tune.update_blocks = blocks;
+  return VX_OK;
+}
+
 int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row) {
   if (!b || !(alpha > 0.f) || !(beta > 0.f) || large_row < 32) return fail(VX_ERR_INVALID, "invalid tuning");
   b->b->tune.alpha = alpha;

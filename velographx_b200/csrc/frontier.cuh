@@ -140,7 +140,10 @@ struct BlockQueue {
   uint32_t items[kBlockQueueCap];
 };
 
-__device__ __forceinline__ void bq_push(BlockQueue& bq, bool pred, uint32_t v, uint32_t* gcnt, uint32_t* gq) {
+// gbase0: the global counter's value that corresponds to gq[0] (a counter
+// that is not reset between uses, as the bottom-up candidate lists use).
+__device__ __forceinline__ void bq_push(BlockQueue& bq, bool pred, uint32_t v, uint32_t* gcnt, uint32_t* gq,
+                                        uint32_t gbase0 = 0u) {
   const uint32_t mask = __ballot_sync(FULL, pred);
   if (!mask) return;
   const int lane = threadIdx.x & 31;
@@ -157,17 +160,17 @@ __device__ __forceinline__ void bq_push(BlockQueue& bq, bool pred, uint32_t v, u
   if (pred) {
     const uint32_t slot = base + r;
     if (slot < kBlockQueueCap) bq.items[slot] = v;
-    else gq[gb + (slot - max(base, kBlockQueueCap))] = v;
+    else gq[(gb - gbase0) + (slot - max(base, kBlockQueueCap))] = v;
   }
 }
 
 // Block-uniform: moves the buffered entries to the global queue.
-__device__ __forceinline__ void bq_flush(BlockQueue& bq, uint32_t* gcnt, uint32_t* gq) {
+__device__ __forceinline__ void bq_flush(BlockQueue& bq, uint32_t* gcnt, uint32_t* gq, uint32_t gbase0 = 0u) {
   __syncthreads();
   const uint32_t n = min(bq.cnt, kBlockQueueCap);
   if (threadIdx.x == 0) bq.gbase = n ? atomicAdd(gcnt, n) : 0u;
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) gq[bq.gbase + i] = bq.items[i];
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) gq[(bq.gbase - gbase0) + i] = bq.items[i];
   __syncthreads();
   if (threadIdx.x == 0) bq.cnt = 0;
   __syncthreads();

@@ -304,6 +304,8 @@ PYBIND11_MODULE(_velographx, m) {
            },
            py::arg("ops"), py::arg("batches"), py::arg("max_batch_ops"))
       .def("set_fused", [](IncrementalBFS& x, bool fused) { detail::check(vx_bfs_set_fused(x.handle(), fused)); })
+      .def("set_update_blocks",
+           [](IncrementalBFS& x, std::uint32_t blocks) { detail::check(vx_bfs_set_update_blocks(x.handle(), blocks)); })
       .def("digest",
            [](IncrementalBFS& x) {
              std::uint64_t d = 0;
