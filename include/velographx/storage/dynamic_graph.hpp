@@ -40,6 +40,8 @@ namespace detail {
   vx_last_error(msg, sizeof msg);
   if (rc == VX_ERR_INVALID) throw std::invalid_argument(msg);
   if (rc == VX_ERR_RANGE) throw std::out_of_range(msg);
+  if (rc == VX_ERR_OVERFLOW) throw std::overflow_error(msg);
+  if (rc == VX_ERR_FORMAT || rc == VX_ERR_IO) throw std::runtime_error(msg);
   throw std::runtime_error(std::string("vx_b200: ") + msg);
 }
 
@@ -71,6 +73,9 @@ class DynamicGraph {
   explicit DynamicGraph(std::size_t vertices = 0, bool directed = false) {
     detail::check(vx_graph_create(vertices, directed ? 1 : 0, &g_));
   }
+  // Takes ownership of a graph the C ABI created (the file loaders).  No
+  // reference counterpart.
+  static DynamicGraph adopt(vx_graph* g) { return DynamicGraph(g, 0); }
   ~DynamicGraph() { vx_graph_destroy(g_); }
   DynamicGraph(const DynamicGraph&) = delete;
   DynamicGraph& operator=(const DynamicGraph&) = delete;
@@ -224,6 +229,8 @@ class DynamicGraph {
     detail::check(vx_graph_dirty_rows(g_, &o, &i));
     return {o, i};
   }
+
+  DynamicGraph(vx_graph* g, int) : g_(g) {}
 
   vx_graph* g_ = nullptr;
   mutable std::vector<VertexId> compact_out_buf_, compact_in_buf_;

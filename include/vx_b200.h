@@ -36,6 +36,9 @@ extern "C" {
 #define VX_ERR_NOMEM (-4)   /* device allocation failed                     */
 #define VX_ERR_DEVICE (-5)  /* a kernel reported an error word (bounded wait
                                expired, loop bound, bad id, arena overflow)  */
+#define VX_ERR_FORMAT (-6)  /* malformed input file   (std::runtime_error)   */
+#define VX_ERR_OVERFLOW (-7) /* id beyond uint32 in a file (std::overflow_error) */
+#define VX_ERR_IO (-8)      /* cannot open, read or write a file (std::runtime_error) */
 
 #define VX_UNREACHABLE 0xFFFFFFFFu
 
@@ -108,6 +111,29 @@ int vx_graph_dirty_rows(vx_graph* g, size_t* out_rows, size_t* in_rows);
  * reaches the reference's density rule and returns 1 in *compacted. */
 int vx_graph_compact(vx_graph* g);
 int vx_graph_maybe_compact(vx_graph* g, double threshold, int* compacted);
+/* ---- On-disk formats --------------------------------------------------
+ * load_edge_list(path, directed) (include/velographx/io.hpp:6, src/io.cpp:23-53):
+ * a text edge list, one "u v" per line, blank lines and lines starting with '#'
+ * or '%' (after leading whitespace) skipped; parsed on the device.  The result
+ * is a new graph with the file's edges bulk-loaded (self-loops and duplicates
+ * dropped, vertex count max id + 1), the logical graph of the reference's
+ * CsrGraph.  Errors name the first bad line as the reference does:
+ * "malformed edge list at line N" and "unexpected trailing data at line N"
+ * (VX_ERR_FORMAT), "vertex id exceeds uint32 range at line N"
+ * (VX_ERR_OVERFLOW), "unable to open edge-list file" (VX_ERR_IO). */
+int vx_graph_load_edge_list(const char* path, int directed, vx_graph** out);
+/* io::save_binary(g, path) (include/velographx/io/binary_graph.hpp:9-14): the
+ * reference's format -- u64 magic 0x564758303031, u64 vertex count, u64
+ * edge_count_directed, then (u32 u, u32 v) for every arc, rows in vertex
+ * order, each ascending.  The graph is not modified. */
+int vx_graph_save_binary(vx_graph* g, const char* path);
+/* io::load_binary(path, directed) (binary_graph.hpp:15-20): a new graph with
+ * the file's vertex count and, for an undirected graph, the pairs with u <= v;
+ * version 1 when any pair was kept, else 0.  Errors: "cannot open input"
+ * (VX_ERR_IO), "invalid VeloGraphX binary graph", "truncated graph file"
+ * (VX_ERR_FORMAT). */
+int vx_graph_load_binary(const char* path, int directed, vx_graph** out);
+
 /* The graph's CUDA stream (cudaStream_t) and a host-side wait for it. */
 int vx_graph_stream(vx_graph* g, void** stream);
 int vx_graph_synchronize(vx_graph* g);

@@ -8,10 +8,13 @@
 // the golden fixtures under tests/golden/, and is the "reference" CPU baseline
 // timed by bench.py.  Nothing in the product loads it.
 //
-// The function set mirrors vx_oracle.h with a vxr_ prefix.
+// The function set mirrors vx_oracle.h with a vxr_ prefix, plus the binary
+// graph format (include/velographx/io/binary_graph.hpp).
 #include <atomic>
 #include <cstdint>
 #include <cstring>
+#include <stdexcept>
+#include <string>
 #include <thread>
 #include <utility>
 #include <vector>
@@ -19,6 +22,7 @@
 #include "velographx/algorithms.hpp"
 #include "velographx/csr_graph.hpp"
 #include "velographx/incremental/bfs.hpp"
+#include "velographx/io/binary_graph.hpp"
 #include "velographx/storage/dynamic_graph.hpp"
 
 using velographx::DynamicGraph;
@@ -169,6 +173,35 @@ int vxr_csr_multi_bfs(void* c, const uint32_t* roots, size_t k, int threads,
   for (int t = 0; t < (threads > 0 ? threads : 1); ++t) pool.emplace_back(worker);
   for (auto& t : pool) t.join();
   return failed.load() ? -1 : 0;
+}
+
+
+// ---- binary graph format ----------------------------------------------------
+// Errors: the exception's message in err (cap bytes), return -1 / null.
+static void put_error(const std::exception& e, char* err, size_t cap) {
+  if (err && cap) {
+    std::strncpy(err, e.what(), cap - 1);
+    err[cap - 1] = 0;
+  }
+}
+
+int vxr_save_binary(void* g, const char* path, char* err, size_t cap) {
+  try {
+    velographx::io::save_binary(*static_cast<DynamicGraph*>(g), path);
+    return 0;
+  } catch (const std::exception& e) {
+    put_error(e, err, cap);
+  }
+  return -1;
+}
+
+void* vxr_load_binary(const char* path, int directed, char* err, size_t cap) {
+  try {
+    return new DynamicGraph(velographx::io::load_binary(path, directed != 0));
+  } catch (const std::exception& e) {
+    put_error(e, err, cap);
+  }
+  return nullptr;
 }
 
 }  // extern "C"

@@ -27,6 +27,9 @@ try:
         from_scipy_csr,
         last_error,
         launch_count,
+        load_binary,
+        load_edge_list,
+        save_binary,
     )
 except ImportError as exc:  # pragma: no cover - exercised only on a broken install
     raise ImportError(
@@ -54,6 +57,9 @@ __all__ = [
     "from_scipy_csr",
     "from_arrow_columns",
     "from_arrow_table",
+    "load_edge_list",
+    "save_binary",
+    "load_binary",
     "capi",
     "LIB_PATH",
 ]

@@ -9,6 +9,7 @@
 #include "../../include/vx_b200.h"
 #include "bfs.cuh"
 #include "graph.cuh"
+#include "io.cuh"
 #include "mrbfs.cuh"
 #include "selector.cuh"
 
@@ -179,6 +180,27 @@ int vx_graph_neighbors(vx_graph* g, uint32_t u, uint32_t* out, size_t cap, size_
 int vx_graph_in_neighbors(vx_graph* g, uint32_t v, uint32_t* out, size_t cap, size_t* n) {
   if (!g || !n) return fail(VX_ERR_INVALID, "null argument");
   return vxh::graph_row(g->g, 1, v, out, cap, n);
+}
+
+int vx_graph_load_edge_list(const char* path, int directed, vx_graph** out) {
+  if (!path || !out) return fail(VX_ERR_INVALID, "null argument");
+  vxh::Graph* g = nullptr;
+  if (int rc = vxh::graph_load_edge_list(path, directed != 0, &g)) return rc;
+  *out = new vx_graph{g};
+  return VX_OK;
+}
+
+int vx_graph_save_binary(vx_graph* g, const char* path) {
+  if (!g || !path) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::graph_save_binary(g->g, path);
+}
+
+int vx_graph_load_binary(const char* path, int directed, vx_graph** out) {
+  if (!path || !out) return fail(VX_ERR_INVALID, "null argument");
+  vxh::Graph* g = nullptr;
+  if (int rc = vxh::graph_load_binary(path, directed != 0, &g)) return rc;
+  *out = new vx_graph{g};
+  return VX_OK;
 }
 
 int vx_graph_ensure_vertex(vx_graph* g, uint32_t v) {

@@ -368,6 +368,37 @@ PYBIND11_MODULE(_velographx, m) {
         return l;
       });
 
+  // files (include/velographx/io.hpp:6, include/velographx/io/binary_graph.hpp:9-20);
+  // load_edge_list returns the static graph as a (compact) Graph
+  m.def(
+      "load_edge_list",
+      [](const std::string& path, bool directed) {
+        vx_graph* g = nullptr;
+        {
+          py::gil_scoped_release release;
+          detail::check(vx_graph_load_edge_list(path.c_str(), directed ? 1 : 0, &g));
+        }
+        return DynamicGraph::adopt(g);
+      },
+      py::arg("path"), py::arg("directed") = false);
+  m.def(
+      "save_binary",
+      [](const DynamicGraph& g, const std::string& path) {
+        py::gil_scoped_release release;
+        detail::check(vx_graph_save_binary(g.handle(), path.c_str()));
+      },
+      py::arg("graph"), py::arg("path"));
+  m.def(
+      "load_binary",
+      [](const std::string& path, bool directed) {
+        vx_graph* g = nullptr;
+        {
+          py::gil_scoped_release release;
+          detail::check(vx_graph_load_binary(path.c_str(), directed ? 1 : 0, &g));
+        }
+        return DynamicGraph::adopt(g);
+      },
+      py::arg("path"), py::arg("directed") = false);
   m.def("from_numpy_edges", &graph_from_numpy_edges, py::arg("edges"), py::arg("directed") = false);
   m.def("from_scipy_csr", &graph_from_scipy_csr, py::arg("csr"), py::arg("directed") = false);
   m.def("from_arrow_columns", &graph_from_arrow_columns, py::arg("src"), py::arg("dst"), py::arg("directed") = false);
