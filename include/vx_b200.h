@@ -215,6 +215,26 @@ int vx_bfs_set_update_blocks(vx_bfs* b, uint32_t blocks);
  * counterpart. */
 int vx_bfs_set_fused(vx_bfs* b, int fused);
 
+/* ---- BasicIncrementalComponents<DynamicGraph>
+ *      (include/velographx/incremental/connected_components.hpp) ----------
+ * Connected components of an undirected graph, maintained on the device.  The
+ * partition after every batch equals the reference's; each component is
+ * labelled by its smallest vertex id (the reference's labels are union-find
+ * roots, which depend on its union order; its API compares them only for
+ * equality). */
+typedef struct vx_cc vx_cc;
+/* BasicIncrementalComponents(Graph&) :19-25 -- VX_ERR_INVALID for a directed
+ * graph; labels every vertex (last_repaired_vertices = vertex count). */
+int vx_cc_create(vx_graph* g, vx_cc** out);
+int vx_cc_destroy(vx_cc* c);
+/* apply(const UpdateBatch&) :35-91 -- also applies the batch to the graph. */
+int vx_cc_apply(vx_cc* c, const uint32_t* src, const uint32_t* dst, const uint8_t* add, size_t n);
+/* component(v) :27-30 for every v: copies min(cap, len) labels, *n = len (the
+ * vertex count when the labels were last updated). */
+int vx_cc_labels(vx_cc* c, uint32_t* out, size_t cap, size_t* n);
+/* last_repaired_vertices() :31-33 */
+int vx_cc_last_repaired_vertices(vx_cc* c, uint64_t* out);
+
 /* ---- Multi-root BFS (up to 256 roots, one launch) ----------------------
  * For every root r, row r of the result equals BasicIncrementalBFS(g,
  * roots[r]).distances() (bfs.hpp:100-120); the reference's multicore harness

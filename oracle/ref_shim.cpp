@@ -9,7 +9,9 @@
 // timed by bench.py.  Nothing in the product loads it.
 //
 // The function set mirrors vx_oracle.h with a vxr_ prefix, plus the binary
-// graph format (include/velographx/io/binary_graph.hpp).
+// graph format (include/velographx/io/binary_graph.hpp) and the maintained
+// connected components and unit-weight SSSP on the same graph
+// (include/velographx/incremental/connected_components.hpp, sssp.hpp).
 #include <atomic>
 #include <cstdint>
 #include <cstring>
@@ -22,6 +24,8 @@
 #include "velographx/algorithms.hpp"
 #include "velographx/csr_graph.hpp"
 #include "velographx/incremental/bfs.hpp"
+#include "velographx/incremental/connected_components.hpp"
+#include "velographx/incremental/sssp.hpp"
 #include "velographx/io/binary_graph.hpp"
 #include "velographx/storage/dynamic_graph.hpp"
 
@@ -202,6 +206,54 @@ void* vxr_load_binary(const char* path, int directed, char* err, size_t cap) {
     put_error(e, err, cap);
   }
   return nullptr;
+}
+
+
+// ---- IncrementalComponents / IncrementalSSSP ---------------------------------
+void* vxr_cc_create(void* g) {
+  try {
+    return new velographx::IncrementalComponents(*static_cast<DynamicGraph*>(g));
+  } catch (const std::exception&) {
+    return nullptr;
+  }
+}
+void vxr_cc_destroy(void* c) { delete static_cast<velographx::IncrementalComponents*>(c); }
+int vxr_cc_apply(void* c, const uint32_t* src, const uint32_t* dst, const uint8_t* add, size_t n) {
+  static_cast<velographx::IncrementalComponents*>(c)->apply(make_batch(src, dst, add, n));
+  return 0;
+}
+// labels of v in [0, n): writes component(v), or UINT32_MAX where component()
+// throws out_of_range; returns the first v that throws (the labels' size)
+size_t vxr_cc_labels(void* c, uint32_t* out, size_t n) {
+  auto* cc = static_cast<velographx::IncrementalComponents*>(c);
+  size_t covered = n;
+  for (size_t v = 0; v < n; ++v) {
+    try {
+      out[v] = cc->component(static_cast<VertexId>(v));
+    } catch (const std::out_of_range&) {
+      out[v] = 0xFFFFFFFFu;
+      if (covered == n) covered = v;
+    }
+  }
+  return covered;
+}
+size_t vxr_cc_last_repaired(void* c) {
+  return static_cast<velographx::IncrementalComponents*>(c)->last_repaired_vertices();
+}
+
+void* vxr_sssp_create(void* g, uint32_t source) {
+  return new velographx::IncrementalSSSP(*static_cast<DynamicGraph*>(g), source);
+}
+void vxr_sssp_destroy(void* s) { delete static_cast<velographx::IncrementalSSSP*>(s); }
+int vxr_sssp_apply(void* s, const uint32_t* src, const uint32_t* dst, const uint8_t* add, size_t n) {
+  static_cast<velographx::IncrementalSSSP*>(s)->apply(make_batch(src, dst, add, n));
+  return 0;
+}
+void vxr_sssp_recompute(void* s) { static_cast<velographx::IncrementalSSSP*>(s)->recompute(); }
+size_t vxr_sssp_distances(void* s, uint64_t* out, size_t cap) {
+  const auto& d = static_cast<velographx::IncrementalSSSP*>(s)->distances();
+  if (out) std::memcpy(out, d.data(), std::min(cap, d.size()) * sizeof(uint64_t));
+  return d.size();
 }
 
 }  // extern "C"

@@ -19,6 +19,8 @@ try:
     from ._velographx import (  # noqa: F401
         Graph,
         IncrementalBFS,
+        IncrementalComponents,
+        IncrementalSSSP,
         MultiRootBFS,
         UpdateBatch,
         from_arrow_columns,
@@ -51,6 +53,8 @@ def capi() -> _ctypes.CDLL:
 __all__ = [
     "Graph",
     "IncrementalBFS",
+    "IncrementalComponents",
+    "IncrementalSSSP",
     "MultiRootBFS",
     "UpdateBatch",
     "from_numpy_edges",

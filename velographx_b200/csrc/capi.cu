@@ -8,6 +8,7 @@
 
 #include "../../include/vx_b200.h"
 #include "bfs.cuh"
+#include "components.cuh"
 #include "graph.cuh"
 #include "io.cuh"
 #include "mrbfs.cuh"
@@ -35,6 +36,9 @@ struct vx_graph {
 struct vx_bfs {
   vxh::Bfs* b;
   vx_graph* owner;
+};
+struct vx_cc {
+  vxh::Components* c;
 };
 struct vx_mrbfs {
   vxh::MrBfs* m;
@@ -441,6 +445,43 @@ int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row) {
   b->b->tune.alpha = alpha;
   b->b->tune.beta = beta;
   b->b->tune.large_row = large_row;
+  return VX_OK;
+}
+
+int vx_cc_create(vx_graph* g, vx_cc** out) {
+  if (!g || !out) return fail(VX_ERR_INVALID, "null argument");
+  vxh::Components* c = nullptr;
+  if (int rc = vxh::cc_create(&c, g->g)) return rc;
+  *out = new vx_cc{c};
+  return VX_OK;
+}
+
+int vx_cc_destroy(vx_cc* c) {
+  if (!c) return VX_OK;
+  vxh::cc_destroy(c->c);
+  delete c;
+  return VX_OK;
+}
+
+int vx_cc_apply(vx_cc* c, const uint32_t* src, const uint32_t* dst, const uint8_t* add, size_t n) {
+  if (!c || (n && (!src || !dst || !add))) return fail(VX_ERR_INVALID, "null argument");
+  if (n == 0) {
+    c->c->last_repaired = 0;
+    return VX_OK;
+  }
+  size_t v_after = 0;
+  if (int rc = upload_batch(c->c->g, src, dst, add, n, &v_after)) return rc;
+  return vxh::cc_apply_staged(c->c, n, v_after);
+}
+
+int vx_cc_labels(vx_cc* c, uint32_t* out, size_t cap, size_t* n) {
+  if (!c || !n || (cap && !out)) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::cc_labels(c->c, out, cap, n);
+}
+
+int vx_cc_last_repaired_vertices(vx_cc* c, uint64_t* out) {
+  if (!c || !out) return fail(VX_ERR_INVALID, "null argument");
+  *out = c->c->last_repaired;
   return VX_OK;
 }
 

@@ -18,11 +18,17 @@
 #include <pybind11/stl.h>
 
 #include "velographx/incremental/bfs.hpp"
+#include "velographx/incremental/connected_components.hpp"
+#include "velographx/incremental/sssp.hpp"
+#include "velographx/io.hpp"
+#include "velographx/io/binary_graph.hpp"
 #include "velographx/storage/dynamic_graph.hpp"
 
 namespace py = pybind11;
 using velographx::DynamicGraph;
 using velographx::IncrementalBFS;
+using velographx::IncrementalComponents;
+using velographx::IncrementalSSSP;
 using velographx::UpdateBatch;
 using velographx::VertexId;
 namespace detail = velographx::detail;
@@ -338,6 +344,40 @@ PYBIND11_MODULE(_velographx, m) {
         detail::check(vx_bfs_set_tuning(x.handle(), alpha, beta, large_row));
       }, py::arg("alpha"), py::arg("beta"), py::arg("large_row"));
 
+  // the reference module's IncrementalComponents (python/bindings.cpp:45)
+  py::class_<IncrementalComponents>(m, "IncrementalComponents")
+      .def(py::init<DynamicGraph&>(), py::arg("graph"), py::keep_alive<1, 2>())
+      .def("component", &IncrementalComponents::component)
+      .def("apply", &IncrementalComponents::apply)
+      .def_property_readonly("last_repaired_vertices", &IncrementalComponents::last_repaired_vertices)
+      .def("apply_arrays",
+           [](IncrementalComponents& x, const u32_array& s, const u32_array& d, const u8_array& a) {
+             Arrays y(s, d, a);
+             {
+               py::gil_scoped_release release;
+               detail::check(vx_cc_apply(x.handle(), y.src.data(), y.dst.data(), y.add.data(), y.n));
+             }
+             x.mark_stale();
+           })
+      .def("labels_array", [](IncrementalComponents& x) {
+        std::size_t n = 0;
+        detail::check(vx_cc_labels(x.handle(), nullptr, 0, &n));
+        py::array_t<std::uint32_t> out(static_cast<py::ssize_t>(n));
+        if (n) {
+          auto* ptr = out.mutable_data();
+          py::gil_scoped_release release;
+          detail::check(vx_cc_labels(x.handle(), ptr, n, &n));
+        }
+        return out;
+      });
+  // BasicIncrementalSSSP<DynamicGraph> (include/velographx/incremental/sssp.hpp:14-69;
+  // not in the reference's Python module)
+  py::class_<IncrementalSSSP>(m, "IncrementalSSSP")
+      .def(py::init<DynamicGraph&, VertexId>(), py::arg("graph"), py::arg("source"), py::keep_alive<1, 2>())
+      .def_property_readonly("distances", [](const IncrementalSSSP& x) { return x.distances(); })
+      .def("apply", &IncrementalSSSP::apply)
+      .def("recompute", &IncrementalSSSP::recompute)
+      .def_property_readonly_static("unreachable", [](py::object) { return IncrementalSSSP::unreachable; });
   py::class_<MultiRoot>(m, "MultiRootBFS")
       .def(py::init<DynamicGraph&, const u32_array&>(), py::arg("graph"), py::arg("roots"), py::keep_alive<1, 2>())
       .def("run", [](MultiRoot& r) { detail::check(vx_mrbfs_run(r.h)); })
