@@ -134,6 +134,18 @@ int vx_graph_save_binary(vx_graph* g, const char* path);
  * (VX_ERR_FORMAT). */
 int vx_graph_load_binary(const char* path, int directed, vx_graph** out);
 
+/* ---- Consolidation (include/velographx/storage/consolidation.hpp) -------
+ * consolidate_to_csr_snapshot(source) :132-163: a new graph holding the
+ * source's logical edges as a fresh CSR (compact, version 1, the source's
+ * vertex count and direction); the source is not modified.  The rows are
+ * merged and re-sorted on the device. */
+int vx_graph_snapshot(vx_graph* g, vx_graph** out);
+/* Device time (ns) of one pass over every live arc of the graph and the arcs
+ * visited: the neighbour-iteration cost the consolidation signal compares
+ * between a graph and its snapshot (evaluate_consolidation, :49-63, takes it
+ * from the caller).  No reference counterpart. */
+int vx_graph_scan_rows(vx_graph* g, uint64_t* arcs, double* ns);
+
 /* The graph's CUDA stream (cudaStream_t) and a host-side wait for it. */
 int vx_graph_stream(vx_graph* g, void** stream);
 int vx_graph_synchronize(vx_graph* g);

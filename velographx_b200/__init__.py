@@ -29,8 +29,10 @@ try:
         from_scipy_csr,
         last_error,
         launch_count,
+        consolidate_to_csr_snapshot,
         load_binary,
         load_edge_list,
+        neighbor_scan_ns,
         save_binary,
     )
 except ImportError as exc:  # pragma: no cover - exercised only on a broken install

@@ -207,6 +207,19 @@ int vx_graph_load_binary(const char* path, int directed, vx_graph** out) {
   return VX_OK;
 }
 
+int vx_graph_snapshot(vx_graph* g, vx_graph** out) {
+  if (!g || !out) return fail(VX_ERR_INVALID, "null argument");
+  vxh::Graph* s = nullptr;
+  if (int rc = vxh::graph_snapshot(g->g, &s)) return rc;
+  *out = new vx_graph{s};
+  return VX_OK;
+}
+
+int vx_graph_scan_rows(vx_graph* g, uint64_t* arcs, double* ns) {
+  if (!g || !arcs || !ns) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::graph_scan_rows(g->g, arcs, ns);
+}
+
 int vx_graph_ensure_vertex(vx_graph* g, uint32_t v) {
   if (!g) return fail(VX_ERR_INVALID, "null argument");
   if ((size_t)v + 1 > vxb::kMaxVertices) return fail(VX_ERR_RANGE, "vertex id beyond the supported maximum (2^31 - 1)");

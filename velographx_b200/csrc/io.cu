@@ -1,4 +1,5 @@
-// On-disk formats of the graph, with the device doing the bulk work:
+// Whole-graph exports -- the on-disk formats and the consolidation snapshot --
+// with the device doing the bulk work:
 //
 //   load_edge_list  (src/io.cpp:23-53)                 a text edge list parsed on
 //                   the device -- newline positions by a chunked count and scan,
@@ -10,7 +11,10 @@
 //   load_binary     (binary_graph.hpp:15-20)             pairs uploaded, the
 //                   undirected filter u <= v applied on the device, then a
 //                   device bulk load (the same logical graph, version and vertex
-//                   count as the reference's apply + compact).
+//                   count as the reference's apply + compact);
+//   consolidate_to_csr_snapshot  (include/velographx/storage/consolidation.hpp:
+//                   132-163)  the same export bulk-loaded into a fresh graph,
+//                   the source untouched.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -18,6 +22,7 @@
 #include <vector>
 
 #include "graph.cuh"
+#include "frontier.cuh"
 #include "graph_dev.cuh"
 #include "io.cuh"
 #include "prims.cuh"
@@ -304,32 +309,122 @@ int graph_load_edge_list(const char* path, bool directed, Graph** out) {
   return 0;
 }
 
-int graph_save_binary(Graph* g, const char* path) {
+namespace {
+
+// Every arc of the logical graph as (u, v) pairs in `pairs` (m entries, rows
+// in vertex order, each ascending), on the graph's stream.
+int export_arcs(Graph* g, DevBufs& d, uint2** pairs_out, uint64_t* m_out) {
   cudaStream_t s = g->stream;
   if (int rc = graph_sync_counters(g)) return rc;
   const uint64_t n = g->V, m = graph_edge_count_directed(g);
   const vxb::DevAdj a = g->view().out;
-  DevBufs d;
   uint32_t *deg = nullptr, *vals = nullptr;
   uint64_t *off = nullptr, *tot = nullptr;
   uint2* pairs = nullptr;
   if (int rc = d.alloc(&deg, n) | d.alloc(&off, n) | d.alloc(&tot, 1) | d.alloc(&vals, m) | d.alloc(&pairs, m))
     return rc;
-  uint64_t total = 0;
   if (n) {
     count_launch();
     live_degree_kernel<<<grid_of(n), kIoThreads, 0, s>>>(a, (uint32_t)n, deg);
     if (int rc = scan_exclusive_u32_to_u64(deg, off, n, tot, g->scratch, s)) return rc;
+    uint64_t total = 0;
     VX_CUDA_TRY(cudaMemcpyAsync(&total, tot, 8, cudaMemcpyDeviceToHost, s));
     VX_CUDA_TRY(cudaStreamSynchronize(s));
     if (total != m) {
-      set_error("save_binary: %llu live arcs against an edge count of %llu", (unsigned long long)total,
+      set_error("graph export: %llu live arcs against an edge count of %llu", (unsigned long long)total,
                 (unsigned long long)m);
       return -5;
     }
     count_launch();
     export_rows_kernel<<<grid_of(32 * n), kIoThreads, 0, s>>>(a, (uint32_t)n, off, vals, pairs);
   }
+  *pairs_out = pairs;
+  *m_out = m;
+  return 0;
+}
+
+// Sum over every live arc of the logical graph (base arcs without tombstones,
+// then delta arcs), one warp per row: the neighbour-iteration cost of the
+// current layout.
+__global__ void scan_rows_kernel(vxb::DevAdj a, uint32_t V, unsigned long long* out) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  unsigned long long acc = 0, arcs = 0;
+  for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < V; u += nw) {
+    auto visit = [&](bool valid, uint32_t v, uint32_t) {
+      if (valid) {
+        acc += v;
+        ++arcs;
+      }
+    };
+    frontier::warp_row(a, u, visit);
+  }
+  acc = vxb::warp_sum(acc);
+  arcs = vxb::warp_sum(arcs);
+  if (lane == 0 && arcs) {
+    atomicAdd(&out[0], acc);
+    atomicAdd(&out[1], arcs);
+  }
+}
+
+}  // namespace
+
+int graph_snapshot(Graph* src, Graph** out) {
+  DevBufs d;
+  uint2* pairs = nullptr;
+  uint64_t m = 0;
+  if (int rc = export_arcs(src, d, &pairs, &m)) return rc;
+  Graph* g = nullptr;
+  if (int rc = graph_create(&g, src->V, src->directed)) return rc;
+  std::unique_ptr<Graph, void (*)(Graph*)> guard(g, graph_destroy);
+  // the pairs are read on the new graph's stream: the export must be done
+  VX_CUDA_TRY(cudaStreamSynchronize(src->stream));
+  if (!src->directed && m) {  // each undirected edge once (u < v); the load adds both arcs
+    unsigned long long* kept = nullptr;
+    if (int rc = d.alloc(&kept, 1)) return rc;
+    VX_CUDA_TRY(cudaMemsetAsync(kept, 0, 8, g->stream));
+    count_launch();
+    keep_upper_kernel<<<grid_of(m), kIoThreads, 0, g->stream>>>(pairs, m, kept);
+  }
+  if (int rc = graph_bulk_load(g, reinterpret_cast<const uint32_t*>(pairs), m)) return rc;
+  *out = guard.release();
+  return 0;
+}
+
+int graph_scan_rows(Graph* g, uint64_t* arcs, double* ns) {
+  cudaStream_t s = g->stream;
+  DevBufs d;
+  unsigned long long* acc = nullptr;
+  if (int rc = d.alloc(&acc, 2)) return rc;
+  cudaEvent_t e0, e1;
+  VX_CUDA_TRY(cudaEventCreate(&e0));
+  VX_CUDA_TRY(cudaEventCreate(&e1));
+  VX_CUDA_TRY(cudaMemsetAsync(acc, 0, 16, s));
+  VX_CUDA_TRY(cudaEventRecord(e0, s));
+  if (g->V) {
+    count_launch();
+    scan_rows_kernel<<<grid_of(32ull * g->V), kIoThreads, 0, s>>>(g->view().out, (uint32_t)g->V, acc);
+  }
+  VX_CUDA_TRY(cudaEventRecord(e1, s));
+  unsigned long long h[2] = {0, 0};
+  VX_CUDA_TRY(cudaMemcpyAsync(h, acc, 16, cudaMemcpyDeviceToHost, s));
+  VX_CUDA_TRY(cudaStreamSynchronize(s));
+  float ms = 0.f;
+  VX_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *arcs = h[1];
+  *ns = (double)ms * 1e6;
+  return 0;
+}
+
+int graph_save_binary(Graph* g, const char* path) {
+  cudaStream_t s = g->stream;
+  DevBufs d;
+  uint2* pairs = nullptr;
+  uint64_t m = 0;
+  if (int rc = export_arcs(g, d, &pairs, &m)) return rc;
+  const uint64_t n = g->V;
   std::vector<uint2> host(m);
   if (m) VX_CUDA_TRY(cudaMemcpyAsync(host.data(), pairs, m * sizeof(uint2), cudaMemcpyDeviceToHost, s));
   VX_CUDA_TRY(cudaStreamSynchronize(s));

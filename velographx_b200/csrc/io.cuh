@@ -1,5 +1,6 @@
-// On-disk formats of the graph (the reference's include/velographx/io.hpp,
-// include/velographx/io/binary_graph.hpp, src/io.cpp).
+// Whole-graph exports: the on-disk formats (the reference's
+// include/velographx/io.hpp, include/velographx/io/binary_graph.hpp,
+// src/io.cpp) and the consolidation snapshot (storage/consolidation.hpp).
 #pragma once
 
 #include "graph.cuh"
@@ -20,5 +21,11 @@ int graph_load_edge_list(const char* path, bool directed, Graph** out);
 int graph_save_binary(Graph* g, const char* path);
 // load_binary(path, directed) (binary_graph.hpp:15-20): a new graph.
 int graph_load_binary(const char* path, bool directed, Graph** out);
+// consolidate_to_csr_snapshot(source) (consolidation.hpp:132-163): a new
+// compact graph with the source's logical edges and vertex count.
+int graph_snapshot(Graph* src, Graph** out);
+// Device time of one pass over every live arc (the neighbour-iteration cost
+// of the current layout) and the arcs it visited.
+int graph_scan_rows(Graph* g, uint64_t* arcs, double* ns);
 
 }  // namespace vxh

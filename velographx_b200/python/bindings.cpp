@@ -22,6 +22,7 @@
 #include "velographx/incremental/sssp.hpp"
 #include "velographx/io.hpp"
 #include "velographx/io/binary_graph.hpp"
+#include "velographx/storage/consolidation.hpp"
 #include "velographx/storage/dynamic_graph.hpp"
 
 namespace py = pybind11;
@@ -439,6 +440,20 @@ PYBIND11_MODULE(_velographx, m) {
         return DynamicGraph::adopt(g);
       },
       py::arg("path"), py::arg("directed") = false);
+  // consolidate_to_csr_snapshot (include/velographx/storage/consolidation.hpp:132-163)
+  m.def(
+      "consolidate_to_csr_snapshot",
+      [](const DynamicGraph& src) {
+        auto snap = velographx::consolidate_to_csr_snapshot(src);
+        py::dict d;
+        d["source_storage_bytes"] = snap.source_storage_bytes;
+        d["consolidated_storage_bytes"] = snap.consolidated_storage_bytes;
+        d["directed_edges"] = snap.directed_edges;
+        d["graph"] = py::cast(std::move(snap.graph));
+        return d;
+      },
+      py::arg("source"));
+  m.def("neighbor_scan_ns", [](const DynamicGraph& g) { return velographx::neighbor_scan_ns(g); }, py::arg("graph"));
   m.def("from_numpy_edges", &graph_from_numpy_edges, py::arg("edges"), py::arg("directed") = false);
   m.def("from_scipy_csr", &graph_from_scipy_csr, py::arg("csr"), py::arg("directed") = false);
   m.def("from_arrow_columns", &graph_from_arrow_columns, py::arg("src"), py::arg("dst"), py::arg("directed") = false);
