@@ -202,43 +202,23 @@ def run_b200(args, rank, world, local):
     cs = torch.cuda.ExternalStream(g.stream)
     A = g.edge_count_directed()
 
-    # ---- autotune the direction switch (alpha, beta) on a few roots, untimed ----
-    def time_bfs(b):
-        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        s0.record(cs)
-        b.recompute()
-        s1.record(cs)
-        s1.synchronize()
-        return s0.elapsed_time(s1)
-
-    tune_roots = roots[: min(4, len(roots))].tolist()
-    best, tuning = None, []
-    alphas = (4.0, 14.0, 40.0, 120.0) if args.alpha is None else (args.alpha,)
-    betas = (8.0, 24.0, 96.0) if args.beta is None else (args.beta,)
+    # ---- the library's autotuner picks the direction switch and the
+    # grid-expanded row length on a few roots (untimed) ----
+    tuner = vx.IncrementalBFS(g, int(roots[0]))
     if args.alpha is not None and args.beta is not None:
-        alphas, betas, best = (), (), (args.alpha, args.beta, 0.0)
-    for alpha in alphas:
-        for beta in betas:
-            ts = []
-            for r in tune_roots:
-                b = vx.IncrementalBFS(g, int(r))
-                b.set_tuning(alpha, beta, 1024)
-                b.recompute()
-                ts.append(time_bfs(b))
-                del b
-            t = float(np.median(ts))
-            tuning.append((alpha, beta, round(t, 4)))
-            if best is None or t < best[2]:
-                best = (alpha, beta, t)
-    alpha, beta = best[0], best[1]
+        tuner.set_tuning(args.alpha, args.beta, 1024)
+        chosen = {"alpha": args.alpha, "beta": args.beta, "large_row": 1024, "fixed": True}
+    else:
+        chosen = tuner.autotune(roots[: min(4, len(roots))])
+    alpha, beta, large_row = tuner.tuning()
+    del tuner
 
     # ---- direction-optimising full BFS from the roots (GTEPS, roofline) ----
     bfs_ms, arcs, levels = [], [], []
     trace = None
     for r in roots.tolist():
         b = vx.IncrementalBFS(g, int(r))
-        b.set_tuning(alpha, beta, 1024)
+        b.set_tuning(alpha, beta, large_row)
         b.recompute()  # warm
         s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -290,7 +270,7 @@ def run_b200(args, rank, world, local):
     # ---- update stream, device-resident batches (value) ----
     root = int(roots[0])
     b = vx.IncrementalBFS(g, root)
-    b.set_tuning(alpha, beta, 1024)
+    b.set_tuning(alpha, beta, large_row)
     ops = args.batch_ops
     dsrc = torch.from_numpy(stream.src.view(np.int32)).cuda()
     ddst = torch.from_numpy(stream.dst.view(np.int32)).cuda()
@@ -366,7 +346,7 @@ def run_b200(args, rank, world, local):
         gv = vx.Graph(V, False)
         gv.bulk_load_edges(edges)
         bv = vx.IncrementalBFS(gv, root)
-        bv.set_tuning(alpha, beta, 1024)
+        bv.set_tuning(alpha, beta, large_row)
         for i in range(min(args.ref_batches, stream.batches)):
             bv.apply_arrays(*stream.batch(i))
             gpu_recs.append(record(gv, bv))
@@ -407,7 +387,8 @@ def run_b200(args, rank, world, local):
         "bfs": {"roots": int(len(roots)), "gteps": gteps, "ms_mean": float(bfs_ms.mean()),
                 "ms_median": float(np.median(bfs_ms)), "levels_median": float(np.median(levels)),
                 "arcs": int(A), "level_trace_root0_us_nf_dir": trace,
-                "autotune": {"alpha": alpha, "beta": beta, "sweep_alpha_beta_ms": tuning}},
+                "autotune": {"alpha": alpha, "beta": beta, "large_row": int(large_row), "chosen": chosen,
+                             "by": "vx_bfs_autotune (36 candidates, median of 4 roots)"}},
         "multiroot_bfs": multiroot,
         "repair_last": {"affected": st["last_affected_vertices"], "candidates": st["last_deletion_candidates"],
                         "full": st["last_used_full_recompute"]},

@@ -2092,6 +2092,68 @@ int bfs_recompute(Bfs* b) {
   return launch(b, p, kModeFull);
 }
 
+// The direction switch and the grid-expanded row length of the full BFS,
+// picked by timing: every candidate (alpha, beta, large_row) of a small grid
+// runs a full BFS from each of the given roots (CUDA events on the graph's
+// stream, one untimed warm-up per candidate), the median over the roots
+// decides, and the best candidate stays set on b.  The distances from b's
+// own source are recomputed afterwards.
+int bfs_autotune(Bfs* b, const uint32_t* roots, size_t k, float* chosen) {
+  static const float kAlpha[] = {4.f, 14.f, 40.f, 120.f};
+  static const float kBeta[] = {8.f, 24.f, 96.f};
+  static const uint32_t kLarge[] = {512u, 1024u, 4096u};
+  Graph* g = b->g;
+  cudaStream_t s = g->stream;
+  const uint32_t source = b->source;
+  const BfsTuning keep = b->tune;
+  cudaEvent_t e0, e1;
+  VX_CUDA_TRY(cudaEventCreate(&e0));
+  VX_CUDA_TRY(cudaEventCreate(&e1));
+  float best = -1.f;
+  BfsTuning pick = keep;
+  std::vector<float> ts(k);
+  int rc = 0;
+  for (float al : kAlpha)
+    for (float be : kBeta)
+      for (uint32_t lr : kLarge) {
+        b->tune.alpha = al;
+        b->tune.beta = be;
+        b->tune.large_row = lr;
+        for (size_t r = 0; r < k && !rc; ++r) {
+          b->source = roots[r];
+          if (r == 0) rc = bfs_recompute(b);  // warm-up of this candidate
+          if (!rc && cudaEventRecord(e0, s) != cudaSuccess) rc = -3;
+          if (!rc) rc = bfs_recompute(b);
+          if (!rc && cudaEventRecord(e1, s) != cudaSuccess) rc = -3;
+          if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = -3;
+          if (!rc && cudaEventElapsedTime(&ts[r], e0, e1) != cudaSuccess) rc = -3;
+        }
+        if (rc) break;
+        std::vector<float> sorted(ts);
+        std::sort(sorted.begin(), sorted.end());
+        const float med = sorted[k / 2];
+        if (best < 0.f || med < best) {
+          best = med;
+          pick = b->tune;
+        }
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->source = source;
+  b->tune = rc ? keep : pick;
+  if (rc) {
+    set_error("autotune: timing failed");
+    return rc;
+  }
+  if (chosen) {
+    chosen[0] = pick.alpha;
+    chosen[1] = pick.beta;
+    chosen[2] = (float)pick.large_row;
+    chosen[3] = best;
+  }
+  return bfs_recompute(b);
+}
+
 int bfs_stage(Bfs* b, size_t n, size_t vertex_bound, bool classify) {
   Graph* g = b->g;
   cudaStream_t s = g->stream;

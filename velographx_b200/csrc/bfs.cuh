@@ -105,6 +105,10 @@ struct Bfs {
 int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac);
 void bfs_destroy(Bfs* b);
 int bfs_recompute(Bfs* b);
+// Times a grid of (alpha, beta, large_row) on full BFS from the k roots and
+// keeps the fastest (median over the roots); chosen = {alpha, beta,
+// large_row, median ms}.  Recomputes b's own distances afterwards.
+int bfs_autotune(Bfs* b, const uint32_t* roots, size_t k, float* chosen);
 // Incremental apply of the batch in b->g->batch (ops already on device):
 // bfs_stage (canonicalise + classify on the pre-batch graph) followed by
 // bfs_repair_staged (the reference's apply) or bfs_full_staged (graph apply +

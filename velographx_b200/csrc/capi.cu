@@ -447,6 +447,22 @@ int vx_bfs_level_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n) {
   return vxh::bfs_level_trace(b->b, reinterpret_cast<unsigned long long*>(out), cap, n);
 }
 
+int vx_bfs_autotune(vx_bfs* b, const uint32_t* roots, size_t k, float* chosen) {
+  if (!b || (k && !roots)) return fail(VX_ERR_INVALID, "null argument");
+  if (k == 0) return fail(VX_ERR_INVALID, "autotune needs at least one root");
+  for (size_t i = 0; i < k; ++i)
+    if (roots[i] >= b->b->g->V) return fail(VX_ERR_RANGE, "autotune root beyond the vertex count");
+  return vxh::bfs_autotune(b->b, roots, k, chosen);
+}
+
+int vx_bfs_get_tuning(vx_bfs* b, float* alpha, float* beta, uint32_t* large_row) {
+  if (!b || !alpha || !beta || !large_row) return fail(VX_ERR_INVALID, "null argument");
+  *alpha = b->b->tune.alpha;
+  *beta = b->b->tune.beta;
+  *large_row = b->b->tune.large_row;
+  return VX_OK;
+}
+
 int vx_bfs_set_update_blocks(vx_bfs* b, uint32_t blocks) {
   if (!b) return fail(VX_ERR_INVALID, "null argument");
   b->b->tune.update_blocks = blocks;

@@ -311,6 +311,27 @@ PYBIND11_MODULE(_velographx, m) {
            },
            py::arg("ops"), py::arg("batches"), py::arg("max_batch_ops"))
       .def("set_fused", [](IncrementalBFS& x, bool fused) { detail::check(vx_bfs_set_fused(x.handle(), fused)); })
+      .def(
+          "autotune",
+          [](IncrementalBFS& x, const u32_array& roots) {
+            if (roots.ndim() != 1) throw std::invalid_argument("roots: 1-D array");
+            float c[4] = {0, 0, 0, 0};
+            {
+              py::gil_scoped_release release;
+              detail::check(vx_bfs_autotune(x.handle(), roots.data(), static_cast<std::size_t>(roots.shape(0)), c));
+            }
+            x.mark_stale();
+            return py::dict(py::arg("alpha") = c[0], py::arg("beta") = c[1],
+                            py::arg("large_row") = static_cast<std::uint32_t>(c[2]), py::arg("median_ms") = c[3]);
+          },
+          py::arg("roots"))
+      .def("tuning",
+           [](IncrementalBFS& x) {
+             float a = 0, b = 0;
+             std::uint32_t l = 0;
+             detail::check(vx_bfs_get_tuning(x.handle(), &a, &b, &l));
+             return py::make_tuple(a, b, l);
+           })
       .def("set_update_blocks",
            [](IncrementalBFS& x, std::uint32_t blocks) { detail::check(vx_bfs_set_update_blocks(x.handle(), blocks)); })
       .def("digest",
