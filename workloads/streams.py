@@ -104,7 +104,7 @@ def run_stream(g: Graph, bfs: IncrementalBFS, root: int, stream: w.Stream, check
     per = np.asarray(per)
     return {"batches": nb, "seconds": float(per.sum() * 1e-6), "batches_per_s": float(nb / (per.sum() * 1e-6)),
             "us_median": float(np.median(per)), "us_p90": float(np.percentile(per, 90)), "us_max": float(per.max()),
-            "exact": bool(exact), "exact_checks": checked}
+            "exact": bool(exact), "exact_checks": checked, "_per_batch_us": per}
 
 
 def grid(side: int = 4096, long_range: float = 0.001, batches: int = 500, ops: int = 1000,
@@ -118,6 +118,8 @@ def grid(side: int = 4096, long_range: float = 0.001, batches: int = 500, ops: i
     V = side * side
     g = Graph(V, False)
     g.bulk_load_edges(edges)
+    # device memory for the whole stream up front (no batch grows the arena)
+    g.reserve(ops, ops * batches)
     root = 0
     bfs = IncrementalBFS(g, root)
     cs = torch.cuda.ExternalStream(g.stream)
@@ -136,16 +138,30 @@ def grid(side: int = 4096, long_range: float = 0.001, batches: int = 500, ops: i
                 "vertices": V, "arcs": int(g.edge_count_directed()), "full_bfs_ms": full_ms,
                 "full_bfs_levels": int(levels)})
     del bfs, g
+    # a replica replays every batch untimed: the records of the first
+    # ref_batches (for the CPU reference) and each batch's counters, which
+    # name what the slowest timed batches did
+    per = res.pop("_per_batch_us")
+    g = Graph(V, False)
+    g.bulk_load_edges(edges)
+    g.reserve(ops, ops * batches)
+    b = IncrementalBFS(g, root)
+    recs, stats = [], []
+    for t in range(batches):
+        b.apply_arrays(*stream.batch(t))
+        st = b.stats()
+        stats.append((bool(st["last_used_full_recompute"]), int(st["last_affected_vertices"]),
+                      int(st["last_deletion_candidates"])))
+        if t < ref_batches:
+            recs.append(record(g, b))
+    del b, g
+    slow = np.argsort(per)[::-1][:5]
+    res["fallback_batches"] = int(sum(x[0] for x in stats))
+    res["slowest"] = [{"batch": int(i), "us": round(float(per[i]), 1), "full_recompute": stats[i][0],
+                       "affected": stats[i][1], "candidates": stats[i][2]} for i in slow]
+    res["affected_median"] = float(np.median([x[1] for x in stats]))
     if ref_batches:
         k = min(ref_batches, batches)
-        g = Graph(V, False)
-        g.bulk_load_edges(edges)
-        b = IncrementalBFS(g, root)
-        recs = []
-        for t in range(k):
-            b.apply_arrays(*stream.batch(t))
-            recs.append(record(g, b))
-        del b, g
         res["_check"] = (edges, stream.prefix(k), root, recs)
     return res
 
