@@ -170,6 +170,16 @@ def profiled_traffic():
         return None
 
 
+def profiled_step_traffic():
+    """DRAM bytes per update step from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "update_step_rmat22_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
 # ----------------------------------------------------------------- B200 arm --
 
 def run_b200(args, rank, world, local):
@@ -339,21 +349,45 @@ def run_b200(args, rank, world, local):
 
     # ---- the records of the first ref_batches batches on a fresh replica
     # (untimed), for the per-batch comparison with the CPU reference ----
+    # The same replica counts the algorithmic bytes of the timed batches
+    # (batches warmup .. warmup + steps - 1, the ones the timed region
+    # applied): the update launch's own accounting (vx_bfs_set_accounting)
+    # for the repair and commit, plus the batch's arrays and canonical arcs.
     gpu_recs = []
-    if rank == 0 and world == 1 and not args.no_cpu and args.ref_batches:
-        from workloads.streams import record
+    acct = None
+    from workloads.streams import record
 
-        gv = vx.Graph(V, False)
-        gv.bulk_load_edges(edges)
-        bv = vx.IncrementalBFS(gv, root)
-        bv.set_tuning(alpha, beta, large_row)
-        for i in range(min(args.ref_batches, stream.batches)):
-            bv.apply_arrays(*stream.batch(i))
+    gv = vx.Graph(V, False)
+    gv.bulk_load_edges(edges)
+    gv.reserve(args.batch_ops, args.batch_ops * stream.batches)
+    bv = vx.IncrementalBFS(gv, root)
+    bv.set_tuning(alpha, beta, large_row)
+    want_recs = args.ref_batches if (rank == 0 and world == 1 and not args.no_cpu) else 0
+    for i in range(max(want_recs, args.warmup + args.steps)):
+        if i == args.warmup:
+            bv.set_accounting(True)
+        lo, hi = int(stream.offsets[i]), int(stream.offsets[i + 1])
+        bv.apply_device(dsrc.data_ptr() + 4 * lo, ddst.data_ptr() + 4 * lo, dadd.data_ptr() + lo, hi - lo, V)
+        if i == args.warmup + args.steps - 1:
+            acct = bv.accounting()
+            bv.set_accounting(False)
+        if i < want_recs:
             gpu_recs.append(record(gv, bv))
-        del bv, gv
+    del bv, gv
 
     hbm, hbm_kind = measured_hbm()
     traffic = profiled_traffic()
+    # bytes one update step must move at least (per batch): the op arrays the
+    # canonicalisation reads (9 B per op), its canonical arcs written and read
+    # back (17 B each: u, v, flags, base position), the delta-row entries the
+    # commit reads and writes (4 B), and the repair's row arcs and visited
+    # vertices (4 B each: a column id, a distance)
+    nb_acct = max(1, acct["batches"])
+    step_bytes = (9.0 * args.batch_ops + 2 * 17.0 * acct["canonical_arcs"] / nb_acct
+                  + 4.0 * acct["delta_entries"] / nb_acct + 4.0 * acct["arcs_scanned"] / nb_acct
+                  + 4.0 * acct["vertices_visited"] / nb_acct)
+    step_achieved = step_bytes / (t_dev / args.steps) / 1e9
+    step_traffic = profiled_step_traffic()
     line = {
         "metric": "update-batches/s",
         "value": value,
@@ -383,6 +417,21 @@ def run_b200(args, rank, world, local):
             "frac": achieved / hbm,
             "traffic": (traffic or {}).get("dram_bytes_per_launch"),
             "algorithmic_bytes": "4*A_r + 8*(V+1) + 4*V per root",
+        },
+        "roofline_step": {
+            "kernel": "one update step: canon_cluster_kernel + bfs_stream_kernel (fused commit and repair)",
+            "bound": "hbm",
+            "achieved": step_achieved,
+            "peak": hbm,
+            "peak_kind": hbm_kind,
+            "unit": "GB/s",
+            "frac": step_achieved / hbm,
+            "algorithmic_bytes_per_batch": step_bytes,
+            "traffic": (step_traffic or {}).get("dram_bytes_per_batch"),
+            "counters_per_batch": {k: acct[k] / nb_acct for k in ("arcs_scanned", "vertices_visited",
+                                                                  "delta_entries", "canonical_arcs")},
+            "algorithmic_bytes": "9*ops + 2*17*canonical_arcs + 4*delta_entries + 4*arcs_scanned + "
+                                 "4*vertices_visited per batch (counted by the launch on a replica)",
         },
         "bfs": {"roots": int(len(roots)), "gteps": gteps, "ms_mean": float(bfs_ms.mean()),
                 "ms_median": float(np.median(bfs_ms)), "levels_median": float(np.median(levels)),

@@ -224,6 +224,15 @@ int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row);
  * reference counterpart: the reference BFS is top-down only. */
 int vx_bfs_autotune(vx_bfs* b, const uint32_t* roots, size_t k, float* chosen);
 int vx_bfs_get_tuning(vx_bfs* b, float* alpha, float* beta, uint32_t* large_row);
+/* Algorithmic-byte accounting of the update launches (measurement only; off
+ * by default, and every counted event costs an atomic when on).  on != 0
+ * zeroes the counters and starts counting; vx_bfs_accounting copies the five
+ * sums since then: {row arcs the repair scanned (cascade checks, expansions,
+ * boundary rows, relaxations), vertices it visited (checks, ring items,
+ * invalidations, heads of canonical arcs), delta-row entries the commit read
+ * and wrote, canonical arcs, batches}.  No reference counterpart. */
+int vx_bfs_set_accounting(vx_bfs* b, int on);
+int vx_bfs_accounting(vx_bfs* b, uint64_t* out5);
 /* Thread blocks of the persistent update launch (fused single batch and
  * batched stream): 0 (default) = every block that can be co-resident; fewer
  * blocks shorten the grid barriers and the ring's termination for small

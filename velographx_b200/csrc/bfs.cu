@@ -77,10 +77,18 @@ struct Params {
   uint32_t large_row;
   uint32_t nblocks;
   unsigned long long* trace;  // optional per-level {time, n_f | bottom-up << 63}
+  // optional accounting of the update launch's algorithmic bytes (null: off):
+  // [0] row arcs scanned by the repair, [1] vertices it visited, [2] delta-row
+  // entries the commit read and wrote, [3] canonical arcs, [4] batches
+  unsigned long long* acct;
   uint32_t* bar;              // grid barrier words
 };
 
 constexpr uint32_t kTraceLevels = 256;
+
+__device__ __forceinline__ void acct_add(const Params& p, int k, unsigned long long v) {
+  if (p.acct && v) atomicAdd(&p.acct[k], v);
+}
 
 // Grid barrier; returns false once any block recorded a device error (a
 // barrier that gave up waiting, a loop bound), so every persistent loop ends.
@@ -595,7 +603,7 @@ __device__ __forceinline__ uint32_t item_chunk(unsigned long long it) { return (
 // chunk pushes the rest as items of their own.
 template <class T, class F>
 __device__ void block_rows(const DevAdj& a, const T* items, uint32_t n, LbStage& st, F& f,
-                           const Params* p = nullptr) {
+                           const Params* p = nullptr, unsigned long long* acct = nullptr) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __shared__ uint32_t wsum[kThreads / 32];
   uint32_t len = 0;
@@ -655,6 +663,7 @@ __device__ void block_rows(const DevAdj& a, const T* items, uint32_t n, LbStage&
   if (threadIdx.x + 1 == n) st.pref[n] = ex + len;
   __syncthreads();
   const uint32_t M = n ? st.pref[n] : 0u;
+  if (acct && threadIdx.x == 0 && M) atomicAdd(&acct[0], (unsigned long long)M);
   for (uint32_t e0 = (uint32_t)warp * 32; e0 < M; e0 += kThreads) {
     const uint32_t e = e0 + lane;
     bool valid = false;
@@ -782,6 +791,7 @@ __device__ void drain(const Params& p, RepairSmem& sm, W& w) {
     w.process(sm, n);
     __syncthreads();
     if (threadIdx.x == 0) {
+      acct_add(p, 1, n);
       __threadfence();  // this block's pushes are visible before its items count as done
       atomicAdd(p.rq_done, n);
       atomicAdd(&p.rq_stat[0], 1ull);
@@ -884,6 +894,7 @@ __device__ __forceinline__ bool find_parent(const Params& p, const DevAdj& a, ui
                                             uint32_t lo, uint32_t hi, uint32_t d, uint32_t& kw, uint32_t& yw) {
   const int lane = threadIdx.x & 31;
   for (uint32_t k0 = lo; k0 < hi; k0 += 128) {
+    if (lane == 0) acct_add(p, 0, min(128u, hi - k0));
     uint32_t y[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -980,7 +991,9 @@ __device__ void check_vertex(const Params& p, uint32_t x) {
     __syncwarp();
     __threadfence();
     // past the fallback limit the block path drops expansions; so does this one
-    if (degree_of(p.g.out, x) <= kInlineExpand && !ld_cg(&p.c->fallback)) {
+    const uint32_t odeg = degree_of(p.g.out, x);
+    if (odeg <= kInlineExpand && !ld_cg(&p.c->fallback)) {
+      if (lane == 0) acct_add(p, 0, odeg);
       ExpandChildren ec{&p, x, d};
       warp_row(p.g.out, x, ec);
       inlined = true;
@@ -1096,7 +1109,7 @@ struct Cascade {
         }
         request_check(P, need, x);
       };
-      block_rows(P.g.out, sm.ex, nex, *lb, expand, &P);
+      block_rows(P.g.out, sm.ex, nex, *lb, expand, &P, P.acct);
     }
   }
 };
@@ -1229,6 +1242,7 @@ __device__ void seed_relax(const Params& p, bool lowered, uint32_t v, long long&
     if (deg > kInlineRelax) {
       queue = true;
     } else {
+      acct_add(p, 0, deg);
       const uint32_t dv = ld_cg(&p.dist[v]);
       for (uint32_t k = 0; k < deg; ++k) {
         uint32_t x;
@@ -1272,7 +1286,7 @@ struct Relax {
       const bool lowered = valid && du != kUnreachable && x < P.dist_len && lower(P, x, du + 1, *reach);
       lower_and_push(P, lowered, x);
     };
-    block_rows(P.g.out, sm.items, n, *lb, relax, &P);
+    block_rows(P.g.out, sm.items, n, *lb, relax, &P, P.acct);
   }
 };
 
@@ -1302,7 +1316,7 @@ __device__ void boundary_seeds(const Params& p, RepairSmem& sm, LbStage& lb, uin
       const uint32_t dx = p.dist[x];
       if (dx != kUnreachable) atomicMin(&sm.cnt[j], dx + 1);
     };
-    block_rows(p.g.in, sm.sv, k, lb, bmin);
+    block_rows(p.g.in, sm.sv, k, lb, bmin, nullptr, p.acct);
     bool seed = false;
     uint32_t v = 0;
     if (threadIdx.x < k && sm.sv[threadIdx.x] != 0xFFFFFFFFu) {
@@ -1334,6 +1348,7 @@ __device__ void grid_boundary_min(const Params& p, uint32_t nb) {
     vxb::base_range(a, v, b, e);
     const uint2 dr = a.drow[v];
     const uint64_t nbase = e - b, total = nbase + dr.y;
+    if (w % G == 0 && lane == 0) acct_add(p, 0, total);
     for (uint64_t k = (uint64_t)(w % G) * 32 + lane; k < total; k += (uint64_t)G * 32) {
       uint32_t x;
       if (k < nbase) {
@@ -1368,6 +1383,7 @@ __device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQ
   // kernel or a kernel boundary
   stamp(p, 3);
   const uint32_t na = ld_cg(&c->a_n);
+  if (gtid() == 0) acct_add(p, 1, na);  // invalidated and re-seeded
   long long reach = 0;
   if (na > 0) {
     // invalidate the affected vertices (repair_affected, bfs.hpp:272-283)
@@ -1497,7 +1513,7 @@ __device__ __forceinline__ bool delta_op(uint8_t f, bool insertion) {
 // keeps every entry that is not a removal of the run (delta_remove_kernel of
 // the per-batch path, on the canonical arcs directly).
 __device__ void run_remove(const vxb::DevAdj& a, const uint32_t* fv, const uint8_t* ff, uint32_t s, uint32_t e, uint32_t u,
-                           GraphCounters* gc) {
+                           GraphCounters* gc, unsigned long long* acct) {
   const int lane = threadIdx.x & 31;
   bool any = false;
   for (uint32_t k = s + lane; k < e; k += 32) any |= delta_op(ff[k], false);
@@ -1523,6 +1539,7 @@ __device__ void run_remove(const vxb::DevAdj& a, const uint32_t* fv, const uint8
   }
   if (lane == 0) {
     a.drow[u].y = written;
+    if (acct) atomicAdd(acct, (unsigned long long)(row.y + written));
     atomicAdd(&gc->delta_live[0], (unsigned long long)(-(long long)(row.y - written)));
     gdev::mark_dirty(a.dirty, u, &gc->dirty_rows[0]);
   }
@@ -1533,7 +1550,8 @@ __device__ void run_remove(const vxb::DevAdj& a, const uint32_t* fv, const uint8
 // place when its block has room, else into a new power-of-two arena block
 // (delta_insert_kernel of the per-batch path).
 __device__ void run_insert(const vxb::DevAdj& a, const uint32_t* fv, const uint8_t* ff, uint32_t* scratch, uint32_t s,
-                           uint32_t e, uint32_t u, GraphCounters* gc, unsigned long long arena_cap) {
+                           uint32_t e, uint32_t u, GraphCounters* gc, unsigned long long arena_cap,
+                           unsigned long long* acct) {
   const int lane = threadIdx.x & 31;
   uint32_t nB = 0;
   for (uint32_t base = s; base < e; base += 32) {
@@ -1569,6 +1587,7 @@ __device__ void run_insert(const vxb::DevAdj& a, const uint32_t* fv, const uint8
   }
   if (lane == 0) {
     atomicAdd(&gc->delta_live[0], (unsigned long long)nB);
+    if (acct) atomicAdd(acct, (unsigned long long)(row.y + cnew));
     gdev::mark_dirty(a.dirty, u, &gc->dirty_rows[0]);
   }
 }
@@ -1654,6 +1673,7 @@ __device__ void commit_runs(const Params& p, const StreamArgs& s, uint32_t off, 
       dst[0] = make_uint4(out(0), out(1), out(2), out(3));
       dst[1] = make_uint4(out(4), out(5), out(6), out(7));
       dlive = kInsert ? 1 : -1;
+      acct_add(p, 2, 2ull * row.y + (kInsert ? 1 : -1));
       a.drow[u] = make_uint2(base_off, kInsert ? row.y + 1 : row.y - 1);
       if (need_block) a.dcap[u] = 8u;
       const uint32_t bit = 1u << (u & 31);
@@ -1668,8 +1688,9 @@ __device__ void commit_runs(const Params& p, const StreamArgs& s, uint32_t off, 
     const uint32_t nq = sm.nsv;
     for (uint32_t k = threadIdx.x >> 5; k < nq; k += kThreads / 32) {
       const uint32_t st = sm.sv[k], en = run_end(fu, st, F);
-      if (kInsert) run_insert(a, fv, ff, s.scratch, st, en, fu[st], s.gc, s.arena_cap);
-      else run_remove(a, fv, ff, st, en, fu[st], s.gc);
+      unsigned long long* ac = p.acct ? p.acct + 2 : nullptr;
+      if (kInsert) run_insert(a, fv, ff, s.scratch, st, en, fu[st], s.gc, s.arena_cap, ac);
+      else run_remove(a, fv, ff, st, en, fu[st], s.gc, ac);
     }
     __syncthreads();  // the list is rebuilt by the next round
   }
@@ -1740,7 +1761,12 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
     stamp(q, 1);
     // C: the cascade over the graph without the batch's deletions
     const uint32_t ncand = ld_cg(&c->cand_n);
-    if (gtid() == 0) c->candidates = ncand;
+    if (gtid() == 0) {
+      c->candidates = ncand;
+      acct_add(p, 1, ncand + F);  // candidate checks, heads of the canonical arcs
+      acct_add(p, 3, F);
+      acct_add(p, 4, 1);
+    }
     if (ncand) {
       if (!cascade(q, sm, lb, ncand)) return;
       if (gtid() == 0) c->affected = ld_cg(&c->a_n);
@@ -2011,6 +2037,7 @@ static Params make_params(Bfs* b, uint32_t V, uint32_t dist_len) {
   p.beta = b->tune.beta;
   p.large_row = b->tune.large_row;
   p.trace = b->trace;
+  p.acct = b->acct_on ? b->acct : nullptr;
   p.bar = b->barrier;
   return p;
 }
@@ -2067,6 +2094,7 @@ void bfs_destroy(Bfs* b) {
                       b->lst_a, b->lst_t, b->tent, b->bul, b->sw, b->aff, b->inq[0], b->inq[1]};
   for (uint32_t* p : ptrs) cudaFree(p);
   cudaFree(b->ctr);
+  cudaFree(b->acct);
   cudaFree(b->trace);
   cudaFree(b->barrier);
   cudaFree(b->features);
@@ -2152,6 +2180,24 @@ int bfs_autotune(Bfs* b, const uint32_t* roots, size_t k, float* chosen) {
     chosen[3] = best;
   }
   return bfs_recompute(b);
+}
+
+int bfs_set_accounting(Bfs* b, int on) {
+  if (on && !b->acct && cudaMalloc(&b->acct, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+    set_error("accounting counter allocation failed");
+    return -4;
+  }
+  if (on) VX_CUDA_TRY(cudaMemsetAsync(b->acct, 0, 8 * sizeof(unsigned long long), b->g->stream));
+  b->acct_on = on != 0;
+  return 0;
+}
+
+int bfs_accounting(Bfs* b, unsigned long long* out5) {
+  memset(out5, 0, 5 * sizeof(unsigned long long));
+  if (!b->acct) return 0;
+  VX_CUDA_TRY(cudaMemcpyAsync(out5, b->acct, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, b->g->stream));
+  VX_CUDA_TRY(cudaStreamSynchronize(b->g->stream));
+  return 0;
 }
 
 int bfs_stage(Bfs* b, size_t n, size_t vertex_bound, bool classify) {

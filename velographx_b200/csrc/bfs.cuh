@@ -99,12 +99,20 @@ struct Bfs {
   BfsTuning tune;
   int grid = 0;
   int stream_grid = 0;
+  unsigned long long* acct = nullptr;  // algorithmic-byte accounting (5 counters), when on
+  bool acct_on = false;
   StreamBufs sb;
 };
 
 int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac);
 void bfs_destroy(Bfs* b);
 int bfs_recompute(Bfs* b);
+// Algorithmic-byte accounting of the update launches: on != 0 allocates and
+// zeroes the counters and turns it on; counters are {row arcs scanned by the
+// repair, vertices visited, delta-row entries read and written, canonical
+// arcs, batches} summed since it was turned on.
+int bfs_set_accounting(Bfs* b, int on);
+int bfs_accounting(Bfs* b, unsigned long long* out5);
 // Times a grid of (alpha, beta, large_row) on full BFS from the k roots and
 // keeps the fastest (median over the roots); chosen = {alpha, beta,
 // large_row, median ms}.  Recomputes b's own distances afterwards.

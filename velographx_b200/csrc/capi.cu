@@ -463,6 +463,16 @@ int vx_bfs_get_tuning(vx_bfs* b, float* alpha, float* beta, uint32_t* large_row)
   return VX_OK;
 }
 
+int vx_bfs_set_accounting(vx_bfs* b, int on) {
+  if (!b) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::bfs_set_accounting(b->b, on);
+}
+
+int vx_bfs_accounting(vx_bfs* b, uint64_t* out5) {
+  if (!b || !out5) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::bfs_accounting(b->b, reinterpret_cast<unsigned long long*>(out5));
+}
+
 int vx_bfs_set_update_blocks(vx_bfs* b, uint32_t blocks) {
   if (!b) return fail(VX_ERR_INVALID, "null argument");
   b->b->tune.update_blocks = blocks;

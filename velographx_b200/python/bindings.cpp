@@ -332,6 +332,16 @@ PYBIND11_MODULE(_velographx, m) {
              detail::check(vx_bfs_get_tuning(x.handle(), &a, &b, &l));
              return py::make_tuple(a, b, l);
            })
+      .def("set_accounting",
+           [](IncrementalBFS& x, bool on) { detail::check(vx_bfs_set_accounting(x.handle(), on ? 1 : 0)); })
+      .def("accounting",
+           [](IncrementalBFS& x) {
+             std::uint64_t a[5] = {0, 0, 0, 0, 0};
+             detail::check(vx_bfs_accounting(x.handle(), a));
+             return py::dict(py::arg("arcs_scanned") = a[0], py::arg("vertices_visited") = a[1],
+                             py::arg("delta_entries") = a[2], py::arg("canonical_arcs") = a[3],
+                             py::arg("batches") = a[4]);
+           })
       .def("set_update_blocks",
            [](IncrementalBFS& x, std::uint32_t blocks) { detail::check(vx_bfs_set_update_blocks(x.handle(), blocks)); })
       .def("digest",
