@@ -95,6 +95,7 @@ struct PushVisit {
 };
 
 constexpr uint32_t kMrHead = 8;       // in-arcs a lane pulls itself before its warp helps
+constexpr uint32_t kMrStep = 4;       // of which it loads this many at a time
 constexpr uint32_t kMrBigRow = 4096;  // push rows this long are expanded by the whole grid
 
 // Pull level: one warp per 32 vertices.  Each lane ORs the frontier words of
@@ -125,20 +126,27 @@ __device__ void pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, 
     }
     const uint32_t nb = (uint32_t)(e - b), total = nb + dr.y;
     const uint32_t head = todo ? min(total, kMrHead) : 0u;
-    for (uint32_t j = 0; j < head && !done; ++j) {
-      uint32_t x;
-      if (j < nb) {
-        x = a.col[b + j];
-        if (x & kTomb) continue;
-      } else {
-        x = a.darena[dr.x + (j - nb)];
+    // the head in steps of kMrStep arcs: the step's column loads issue
+    // together, then its frontier-word loads, so a step costs two dependent
+    // round trips instead of two per arc
+    for (uint32_t j0 = 0; j0 < head && !done; j0 += kMrStep) {
+      uint32_t x[kMrStep];
+#pragma unroll
+      for (uint32_t k = 0; k < kMrStep; ++k) {
+        const uint32_t j = j0 + k;
+        x[k] = j >= head ? kTomb : (j < nb ? a.col[b + j] : a.darena[dr.x + (j - nb)]);
+      }
+#pragma unroll
+      for (uint32_t w = 0; w < W; ++w) {
+        uint32_t m = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < kMrStep; ++k)
+          if (!(x[k] & kTomb)) m |= fc[(size_t)x[k] * W + w];
+        acc[w] |= m & ~vis[w];
       }
       done = true;
 #pragma unroll
-      for (uint32_t w = 0; w < W; ++w) {
-        acc[w] |= fc[(size_t)x * W + w] & ~vis[w];
-        done = done && (vis[w] | acc[w]) == word_mask(p, w);
-      }
+      for (uint32_t w = 0; w < W; ++w) done = done && (vis[w] | acc[w]) == word_mask(p, w);
     }
     uint32_t longm = __ballot_sync(FULL, todo && !done && total > head);
     while (longm) {
