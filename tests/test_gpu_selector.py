@@ -167,12 +167,15 @@ def test_reduced_regime_study():
     assert np.all(rd.t_repair > 0) and np.all(rd.t_full > 0)
     assert np.all(np.isfinite(rd.features))
     rep = study.evaluate([rd], train_fraction=0.3, epochs=200)
-    for arm in ("mlp", "heuristic"):
+    for arm in ("mlp", "heuristic", "always_repair", "always_full"):
         r = rep[arm]
         assert 0 <= r["wrong_arm_rate"] <= 1
         assert r["equal_regime_mean_regret"] >= 0 and np.isfinite(r["max_regret"])
     assert rep["mlp"]["fallbacks"] == 0
-    # what the trained network gains over the heuristic on held-out batches
-    # (timing noise gets a 1% slack)
-    assert rep["mlp"]["equal_regime_mean_regret"] <= rep["heuristic"]["equal_regime_mean_regret"] + 0.01, rep
+    # what the trained network gains on held-out batches: it must do at least
+    # as well as the reference's heuristic and as both trivial policies of the
+    # reference's ablation (timing noise between the two arm runs gets 0.5%)
+    mlp = rep["mlp"]["equal_regime_mean_regret"]
+    for arm in ("heuristic", "always_repair", "always_full"):
+        assert mlp <= rep[arm]["equal_regime_mean_regret"] + 0.005, (arm, rep)
     print(rep)
