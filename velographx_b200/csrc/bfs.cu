@@ -1736,27 +1736,37 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
       // so a small batch's searches spread over every SM
       const vxb::DevAdj& a = p.g.out;
       long long tombs = 0;
-      uint32_t dirtied = 0;
+      uint32_t dirtied = 0, removals = 0;
       for (uint32_t i = threadIdx.x * gridDim.x + blockIdx.x; i < F; i += nthreads()) {
         uint8_t f = s.ff[off + i];
         if (!s.classified) {
           f = gdev::classify_arc(a, s.fu[off + i], s.fv[off + i], f, s.fpos[off + i]);
           s.ff[off + i] = f;
         }
+        removals += !(f & kFAdd) && (f & kFChanged);
         tombs += gdev::tomb_arc(a, s.fu[off + i], f, s.fpos[off + i], 0, dirtied);
       }
       tombs = vxb::warp_sum(tombs);
       dirtied = vxb::warp_sum(dirtied);
+      removals = vxb::warp_sum(removals);
       if (lane == 0 && tombs) atomicAdd(&s.gc->tombs[0], (unsigned long long)tombs);
       if (lane == 0 && dirtied) atomicAdd(&s.gc->dirty_rows[0], (unsigned long long)dirtied);
+      if (lane == 0 && removals) atomicAdd(&c->rmb[bi & 1], removals);
       if (s.digest && bi > 0) digest_pass(p.dist, lpre, &s.digest[bi - 1]);
     }
     if (!sync_grid(p)) return;
     phase(0);
-    // B: delta removals; deletion candidates registered
-    commit_runs<false>(q, s, off, F, sm);
-    register_candidates(q);
-    if (!sync_grid(p)) return;
+    // B: delta removals; deletion candidates registered.  A batch without a
+    // removal arc has neither, and skips the phase and its barrier.  The other
+    // parity's counter was last read before the previous batch's later
+    // barriers: it is cleared here for the next batch.
+    const uint32_t nrm = ld_cg(&c->rmb[bi & 1]);
+    if (gtid() == 0) c->rmb[(bi + 1) & 1] = 0u;
+    if (nrm) {
+      commit_runs<false>(q, s, off, F, sm);
+      register_candidates(q);
+      if (!sync_grid(p)) return;
+    }
     phase(1);
     stamp(q, 1);
     // C: the cascade over the graph without the batch's deletions
@@ -1808,6 +1818,8 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
     }
   }
   if (s.digest && s.nb) digest_pass(p.dist, s.vpost[s.nb - 1], &s.digest[s.nb - 1]);
+  // every read of the removal counters came before the last end-of-batch barrier
+  if (gtid() == 0) c->rmb[0] = c->rmb[1] = 0u;
 }
 
 __global__ void __launch_bounds__(kThreads, 3) bfs_kernel(Params p, int mode) {

@@ -40,6 +40,10 @@ struct BfsCounters {
   // (classify + tombstones, removals + candidates, cascade, insertions,
   // post-batch repair, end-of-batch barrier), summed over its batches, ns
   unsigned long long stream_ns[6];
+  // removal arcs of the update launch's current batch (two slots, by batch
+  // parity; zero between launches): a batch without any skips the removal
+  // phase and its barrier
+  uint32_t rmb[2];
 };
 
 struct BfsTuning {
