@@ -265,8 +265,18 @@ def run_b200(args, rank, world, local):
             runs.append(s0.elapsed_time(s1))
         ms = float(np.median(runs))
         marcs = mr.reached_arcs()
+        # bit-parallel algorithmic bytes: every level reads each row once for
+        # all roots (offsets + columns) and the W frontier/visited words of
+        # every vertex, plus one distance write per (root, vertex)
+        W = (k + 31) // 32
+        b_bitpar = mr.levels * (8.0 * (V + 1) + 4.0 * A + 2 * 4.0 * W * V) + 4.0 * k * V
+        b_noshare = float((4.0 * np.asarray([marcs / max(1, k)]) + 8.0 * (V + 1) + 4.0 * V)[0]) * k
         multiroot[str(k)] = {"ms": ms, "ms_runs": [round(x, 3) for x in runs],
-                             "gteps": marcs / 2 / (ms * 1e-3) / 1e9, "levels": mr.levels}
+                             "gteps": marcs / 2 / (ms * 1e-3) / 1e9, "levels": mr.levels,
+                             "algorithmic_bytes_bitparallel": b_bitpar,
+                             "achieved_gbs_bitparallel": b_bitpar / (ms * 1e-3) / 1e9,
+                             "algorithmic_bytes_no_sharing": b_noshare,
+                             "achieved_gbs_no_sharing": b_noshare / (ms * 1e-3) / 1e9}
         if k == 64:  # rows of the last run against single-root full BFS (untimed)
             d = mr.distances_array()
             rows = (0, 21, 42, 63)
