@@ -234,9 +234,10 @@ int vx_bfs_get_tuning(vx_bfs* b, float* alpha, float* beta, uint32_t* large_row)
 int vx_bfs_set_accounting(vx_bfs* b, int on);
 int vx_bfs_accounting(vx_bfs* b, uint64_t* out5);
 /* Thread blocks of the persistent update launch (fused single batch and
- * batched stream): 0 (default) = every block that can be co-resident; fewer
- * blocks shorten the grid barriers and the ring's termination for small
- * batches.  Results are the same for every value.  No reference counterpart. */
+ * batched stream): 0 (default) = one per SM; any count up to the co-resident
+ * maximum (larger counts are clamped to it).  Fewer blocks shorten the grid
+ * barriers and the work ring's polling.  Results are the same for every
+ * value.  No reference counterpart. */
 int vx_bfs_set_update_blocks(vx_bfs* b, uint32_t blocks);
 /* fused != 0 (default): an undirected batch's commit and repair run in one
  * persistent launch after staging; 0: the per-phase path (a launch per commit

@@ -40,6 +40,9 @@ using namespace frontier;
 
 constexpr int kThreads = 512;
 enum { kModeFull = 0, kModePre = 1, kModePost = 2 };
+// slots past the vertex count in each candidate list: the per-block segments
+// of ceil(V / blocks) slots cover at most V + blocks - 1 (blocks <= 148 * 4)
+constexpr uint32_t kListSlack = 1024;
 
 struct Params {
   vxb::DevGraph g;
@@ -54,8 +57,8 @@ struct Params {
   uint32_t* lst_a;
   uint32_t* lst_t;
   uint32_t* tent;
-  uint32_t* bul;      // bottom-up candidate lists A (bul[0, bul_half)) and B (bul[bul_half, 2 * bul_half))
-  uint32_t bul_half;
+  uint32_t* bul;      // bottom-up candidate lists A (bul[0, bul_half)) and B (bul[bul_half, 2 * bul_half)),
+  uint32_t bul_half;  // each cut into one segment per block (bul_half >= V + blocks)
   unsigned long long* sw;  // support words of the pre-batch cascade (zero between batches)
   unsigned long long* ring;  // work ring of the repair phases (kSent between phases)
   uint32_t ring_mask;
@@ -289,25 +292,38 @@ __device__ void grid_rows(const DevAdj& a, const uint32_t* rows, uint32_t n, F& 
 
 constexpr uint32_t kBuHead = 8;  // arcs a lane scans itself before the warp helps
 
-// Bottom-up over a candidate list: lin[0, nin) holds the vertices that may
-// still be reached (unvisited when the list was made, in-degree > 0; the
-// first list is every such vertex, built by the full BFS's initialisation,
-// later ones the previous level's misses).  One warp per 32 entries: each
-// lane scans the first kBuHead in-arcs of its row, the rest of longer rows is
-// scanned by the whole warp 32 arcs at a time, every scan stops at the first
-// parent in the frontier bitmap.  Entries visited since the list was made are
-// skipped; entries that find no parent are appended to the next list (lout,
-// counter cnt_out whose value out_base corresponds to lout[0]), so isolated
-// vertices cost nothing and a later level scans only the remaining ones.
-// Entries are loaded two groups ahead and their visited words and row bounds
-// one group ahead, so those loads are in flight while a group is scanned.
+// Appends v where pred holds to a block-private list segment (seg, counter
+// n in shared memory), in lane order within the warp.  Warp-uniform.
+__device__ __forceinline__ void seg_append(bool pred, uint32_t v, uint32_t* seg, uint32_t* n) {
+  const uint32_t m = __ballot_sync(FULL, pred);
+  if (!m) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(n, (uint32_t)__popc(m));
+  base = __shfl_sync(FULL, base, leader);
+  if (pred) seg[base + __popc(m & vxb::lanemask_lt())] = v;
+}
+
+// Bottom-up over this block's segment of a candidate list: lin[0, nin) holds
+// vertices that may still be reached (unvisited when the list was made,
+// in-degree > 0; the first list is every such vertex of the block's range,
+// built by the full BFS's initialisation, later ones the previous level's
+// misses).  One warp per 32 entries: each lane scans the first kBuHead
+// in-arcs of its row, the rest of longer rows is scanned by the whole warp 32
+// arcs at a time, every scan stops at the first parent in the frontier
+// bitmap.  Entries visited since the list was made are skipped; entries that
+// find no parent go to the block's segment of the other list (lout, counter
+// nout in shared memory), so isolated vertices cost nothing and a later level
+// scans only the vertices still unreached.  Entries are loaded two groups
+// ahead and their visited words and row bounds one group ahead, so those
+// loads are in flight while a group is scanned.  Block-uniform.
 __device__ void bu_list_level(const Params& p, uint32_t level, const uint32_t* fbc, uint32_t* fbn, uint32_t* qout,
                               uint32_t* cnt_n, BlockQueue& bq, const uint32_t* lin, uint32_t nin, uint32_t* lout,
-                              uint32_t* cnt_out, uint32_t out_base, BlockQueue& bqf) {
+                              uint32_t* nout) {
   const DevAdj& a = p.g.in;
   const int lane = threadIdx.x & 31;
-  const uint32_t step = nwarps() * 32;
-  uint32_t base = gwarp() * 32;
+  const uint32_t step = kThreads;  // the block's warps take consecutive 32-entry groups
+  uint32_t base = (threadIdx.x >> 5) * 32;
   uint32_t v1 = base + step + lane < nin ? lin[base + step + lane] : kUnreachable;
   uint32_t v0 = base + lane < nin ? lin[base + lane] : kUnreachable;
   uint32_t vis0 = 0;
@@ -396,38 +412,41 @@ __device__ void bu_list_level(const Params& p, uint32_t level, const uint32_t* f
       atomicOr(&fbn[word], bits);
     }
     bq_push(bq, found, v, cnt_n, qout);
-    bq_push(bqf, todo && !found, v, cnt_out, lout, out_base);
+    seg_append(todo && !found, v, lout, nout);
   }
   bq_flush(bq, cnt_n, qout);
-  bq_flush(bqf, cnt_out, lout, out_base);
 }
 
 // ------------------------------------------------------------ full BFS --
 
-// Precondition: c->bun[0] == c->bun[1] == 0 (set by the host before a
-// recompute launch, by repair_post before its fallback, by the allocation-free
-// entry's counter reset, and by the end of every full BFS).
-__device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst, BlockQueue& bqf) {
+__device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
   BfsCounters* c = p.c;
-  if (threadIdx.x == 0) bq.cnt = bqf.cnt = 0;
+  __shared__ uint32_t seg_n[2];  // entries of this block's segment of each candidate list
+  if (threadIdx.x == 0) bq.cnt = 0;
   const uint32_t V = p.V;
   const uint32_t words = (V + 31) >> 5;
   // one pass sets every vertex unreached and the source at level 0 (bits
   // past V count as visited, so bottom-up never scans them), and lists the
   // bottom-up candidates: every vertex but the source with a nonempty in-row
-  // (isolated vertices never enter a bottom-up level)
+  // (isolated vertices never enter a bottom-up level).  Each block takes a
+  // contiguous range of vertices and lists its candidates in its own segment
+  // of list A (shared-memory counter, no global atomics); a bottom-up level
+  // scans the block's own segment.
   const uint32_t s = p.source;
   const bool has_source = s < V;
-  for (uint32_t i0 = gwarp() * 32; i0 < V; i0 += nwarps() * 32) {
-    const uint32_t i = i0 + (threadIdx.x & 31);
+  const uint32_t seg = (V + gridDim.x - 1) / gridDim.x;  // vertices (and list slots) per block
+  const uint32_t seg_lo = blockIdx.x * seg, seg_hi = min(V, seg_lo + seg);
+  if (threadIdx.x == 0) seg_n[0] = seg_n[1] = 0;
+  __syncthreads();
+  for (uint32_t i0 = seg_lo; i0 < seg_hi; i0 += kThreads) {
+    const uint32_t i = i0 + threadIdx.x;
     bool cand = false;
-    if (i < V) {
+    if (i < seg_hi) {
       p.dist[i] = i == s ? 0u : kUnreachable;
       cand = has_source && i != s && degree_of(p.g.in, i) != 0u;
     }
-    bq_push(bqf, cand, i, &c->bun[0], p.bul);
+    seg_append(cand, i, p.bul + seg_lo, &seg_n[0]);
   }
-  bq_flush(bqf, &c->bun[0], p.bul);
   for (uint32_t i = gtid(); i < words; i += nthreads()) {
     const uint32_t lo = i * 32;
     const uint32_t sbit = has_source && i == (s >> 5) ? 1u << (s & 31) : 0u;
@@ -461,10 +480,8 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst, BlockQu
   // barrier that ends the level before it
   uint32_t n_f = ld_cg(&c->lvl_n[0]);
   unsigned long long m_f = __ldcg(&c->lvl_m[0]);
-  // bottom-up candidate lists: list k holds entries [lbase[k], ld(bun[k])) of
-  // its counter's range (counters are never reset during the BFS, so every
-  // block derives the same bases); the first bottom-up level reads list 0
-  uint32_t lin = 0, lbase[2] = {0u, 0u};  // the counters read 0 at entry (precondition)
+  // bottom-up candidate lists: the first bottom-up level reads list 0
+  uint32_t lin = 0;
   for (;; ++level) {
     if (level > V + 1) {
       if (gtid() == 0) atomicOr(&c->err, vxb::kErrLoopBound);
@@ -499,12 +516,10 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst, BlockQu
     }
     if (bottom_up) {
       const uint32_t lout = lin ^ 1u;
-      // list lout was last emptied when it was consumed, so its counter still
-      // reads lbase[lout]; at most nin entries are appended to it
-      const uint32_t nin = min(ld_cg(&c->bun[lin]) - lbase[lin], p.bul_half);
-      bu_list_level(p, level, p.fb[cur], p.fb[nxt], p.q[nxt], &c->lvl_n[nxt], bq, p.bul + lin * p.bul_half, nin,
-                    p.bul + lout * p.bul_half, &c->bun[lout], lbase[lout], bqf);
-      lbase[lin] += nin;  // consumed: its next contents start at the counter's current value
+      if (threadIdx.x == 0) seg_n[lout] = 0;
+      __syncthreads();
+      bu_list_level(p, level, p.fb[cur], p.fb[nxt], p.q[nxt], &c->lvl_n[nxt], bq, p.bul + lin * p.bul_half + seg_lo,
+                    seg_n[lin], p.bul + lout * p.bul_half + seg_lo, &seg_n[lout]);
       lin = lout;
       if (!sync_grid(p)) return;
       prev_n = n_f;
@@ -536,9 +551,6 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst, BlockQu
     c->reachable = reached;
     c->levels = level;
     c->arcs = m_visited;
-    // every append of this BFS came before the barrier that ended its last
-    // level: the list counters are free again for the next one
-    c->bun[0] = c->bun[1] = 0u;
     if (p.trace && level < kTraceLevels) {
       p.trace[2 * level] = globaltimer();
       p.trace[2 * level + 1] = 0;
@@ -699,15 +711,6 @@ struct RepairSmem {
   uint32_t cnt[kThreads];    // chunk + 1 of a chunk-check sv item (0: plain check); boundary minima
   uint32_t d[kThreads];      // distance of each staged item
   uint32_t g0, n, stop, nsv, nex, fallback;
-};
-
-// The repair phases' shared memory and the full BFS's candidate-list queue
-// share one allocation: a full BFS (recompute, or the fallback of the
-// post-batch repair) runs while no repair phase is active, and every repair
-// phase sets the fields it reads before reading them.
-union RepairUnion {
-  RepairSmem sm;
-  BlockQueue bqf;
 };
 
 // Drains the ring; W::process(sm, n) handles sm.items[0, n) block-uniformly.
@@ -1367,14 +1370,13 @@ __device__ void grid_boundary_min(const Params& p, uint32_t nb) {
   }
 }
 
-__device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQueue& bq, BlockQueue& bqf) {
+__device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQueue& bq) {
   BfsCounters* c = p.c;
   const int lane = threadIdx.x & 31;
   if (ld_cg(&c->fallback)) {
-    if (gtid() == 0) c->bun[0] = c->bun[1] = 0u;  // the full BFS's precondition (after the barrier below)
     clear_workspace(p);
     if (!sync_grid(p)) return;
-    full_bfs(p, bq, lb, bqf);
+    full_bfs(p, bq, lb);
     if (gtid() == 0) c->full = 1;
     return;
   }
@@ -1696,8 +1698,7 @@ __device__ void commit_runs(const Params& p, const StreamArgs& s, uint32_t off, 
   }
 }
 
-__device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm, LbStage& lb, BlockQueue& bq,
-                                   BlockQueue& bqf) {
+__device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm, LbStage& lb, BlockQueue& bq) {
   BfsCounters* c = p.c;
   const int lane = threadIdx.x & 31;
   unsigned long long tmark = globaltimer();
@@ -1803,7 +1804,7 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
     // E: the post-batch repair (or the fallback full BFS) on the new graph
     q.V = Vpost;
     q.dist_len = Vpost;
-    repair_post(q, sm, lb, bq, bqf);
+    repair_post(q, sm, lb, bq);
     if (ld_cg(&c->err)) return;
     phase(4);
     // every block's counter updates are in before they are recorded, and
@@ -1825,17 +1826,17 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
 __global__ void __launch_bounds__(kThreads, 3) bfs_kernel(Params p, int mode) {
   __shared__ BlockQueue bq;
   __shared__ LbStage lb;
-  __shared__ RepairUnion ru;
-  if (mode == kModeFull) full_bfs(p, bq, lb, ru.bqf);
-  else if (mode == kModePre) repair_pre(p, ru.sm, lb);
-  else repair_post(p, ru.sm, lb, bq, ru.bqf);
+  __shared__ RepairSmem sm;
+  if (mode == kModeFull) full_bfs(p, bq, lb);
+  else if (mode == kModePre) repair_pre(p, sm, lb);
+  else repair_post(p, sm, lb, bq);
 }
 
 __global__ void __launch_bounds__(kThreads, 2) bfs_stream_kernel(Params p, StreamArgs s) {
   __shared__ BlockQueue bq;
   __shared__ LbStage lb;
-  __shared__ RepairUnion ru;
-  stream_kernel_body(p, s, ru.sm, lb, bq, ru.bqf);
+  __shared__ RepairSmem sm;
+  stream_kernel_body(p, s, sm, lb, bq);
 }
 
 // Stream canonicalisation: both arcs of every non-self-loop op keyed by
@@ -1973,7 +1974,7 @@ static int ensure_capacity(Bfs* b, size_t V) {
   rc |= realloc_copy(&b->lst_a, c, 0, 0);
   rc |= realloc_copy(&b->lst_t, c, 0, 0);
   rc |= realloc_copy(&b->tent, c, 0, 0);
-  rc |= realloc_copy(&b->bul, 2 * c, 0, 0);
+  rc |= realloc_copy(&b->bul, 2 * (c + kListSlack), 0, 0);
   const cudaError_t e = cudaStreamSynchronize(s);
   for (uint32_t* p : old) cudaFree(p);
   if (rc) return -4;
@@ -2027,7 +2028,7 @@ static Params make_params(Bfs* b, uint32_t V, uint32_t dist_len) {
   p.lst_t = b->lst_t;
   p.tent = b->tent;
   p.bul = b->bul;
-  p.bul_half = (uint32_t)b->cap;
+  p.bul_half = (uint32_t)(b->cap + kListSlack);
   p.sw = reinterpret_cast<unsigned long long*>(b->sw);
   p.ring = b->ring;
   p.ring_mask = b->ring_slots ? (uint32_t)(b->ring_slots - 1) : 0u;
@@ -2122,8 +2123,7 @@ int bfs_recompute(Bfs* b) {
   const size_t V = g->V;
   if (int rc = ensure_capacity(b, std::max<size_t>(V, 1))) return rc;
   b->dist_len = V;
-  // last_* counters, and the full BFS's candidate-list counters (bun)
-  VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->candidates, 0, 6 * sizeof(uint32_t), g->stream));
+  VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->candidates, 0, 4 * sizeof(uint32_t), g->stream));
   if (V == 0) {
     VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->reachable, 0, 8, g->stream));
     return 0;
@@ -2241,8 +2241,11 @@ static int launch_stream(Bfs* b, Params& p, StreamArgs& sa) {
     }
     b->stream_grid = per_sm * sm_count();
   }
-  const uint32_t want = b->tune.update_blocks;
-  p.nblocks = want && want < (uint32_t)b->stream_grid ? want : (uint32_t)b->stream_grid;
+  // one block per SM by default: against two per SM (every co-resident
+  // block) the grid barriers and the work ring's polling are cheaper, and the
+  // update step measured 13% faster at R-MAT 22 and R-MAT 20
+  const uint32_t want = b->tune.update_blocks ? b->tune.update_blocks : (uint32_t)sm_count();
+  p.nblocks = want < (uint32_t)b->stream_grid ? want : (uint32_t)b->stream_grid;
   void* args[] = {&p, &sa};
   count_launch();
   VX_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)bfs_stream_kernel, dim3(p.nblocks), dim3(kThreads), args,
@@ -2586,7 +2589,7 @@ struct StaticBfsScratch {
   uint32_t fb[3][kStaticWords];
   uint32_t q[3][kStaticMaxVertices];
   uint32_t big[kStaticMaxVertices];
-  uint32_t bul[2 * kStaticMaxVertices];  // the bottom-up candidate lists
+  uint32_t bul[2 * (kStaticMaxVertices + kListSlack)];  // the bottom-up candidate lists
   uint2 drow[kStaticMaxVertices];  // kept all-zero: a plain CSR has no delta rows
   BfsCounters ctr;
   uint32_t bar[vxb::kBarrierWords];
@@ -2666,7 +2669,7 @@ extern "C" int vx_bfs_csr_static(const uint64_t* d_out_offsets, const uint32_t* 
   }
   p.big = sc->big;
   p.bul = sc->bul;
-  p.bul_half = vxh::kStaticMaxVertices;
+  p.bul_half = vxh::kStaticMaxVertices + vxh::kListSlack;
   p.c = &sc->ctr;
   p.total_arcs = arcs;
   p.alpha = 14.0f;

@@ -17,7 +17,6 @@ struct BfsCounters {
   uint32_t affected;              // last_affected_vertices
   uint32_t full;                  // last_used_full_recompute
   uint32_t fallback;              // fixpoint exceeded the fallback limit
-  uint32_t bun[2];                // bottom-up candidate lists: entries appended in this BFS (zero at its start)
   uint32_t err;
   // per-level counters of the persistent loops (3-way rotation)
   uint32_t lvl_n[3];
