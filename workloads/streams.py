@@ -187,7 +187,7 @@ def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int 
     out = {"workload": f"rmat{scale}-undirected-ef16-{batches}x{ops}-insertions", "vertices": V, "root": int(root),
            "batches": batches}
     e0, e1 = _events()
-    plain_runs, batched_runs, same = [], [], True
+    plain_runs, batched_runs, same, phases = [], [], True, []
     for _ in range(repeats):
         g = Graph(V, False)
         g.bulk_load_edges(edges)
@@ -217,6 +217,8 @@ def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int 
         torch.cuda.synchronize()
         batched_runs.append(batches / (e0.elapsed_time(e1) * 1e-3))
         same = same and [int(x) for x in digs] == [int(x) for x in plain_digests]
+        ph = b2.phase_trace()[21:27]
+        phases.append([x / 1e3 / batches for x in ph])
         del b, g, b2, g2
     # the records of every batch, on one more replica (untimed)
     g = Graph(V, False)
@@ -228,7 +230,10 @@ def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int 
     same = same and [r[0] for r in recs] == [int(x) for x in digs]
     del b, g
     out["plain"] = {"batches_per_s": float(np.median(plain_runs)), "runs": [round(x) for x in plain_runs]}
-    out["batched"] = {"batches_per_s": float(np.median(batched_runs)), "runs": [round(x) for x in batched_runs]}
+    out["batched"] = {"batches_per_s": float(np.median(batched_runs)), "runs": [round(x) for x in batched_runs],
+                      "phase_us_per_batch": dict(zip(
+                          ["classify", "removals", "cascade", "insertions", "post_repair", "end_barrier"],
+                          [round(float(np.median([r[k] for r in phases])), 2) for k in range(6)]))}
     out["plain_equals_batched"] = bool(same)
     out["_check"] = (edges, st, root, recs)
     return out
