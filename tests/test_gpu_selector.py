@@ -161,7 +161,7 @@ def test_reduced_regime_study():
     V = 1 << 14
     edges = w.rmat_edges(14, 16, seed=21)
     root = w.max_degree_root(edges, V)
-    sizes = np.tile([10, 300, 3000, 30000], 12)
+    sizes = np.tile([10, 300, 3000, 30000], 24)
     rd = study.collect("rmat14", edges, V, root, sizes, 0.75, seed=4)
     assert rd.exact
     assert np.all(rd.t_repair > 0) and np.all(rd.t_full > 0)

@@ -78,6 +78,7 @@ class MLPSelector:
         _check(self.lib.vx_selector_create(seed, C.byref(self.h)))
         self.mu = np.zeros(2)
         self.sd = np.ones(2)
+        self.margin = 0.0  # log-ratio margin full must win by (fit calibrates it)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -124,7 +125,30 @@ class MLPSelector:
         loss = C.c_float()
         _check(self.lib.vx_selector_train(self.h, X.ctypes.data_as(_f32p), Y.ctypes.data_as(_f32p), len(X), epochs,
                                           batch, lr, seed, C.byref(loss)))
+        self.margin = self.calibrate_margin(X, t_repair, t_full)
         return loss.value
+
+    # candidate margins of the predicted log ratio log(t_full / t_repair)
+    MARGINS = (0.0, 0.02, 0.05, 0.1, 0.2, 0.4, 0.8, np.inf)
+
+    def calibrate_margin(self, X, t_repair, t_full) -> float:
+        """The margin by which the predicted full time must undercut the
+        predicted repair time before full is chosen, picked on the training
+        batches: the candidate with the smallest mean regret there (an
+        infinite margin is always repair; ties go to the larger margin, the
+        cheaper mistake).  Prediction errors on a noisy training set
+        otherwise send batches to the full arm whose rare wins do not pay for
+        its losses."""
+        Y = self.predict_log(X)
+        d = Y[:, 1] - Y[:, 0]
+        oracle = np.minimum(t_repair, t_full)
+        best, best_r = 0.0, np.inf
+        for m in self.MARGINS:
+            full = np.isfinite(d) & (d <= -m)
+            r = float(np.mean(np.maximum(0.0, (np.where(full, t_full, t_repair) - oracle) / oracle)))
+            if r <= best_r:
+                best, best_r = m, r
+        return best
 
     def predict_raw(self, X) -> np.ndarray:
         """The network's two outputs for each row of X (standardised units)."""
@@ -140,12 +164,13 @@ class MLPSelector:
         return np.stack([Y[:, 0] - Y[:, 1] / 2, Y[:, 0] + Y[:, 1] / 2], axis=1)
 
     def choose_full(self, X):
-        """(choose_full, ok): full where it is predicted no slower (full wins
-        ties); ok is False where a prediction is not finite, and the caller
-        then falls back to the heuristic."""
+        """(choose_full, ok): full where its predicted log time undercuts
+        repair's by the calibrated margin (with margin 0, full wins ties); ok
+        is False where a prediction is not finite, and the caller then falls
+        back to the heuristic."""
         Y = self.predict_log(X)
         ok = np.all(np.isfinite(Y), axis=1)
-        return np.where(ok, Y[:, 1] <= Y[:, 0], False), ok
+        return np.where(ok, Y[:, 1] - Y[:, 0] <= -self.margin, False), ok
 
 
 class Heuristic:

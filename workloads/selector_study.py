@@ -219,7 +219,7 @@ def evaluate(regimes: list[RegimeData], train_fraction: float = 0.3, seed: int =
         tr_f.append(rg.t_full[:k])
     mlp = MLPSelector(seed)
     loss = mlp.fit(np.concatenate(tr_X), np.concatenate(tr_r), np.concatenate(tr_f), epochs=epochs, seed=seed)
-    out = {"train_loss": loss, "regimes": {}}
+    out = {"train_loss": loss, "margin": float(mlp.margin), "regimes": {}}
     names = ("mlp", "mlp_online", "heuristic", "always_repair", "always_full")
     regrets = {n: [] for n in names}
     wrong = dict.fromkeys(names, 0)
@@ -244,7 +244,7 @@ def evaluate(regimes: list[RegimeData], train_fraction: float = 0.3, seed: int =
         pred = mlp.predict_log(X)
         ok = np.all(np.isfinite(pred), axis=1)
         fallbacks += int((~ok).sum())
-        static = np.where(ok, pred[:, 1] <= pred[:, 0], h_full)
+        static = np.where(ok, mlp.choose_full(X)[0], h_full)
         choice = {"mlp": static, "mlp_online": calibrated_choices(pred, ok, tr, tf, h_full), "heuristic": h_full,
                   "always_repair": np.zeros(len(tr), bool), "always_full": np.ones(len(tr), bool)}
         row = {"batches": len(tr), "full_share_oracle": float(oracle_full.mean()), "exact": rg.exact}
