@@ -83,9 +83,20 @@ __global__ void cc_rows_kernel(vxb::DevAdj a, uint32_t V, uint32_t* label, const
   }
 }
 
+// Every label becomes its root.  The walk only reads: with path halving, a
+// thread that read a vertex's old parent could store it back after the
+// vertex's own thread had stored the root, leaving a label that is not a
+// root.  Here each thread stores only its own label, and a concurrent reader
+// sees either the old parent or the root, both ancestors.
 __global__ void cc_compress_kernel(uint32_t* label, uint32_t V) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x)
-    label[v] = cc_find(label, v);
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+    uint32_t x = v, p = __ldcg(&label[v]);
+    while (p != x) {
+      x = p;
+      p = __ldcg(&label[x]);
+    }
+    __stcg(&label[v], x);
+  }
 }
 
 // Step 2: roots of the endpoints of effective deletions (present before the
