@@ -1482,12 +1482,7 @@ struct StreamArgs {
 };
 
 // Order-independent 64-bit digest of dist[0, n): sum of splitmix64(v << 32 | dist[v]).
-__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
-  z += 0x9E3779B97F4A7C15ull;
-  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-  return z ^ (z >> 31);
-}
+using vxb::mix64;
 
 __device__ void digest_pass(const uint32_t* dist, uint32_t n, unsigned long long* out) {
   unsigned long long h = 0;

@@ -94,119 +94,218 @@ struct PushVisit {
   }
 };
 
-constexpr uint32_t kMrHead = 8;       // in-arcs a lane pulls itself before its warp helps
-constexpr uint32_t kMrStep = 4;       // of which it loads this many at a time
-constexpr uint32_t kMrBigRow = 4096;  // push rows this long are expanded by the whole grid
-
-// Pull level: one warp per 32 vertices.  Each lane ORs the frontier words of
-// the first kMrHead in-neighbours of its vertex; the rest of a longer row is
-// read by the whole warp, 32 arcs per step, the words OR-reduced across the
-// warp, until every root has reached the vertex or the row ends.
+// arc slots a lane loads per round of a pull group (fewer when every arc
+// brings more frontier words into registers)
 template <uint32_t W>
-__device__ void pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, uint32_t level, uint32_t* qn,
-                           uint32_t* qout) {
+struct MrSlots {
+  static constexpr uint32_t value = W <= 2 ? 8 : 4;
+};
+constexpr uint32_t kMrBigRow = 4096;     // push rows this long are expanded by the whole grid
+constexpr uint32_t kMrBigPull = 2048;    // pull rows this long are read by the whole grid
+constexpr uint32_t kMrWarps = kThreads / 32;
+
+// Per-warp staging of one pull group: the rows of its 32 vertices and their
+// OR accumulators ([lane][word]).
+struct MrWarpStage {
+  uint64_t rb[32];
+  uint32_t nb[32];
+  uint32_t dx[32];
+  uint32_t acc[32 * 8];
+};
+
+// Newly reached roots of the warp's 32 consecutive vertices (v = base + lane)
+// at distance lvl, one root at a time, so every store of a root's row covers
+// the warp's vertices together.
+template <uint32_t W>
+__device__ __forceinline__ void write_dists_warp(const MrParams& p, uint32_t v, const uint32_t* acc, uint32_t lvl) {
+#pragma unroll
+  for (uint32_t w = 0; w < W; ++w) {
+    uint32_t roots = __reduce_or_sync(FULL, acc[w]);
+    while (roots) {
+      const uint32_t b = __ffs(roots) - 1;
+      roots &= roots - 1;
+      if ((acc[w] >> b) & 1u) p.dist[(size_t)(32 * w + b) * p.V + v] = lvl;
+    }
+  }
+}
+
+// Pull level.  Warps take groups of 32 consecutive vertices from a counter.
+// The in-rows of a group's vertices that some root has not reached yet are
+// read as one flattened arc list: each round, every lane loads MrSlots<W> arcs (a
+// lane finds the owner of its arc by a binary search over the group's
+// inclusive row ends), then their frontier words, and ORs them into the
+// owner's accumulator in shared memory; an owner that every root has reached
+// stops being read.  Rows of kMrBigPull arcs or more are listed and read by
+// the whole grid afterwards, with the words OR-ed into nxt (zero outside push
+// levels).  Ends with a grid barrier; returns false when one failed.
+template <uint32_t W>
+__device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, uint32_t level, uint32_t* gnext,
+                           uint32_t* nbig, uint32_t* qn, uint32_t* qout, MrWarpStage& ws) {
+  constexpr uint32_t kMrU = MrSlots<W>::value;
   const DevAdj& a = p.g.in;
-  const int lane = threadIdx.x & 31;
-  for (uint32_t base = gwarp() * 32; base < p.V; base += nwarps() * 32) {
+  const uint32_t lane = threadIdx.x & 31;
+  for (;;) {
+    uint32_t grp = 0;
+    if (lane == 0) grp = atomicAdd(gnext, 1u);
+    const uint32_t base = __shfl_sync(FULL, grp, 0) * 32;
+    if (base >= p.V) break;
     const uint32_t v = base + lane;
-    uint32_t vis[W], acc[W];
+    uint32_t vis[W];
     bool done = true;
 #pragma unroll
     for (uint32_t w = 0; w < W; ++w) {
       vis[w] = v < p.V ? p.vis[(size_t)v * W + w] : word_mask(p, w);
-      acc[w] = 0;
       done = done && vis[w] == word_mask(p, w);
+      ws.acc[lane * W + w] = 0u;
     }
-    const bool todo = !done;
-    uint64_t b = 0, e = 0;
-    uint2 dr = make_uint2(0, 0);
-    if (todo) {
+    uint32_t len = 0;
+    if (!done) {
+      uint64_t b, e;
       vxb::base_range(a, v, b, e);
-      dr = a.drow[v];
+      const uint2 dr = a.drow[v];
+      const uint32_t nb = (uint32_t)(e - b);
+      len = nb + dr.y;
+      if (len >= kMrBigPull) {  // the whole grid reads it after the barrier
+        p.big[atomicAdd(nbig, 1u)] = v;
+        len = 0;
+      }
+      ws.rb[lane] = b;
+      ws.nb[lane] = nb;
+      ws.dx[lane] = dr.x;
     }
-    const uint32_t nb = (uint32_t)(e - b), total = nb + dr.y;
-    const uint32_t head = todo ? min(total, kMrHead) : 0u;
-    // the head in steps of kMrStep arcs: the step's column loads issue
-    // together, then its frontier-word loads, so a step costs two dependent
-    // round trips instead of two per arc
-    for (uint32_t j0 = 0; j0 < head && !done; j0 += kMrStep) {
-      uint32_t x[kMrStep];
+    uint32_t incl = len;
 #pragma unroll
-      for (uint32_t k = 0; k < kMrStep; ++k) {
-        const uint32_t j = j0 + k;
-        x[k] = j >= head ? kTomb : (j < nb ? a.col[b + j] : a.darena[dr.x + (j - nb)]);
-      }
-#pragma unroll
-      for (uint32_t w = 0; w < W; ++w) {
-        uint32_t m = 0;
-#pragma unroll
-        for (uint32_t k = 0; k < kMrStep; ++k)
-          if (!(x[k] & kTomb)) m |= fc[(size_t)x[k] * W + w];
-        acc[w] |= m & ~vis[w];
-      }
-      done = true;
-#pragma unroll
-      for (uint32_t w = 0; w < W; ++w) done = done && (vis[w] | acc[w]) == word_mask(p, w);
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+      const uint32_t t = __shfl_up_sync(FULL, incl, d);
+      if (lane >= d) incl += t;
     }
-    uint32_t longm = __ballot_sync(FULL, todo && !done && total > head);
-    while (longm) {
-      const int l = __ffs(longm) - 1;
-      longm &= longm - 1;
-      const uint64_t bb = __shfl_sync(FULL, b, l);
-      const uint32_t nbl = __shfl_sync(FULL, nb, l), tot = __shfl_sync(FULL, total, l);
-      const uint32_t dx = __shfl_sync(FULL, dr.x, l);
-      uint32_t vl[W], al[W];
+    const uint32_t T = __shfl_sync(FULL, incl, 31);
+    uint32_t active = __ballot_sync(FULL, len > 0);
+    __syncwarp();
+    for (uint32_t j0 = 0; j0 < T && active; j0 += 32 * kMrU) {
+      uint32_t x[kMrU], own[kMrU];
 #pragma unroll
-      for (uint32_t w = 0; w < W; ++w) {
-        vl[w] = __shfl_sync(FULL, vis[w], l);
-        al[w] = __shfl_sync(FULL, acc[w], l);
-      }
-      bool full = false;
-      for (uint32_t k0 = kMrHead; k0 < tot && !full; k0 += 32) {
-        const uint32_t k = k0 + lane;
-        uint32_t add[W];
+      for (uint32_t u = 0; u < kMrU; ++u) {
+        const uint32_t j = j0 + u * 32 + lane;
+        // owner = lanes whose row ends at or before j; the last end found is
+        // where the owner's row starts in the flattened list
+        uint32_t o = 0, lo = 0;
 #pragma unroll
-        for (uint32_t w = 0; w < W; ++w) add[w] = 0;
-        if (k < tot) {
-          uint32_t x = 0;
-          bool valid = true;
-          if (k < nbl) {
-            x = a.col[bb + k];
-            valid = !(x & kTomb);
-          } else {
-            x = a.darena[dx + (k - nbl)];
+        for (uint32_t step = 16; step >= 1; step >>= 1) {
+          const uint32_t t = __shfl_sync(FULL, incl, o + step - 1);
+          if (t <= j) {
+            o += step;
+            lo = t;
           }
-          if (valid)
-#pragma unroll
-            for (uint32_t w = 0; w < W; ++w) add[w] = fc[(size_t)(x & kIdMask) * W + w];
         }
-        full = true;
-#pragma unroll
-        for (uint32_t w = 0; w < W; ++w) {
-          al[w] |= __reduce_or_sync(FULL, add[w]) & ~vl[w];
-          full = full && (vl[w] | al[w]) == word_mask(p, w);
+        own[u] = o;
+        x[u] = kTomb;
+        if (j < T && ((active >> o) & 1u)) {
+          const uint32_t k = j - lo, nbo = ws.nb[o];
+          x[u] = k < nbo ? a.col[ws.rb[o] + k] : a.darena[ws.dx[o] + (k - nbo)];
         }
       }
-      if (lane == l)
+      uint32_t m[kMrU][W];
 #pragma unroll
-        for (uint32_t w = 0; w < W; ++w) acc[w] = al[w];
+      for (uint32_t u = 0; u < kMrU; ++u)
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w) m[u][w] = (x[u] & kTomb) ? 0u : fc[(size_t)x[u] * W + w];
+#pragma unroll
+      for (uint32_t u = 0; u < kMrU; ++u)
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w)
+          if (m[u][w]) atomicOr(&ws.acc[own[u] * W + w], m[u][w]);
+      __syncwarp();
+      bool fin = false;
+      if ((active >> lane) & 1u) {
+        fin = true;
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w) fin = fin && (vis[w] | ws.acc[lane * W + w]) == word_mask(p, w);
+      }
+      active &= ~__ballot_sync(FULL, fin);
     }
+    __syncwarp();
+    uint32_t acc[W];
     bool any = false;
 #pragma unroll
     for (uint32_t w = 0; w < W; ++w) {
-      if (!todo || !acc[w]) continue;
-      any = true;
-      p.vis[(size_t)v * W + w] = vis[w] | acc[w];
-      fn[(size_t)v * W + w] = acc[w];
-      write_dists(p, v, w, acc[w], level + 1);
+      acc[w] = ws.acc[lane * W + w] & ~vis[w];
+      if (acc[w]) {
+        any = true;
+        p.vis[(size_t)v * W + w] = vis[w] | acc[w];
+        fn[(size_t)v * W + w] = acc[w];
+      }
     }
+    write_dists_warp<W>(p, v, acc, level + 1);
     const uint32_t slot = vxb::warp_append(any, qn);
     if (any) qout[slot] = v;
+    __syncwarp();  // the next group overwrites the stage
   }
+  if (!mr_sync(p)) return false;
+  const uint32_t nb = __ldcg(nbig);
+  if (nb == 0) return true;
+  // long rows: every warp takes 32 * MrSlots<W>-arc slices; the slices of row r
+  // start at warp r (mod the warp count) so the rows spread over the grid
+  const uint32_t nw = nwarps(), gw = gwarp();
+  for (uint32_t r = 0; r < nb; ++r) {
+    const uint32_t v = p.big[r];
+    uint32_t vis[W];
+#pragma unroll
+    for (uint32_t w = 0; w < W; ++w) vis[w] = __ldcg(&p.vis[(size_t)v * W + w]);
+    uint64_t b, e;
+    vxb::base_range(a, v, b, e);
+    const uint2 dr = a.drow[v];
+    const uint32_t nbv = (uint32_t)(e - b), total = nbv + dr.y;
+    const uint32_t nslices = (total + 32 * kMrU - 1) / (32 * kMrU);
+    for (uint32_t s = (gw + nw - r % nw) % nw; s < nslices; s += nw) {
+      bool full = true;
+#pragma unroll
+      for (uint32_t w = 0; w < W; ++w) full = full && (vis[w] | __ldcg(&p.nxt[(size_t)v * W + w])) == word_mask(p, w);
+      if (full) break;
+      uint32_t x[kMrU];
+#pragma unroll
+      for (uint32_t u = 0; u < kMrU; ++u) {
+        const uint32_t k = s * 32 * kMrU + u * 32 + lane;
+        x[u] = k >= total ? kTomb : (k < nbv ? a.col[b + k] : a.darena[dr.x + (k - nbv)]);
+      }
+      uint32_t add[W];
+#pragma unroll
+      for (uint32_t w = 0; w < W; ++w) add[w] = 0u;
+#pragma unroll
+      for (uint32_t u = 0; u < kMrU; ++u)
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w)
+          if (!(x[u] & kTomb)) add[w] |= fc[(size_t)x[u] * W + w];
+#pragma unroll
+      for (uint32_t w = 0; w < W; ++w) {
+        const uint32_t red = __reduce_or_sync(FULL, add[w]) & ~vis[w];
+        if (lane == 0 && red) atomicOr(&p.nxt[(size_t)v * W + w], red);
+      }
+    }
+  }
+  if (!mr_sync(p)) return false;
+  for (uint32_t r = gtid(); r < nb; r += nthreads()) {
+    const uint32_t v = p.big[r];
+    bool any = false;
+#pragma unroll
+    for (uint32_t w = 0; w < W; ++w) {
+      const size_t o = (size_t)v * W + w;
+      const uint32_t m = __ldcg(&p.nxt[o]) & ~p.vis[o];
+      p.nxt[o] = 0u;
+      if (!m) continue;
+      any = true;
+      p.vis[o] |= m;
+      fn[o] = m;
+      write_dists(p, v, w, m, level + 1);
+    }
+    if (any) qout[atomicAdd(qn, 1u)] = v;
+  }
+  return mr_sync(p);
 }
 
 template <uint32_t W>
 __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
+  __shared__ MrWarpStage stage[kMrWarps];
   MrCounters* c = p.c;
   // roots (queued once per distinct vertex)
   for (uint32_t r = gtid(); r < p.K; r += nthreads()) {
@@ -235,6 +334,7 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
       c->qn[clr] = 0;
       c->tn[clr] = 0;
       c->nbig[clr] = 0;
+      c->gnext[clr] = 0;
     }
     // frontier words of level-1 are no longer read: clear them for reuse,
     // through its queue when it was small, else all of them with plain stores
@@ -248,8 +348,8 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
     if ((float)n_f > p.pull_frac * (float)p.V) {
       // pull: every vertex not reached by all roots ORs its in-neighbours'
       // frontier words, stopping once all roots reached it
-      pull_level<W>(p, fc, fn, level, &c->qn[nx], p.q[nx]);
-      if (!mr_sync(p)) return;
+      if (!pull_level<W>(p, fc, fn, level, &c->gnext[cur], &c->nbig[cur], &c->qn[nx], p.q[nx], stage[threadIdx.x >> 5]))
+        return;
     } else {
       // push along the rows of the queued frontier vertices, one warp each
       const DevAdj& a = p.g.out;

@@ -16,7 +16,8 @@ struct MrCounters {
   // block has already started for the current level.
   uint32_t qn[3];    // frontier queue lengths
   uint32_t tn[3];    // touched heads of a push level
-  uint32_t nbig[3];  // frontier rows of a push level long enough for the whole grid
+  uint32_t nbig[3];  // rows of a level long enough for the whole grid
+  uint32_t gnext[3]; // next 32-vertex group of a pull level
   uint32_t levels;
   uint32_t err;
   unsigned long long arcs;  // reached-arc total (mrbfs_reached_arcs)

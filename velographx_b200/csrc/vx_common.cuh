@@ -86,6 +86,16 @@ __device__ __forceinline__ T warp_max(T v) {
   return v;
 }
 
+// splitmix64's finaliser (Steele, Lea and Flood, "Fast splittable
+// pseudorandom number generators", OOPSLA 2014): the per-entry hash of the
+// distance digests, sum over v of mix64(v << 32 | dist[v]) modulo 2^64.
+__host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
 // Warp-aggregated append: every lane with `pred` gets a unique slot in
 // list[0..*count).  Returns the lane's slot (or UINT32_MAX when !pred).
 __device__ __forceinline__ uint32_t warp_append(bool pred, uint32_t* count) {
