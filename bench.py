@@ -273,6 +273,8 @@ def run_b200(args, rank, world, local):
         b_noshare = float((4.0 * np.asarray([marcs / max(1, k)]) + 8.0 * (V + 1) + 4.0 * V)[0]) * k
         multiroot[str(k)] = {"ms": ms, "ms_runs": [round(x, 3) for x in runs],
                              "gteps": marcs / 2 / (ms * 1e-3) / 1e9, "levels": mr.levels,
+                             "level_trace_us_nf_dir": [[round(us, 1), int(nf), "pull" if pull else "push"]
+                                                       for us, nf, pull in mr.level_trace()],
                              "algorithmic_bytes_bitparallel": b_bitpar,
                              "achieved_gbs_bitparallel": b_bitpar / (ms * 1e-3) / 1e9,
                              "algorithmic_bytes_no_sharing": b_noshare,

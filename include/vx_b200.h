@@ -190,13 +190,20 @@ int vx_bfs_phase_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
 /* A stream of update batches applied in order, with the same result after
  * every batch as vx_bfs_apply on each: batch t is ops [offsets[t],
  * offsets[t+1]) of the host arrays (offsets[0] == 0, nbatches + 1 entries).
- * Undirected graphs run the whole stream in one persistent launch after one
- * upload and one stream-wide canonicalisation; other streams are applied
- * batch by batch.  Optional host outputs: digests[t] = vx_bfs_digest after
- * batch t; stats[4t..4t+3] = {last_deletion_candidates,
- * last_affected_vertices, last_used_full_recompute, reachable_count mod
- * 2^32} after batch t.  The reference applies batches one call at a time
- * (bfs.hpp:29-98); this entry has no counterpart there. */
+ * Undirected graphs: without stats, every batch but the last goes through
+ * version-parallel windows (vx_bfs_set_stream_window): each window's batches
+ * are answered together by one bit-parallel BFS over the window's graph
+ * versions, then committed to the graph as one merged batch; the last batch
+ * goes through the update launch, so that the repair counters after the call
+ * are its own.  With stats, the whole stream runs in one persistent update
+ * launch after one upload and one stream-wide canonicalisation.  Directed
+ * graphs are applied batch by batch.  The distances after every batch, the
+ * graph and its version count are the same on every route.  Optional host
+ * outputs: digests[t] = vx_bfs_digest after batch t; stats[4t..4t+3] =
+ * {last_deletion_candidates, last_affected_vertices,
+ * last_used_full_recompute, reachable_count mod 2^32} after batch t.  The
+ * reference applies batches one call at a time (bfs.hpp:29-98); this entry
+ * has no counterpart there. */
 int vx_bfs_apply_stream(vx_bfs* b, const uint32_t* src, const uint32_t* dst, const uint8_t* add,
                         const uint64_t* offsets, size_t nbatches, uint64_t* digests, uint32_t* stats);
 /* Order-independent 64-bit digest of the current distances: the sum over v of
@@ -239,6 +246,11 @@ int vx_bfs_accounting(vx_bfs* b, uint64_t* out5);
  * barriers and the work ring's polling.  Results are the same for every
  * value.  No reference counterpart. */
 int vx_bfs_set_update_blocks(vx_bfs* b, uint32_t blocks);
+/* Batches per version-parallel window of vx_bfs_apply_stream (1..256,
+ * default 64; larger values are clamped to 256); 0 sends every batch through
+ * the persistent update launch.  Same results for every value.  No reference
+ * counterpart. */
+int vx_bfs_set_stream_window(vx_bfs* b, uint32_t batches);
 /* fused != 0 (default): an undirected batch's commit and repair run in one
  * persistent launch after staging; 0: the per-phase path (a launch per commit
  * step and for each half of the repair) -- the plain baseline the batched
@@ -283,6 +295,11 @@ int vx_mrbfs_distances_device(vx_mrbfs* m, const uint32_t** d_dist, size_t* n);
  * level count of the last run. */
 int vx_mrbfs_reached_arcs(vx_mrbfs* m, uint64_t* out);
 int vx_mrbfs_levels(vx_mrbfs* m, uint32_t* out);
+/* Level trace of the last run: for each level (up to 64) its start time in
+ * ns and its frontier size with bit 63 set for a pull level, then a closing
+ * timestamp; copies min(cap, *n) values, *n = 2 * levels + 1.  No reference
+ * counterpart (diagnostics). */
+int vx_mrbfs_level_trace(vx_mrbfs* m, uint64_t* out, size_t cap, size_t* n);
 /* Pull (bottom-up) when the frontier holds more than frac * V vertices. */
 int vx_mrbfs_set_pull_fraction(vx_mrbfs* m, float frac);
 /* One-shot form: create, run, copy k*V distances into out (cap entries). */

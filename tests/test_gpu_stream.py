@@ -12,7 +12,8 @@ import numpy as np
 import pytest
 
 from oracle import OracleBFS, OracleGraph
-from tests.helpers import fallback_limit
+from tests.helpers import fallback_limit, messy_stream
+from tests.helpers import splitmix_digest as digest
 
 pytestmark = pytest.mark.gpu
 
@@ -22,42 +23,6 @@ if not torch.cuda.is_available():
 
 import velographx_b200 as vx  # noqa: E402
 import workloads as w  # noqa: E402
-
-
-def mix64(z: np.ndarray) -> np.ndarray:
-    """splitmix64 finaliser on uint64 arrays (wrapping arithmetic)."""
-    with np.errstate(over="ignore"):
-        z = z + np.uint64(0x9E3779B97F4A7C15)
-        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
-        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
-        return z ^ (z >> np.uint64(31))
-
-
-def digest(dist: np.ndarray) -> int:
-    v = np.arange(dist.size, dtype=np.uint64)
-    h = mix64((v << np.uint64(32)) | dist.astype(np.uint64))
-    with np.errstate(over="ignore"):
-        return int(np.sum(h, dtype=np.uint64))
-
-
-def messy_stream(edges, V, sizes, seed, grow=0):
-    """mixed_stream plus duplicates, self-loops and (optionally) ids past V."""
-    rng = np.random.default_rng(seed)
-    st = w.mixed_stream(edges, V, sizes, 0.6, seed=seed)
-    src, dst, add = st.src.copy(), st.dst.copy(), st.add.copy()
-    n = src.size
-    if n:
-        k = max(1, n // 20)
-        i = rng.integers(0, n, k)
-        j = rng.integers(0, n, k)
-        src[i], dst[i] = src[j], dst[j]  # repeated arcs, mixed ops
-        add[i] = rng.integers(0, 2, k).astype(np.uint8)
-        loops = rng.integers(0, n, max(1, n // 50))
-        dst[loops] = src[loops]
-        if grow:
-            g_ = rng.integers(0, n, max(1, n // 100))
-            dst[g_] = rng.integers(V, V + grow, g_.size).astype(np.uint32)
-    return src, dst, add, st.offsets.astype(np.uint64)
 
 
 def test_digest_matches_numpy():

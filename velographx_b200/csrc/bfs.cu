@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "bfs.cuh"
+#include "vstream.cuh"
 #include "graph_dev.cuh"
 #include "frontier.cuh"
 
@@ -2109,9 +2110,12 @@ void bfs_destroy(Bfs* b) {
   cudaFree(b->rq);
   cudaFree(b->ring);
   b->sb.free_all();
+  delete b->vb;
   cudaFreeHost(b->hctr);
   delete b;
 }
+
+int bfs_ensure_capacity(Bfs* b, size_t V) { return ensure_capacity(b, V); }
 
 int bfs_recompute(Bfs* b) {
   Graph* g = b->g;
@@ -2426,14 +2430,11 @@ int StreamBufs::ensure(size_t n, size_t nb, size_t maxf) {
 }
 
 int bfs_apply_stream(Bfs* b, const uint32_t* hs, const uint32_t* hd, const uint8_t* ha, const uint64_t* hoff,
-                     size_t nb, uint64_t* digests, uint32_t* stats, int* done) {
+                     size_t nb, uint64_t* digests, uint32_t* stats, size_t* applied) {
   Graph* g = b->g;
   cudaStream_t st = g->stream;
-  *done = 0;
-  if (nb == 0) {
-    *done = 1;
-    return 0;
-  }
+  *applied = 0;
+  if (nb == 0) return 0;
   if (hoff[0] != 0) {
     set_error("batch offsets must start at 0");
     return -1;
@@ -2469,6 +2470,35 @@ int bfs_apply_stream(Bfs* b, const uint32_t* hs, const uint32_t* hd, const uint8
   while (bbits < 32 && ((size_t)1 << bbits) < std::max<size_t>(V, 2)) ++bbits;
   int tbits = 1;
   while (tbits < 40 && ((size_t)1 << tbits) < nb) ++tbits;
+  const uint32_t window = std::min<uint32_t>(b->tune.stream_window, kMaxVersions);
+  if (!stats && window && !g->directed && nb >= 2 && 2 * bbits + 8 <= 64 && n < (1ull << 31)) {
+    // every batch but the last in version-parallel windows
+    StreamBufs& S = b->sb;
+    if (int rc = S.ensure(n, nb, maxf)) return rc;
+    VX_CUDA_TRY(cudaMemcpyAsync(S.src, hs, n * 4, cudaMemcpyHostToDevice, st));
+    VX_CUDA_TRY(cudaMemcpyAsync(S.dst, hd, n * 4, cudaMemcpyHostToDevice, st));
+    VX_CUDA_TRY(cudaMemcpyAsync(S.add, ha, n, cudaMemcpyHostToDevice, st));
+    // every window's buffers up front, so that no window allocates
+    size_t wops = 0;
+    for (size_t t0 = 0; t0 + 1 < nb; t0 += window)
+      wops = std::max<size_t>(wops, hoff[std::min<size_t>(t0 + window, nb - 1)] - hoff[t0]);
+    if (int rc = stream_versions_reserve(b, wops, std::max<size_t>(b->dist_len, vpost[nb - 2]),
+                                         std::min<size_t>(window, nb - 1)))
+      return rc;
+    for (size_t t0 = 0; t0 + 1 < nb; t0 += window) {
+      const size_t t1 = std::min<size_t>(t0 + window, nb - 1);
+      if (int rc = stream_versions(b, S.src, S.dst, S.add, hoff, vpost.data(), t0, t1, digests)) return rc;
+      *applied = t1;
+    }
+    const uint64_t tail[2] = {0, hoff[nb] - hoff[nb - 1]};
+    const uint64_t lo = hoff[nb - 1];
+    size_t last = 0;
+    if (int rc = bfs_apply_stream(b, hs + lo, hd + lo, ha + lo, tail, 1, digests ? digests + nb - 1 : nullptr,
+                                  nullptr, &last))
+      return rc;
+    *applied += last;
+    return 0;
+  }
   // the persistent path covers undirected graphs whose (batch, u, v) keys fit
   // 64 bits and whose arena takes the whole stream; the caller loops otherwise
   if (g->directed || 2 * bbits + tbits > 64 || n >= (1ull << 31)) return 0;
@@ -2534,7 +2564,7 @@ int bfs_apply_stream(Bfs* b, const uint32_t* hs, const uint32_t* hd, const uint8
   if (digests) VX_CUDA_TRY(cudaMemcpyAsync(digests, S.digest, nb * 8, cudaMemcpyDeviceToHost, st));
   if (stats) VX_CUDA_TRY(cudaMemcpyAsync(stats, S.bstats, nb * 16, cudaMemcpyDeviceToHost, st));
   if (digests || stats) VX_CUDA_TRY(cudaStreamSynchronize(st));
-  *done = 1;
+  *applied = nb;
   return 0;
 }
 

@@ -51,7 +51,12 @@ struct BfsTuning {
   uint32_t large_row = 1024; // rows this long are expanded by the whole grid
   bool fused = true;         // undirected batches: one persistent launch after staging
   uint32_t update_blocks = 0;  // blocks of the update launch (0: every co-resident block)
+  // batches per version-parallel window of a stream whose per-batch repair
+  // counters are not asked for (0: every batch by the update launch)
+  uint32_t stream_window = 64;
 };
+
+struct VersionBufs;
 
 // Device buffers of the batched stream path (kept between calls).
 struct StreamBufs {
@@ -105,6 +110,7 @@ struct Bfs {
   unsigned long long* acct = nullptr;  // algorithmic-byte accounting (5 counters), when on
   bool acct_on = false;
   StreamBufs sb;
+  VersionBufs* vb = nullptr;  // version-parallel stream buffers, made on first use
 };
 
 int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac);
@@ -135,13 +141,18 @@ int bfs_reached_arcs(Bfs* b, unsigned long long* arcs);  // sum of degrees of re
 int bfs_level_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n);
 int bfs_phase_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n);
 // The batches [hoff[t], hoff[t+1]) of host arrays (hoff[0] == 0) applied in
-// order in one persistent launch; *done = 0 when the stream is not one the
-// persistent path takes (directed graph, keys past 64 bits, arena), and the
-// caller then applies the batches one by one.  digests / stats (optional,
-// host) receive the distance digest and {candidates, affected, full,
-// reachable} after every batch.
+// order.  Undirected streams: without stats, every batch but the last in
+// version-parallel windows of tune.stream_window batches, the last one (so
+// that the object's repair counters are its own) by the update launch;
+// otherwise all of them in one persistent update launch.  *applied = the
+// number of leading batches applied; the caller applies the rest one by one
+// (directed graphs, keys past 64 bits, an arena the stream does not fit).
+// digests / stats (optional, host) receive the distance digest and
+// {candidates, affected, full, reachable} after every batch.
 int bfs_apply_stream(Bfs* b, const uint32_t* hs, const uint32_t* hd, const uint8_t* ha, const uint64_t* hoff,
-                     size_t nb, uint64_t* digests, uint32_t* stats, int* done);
+                     size_t nb, uint64_t* digests, uint32_t* stats, size_t* applied);
+// Distance, bitmap and list buffers for V vertices.
+int bfs_ensure_capacity(Bfs* b, size_t V);
 // Order-independent digest of the current distances: the sum over v of
 // splitmix64(v << 32 | dist[v]) modulo 2^64.
 int bfs_digest(Bfs* b, uint64_t* out);

@@ -8,6 +8,7 @@
 
 #include "../../include/vx_b200.h"
 #include "bfs.cuh"
+#include "vstream.cuh"
 #include "components.cuh"
 #include "graph.cuh"
 #include "io.cuh"
@@ -392,10 +393,9 @@ int vx_bfs_apply_stream(vx_bfs* b, const uint32_t* src, const uint32_t* dst, con
                         const uint64_t* offsets, size_t nbatches, uint64_t* digests, uint32_t* stats) {
   if (!b || !offsets || (nbatches && offsets[nbatches] && (!src || !dst || !add)))
     return fail(VX_ERR_INVALID, "null argument");
-  int done = 0;
-  if (int rc = vxh::bfs_apply_stream(b->b, src, dst, add, offsets, nbatches, digests, stats, &done)) return rc;
-  if (done) return VX_OK;
-  for (size_t t = 0; t < nbatches; ++t) {
+  size_t applied = 0;
+  if (int rc = vxh::bfs_apply_stream(b->b, src, dst, add, offsets, nbatches, digests, stats, &applied)) return rc;
+  for (size_t t = applied; t < nbatches; ++t) {
     const uint64_t lo = offsets[t];
     if (int rc = vx_bfs_apply(b, src + lo, dst + lo, add + lo, offsets[t + 1] - lo)) return rc;
     if (digests)
@@ -429,7 +429,11 @@ int vx_graph_reserve(vx_graph* g, size_t max_batch_ops, size_t total_ops) {
 
 int vx_bfs_reserve_stream(vx_bfs* b, size_t ops, size_t batches, size_t max_batch_ops) {
   if (!b) return fail(VX_ERR_INVALID, "null argument");
-  return b->b->sb.ensure(ops, batches, 2 * std::max<size_t>(max_batch_ops, 1));
+  if (int rc = b->b->sb.ensure(ops, batches, 2 * std::max<size_t>(max_batch_ops, 1))) return rc;
+  const size_t window = std::min<size_t>(b->b->tune.stream_window, batches);
+  if (window == 0 || b->b->g->directed) return VX_OK;
+  const size_t wops = std::min<size_t>(ops, window * std::max<size_t>(max_batch_ops, 1));
+  return vxh::stream_versions_reserve(b->b, wops, b->b->g->V, window);
 }
 
 int vx_bfs_digest(vx_bfs* b, uint64_t* out) {
@@ -476,6 +480,12 @@ int vx_bfs_accounting(vx_bfs* b, uint64_t* out5) {
 int vx_bfs_set_update_blocks(vx_bfs* b, uint32_t blocks) {
   if (!b) return fail(VX_ERR_INVALID, "null argument");
   b->b->tune.update_blocks = blocks;
+  return VX_OK;
+}
+
+int vx_bfs_set_stream_window(vx_bfs* b, uint32_t batches) {
+  if (!b) return fail(VX_ERR_INVALID, "null argument");
+  b->b->tune.stream_window = batches;
   return VX_OK;
 }
 
@@ -574,6 +584,11 @@ int vx_mrbfs_levels(vx_mrbfs* m, uint32_t* out) {
   if (int rc = vxh::mrbfs_sync(m->m)) return rc;
   *out = m->m->hctr->levels;
   return VX_OK;
+}
+
+int vx_mrbfs_level_trace(vx_mrbfs* m, uint64_t* out, size_t cap, size_t* n) {
+  if (!m || !n || (cap && !out)) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::mrbfs_level_trace(m->m, reinterpret_cast<unsigned long long*>(out), cap, n);
 }
 
 int vx_mrbfs_set_pull_fraction(vx_mrbfs* m, float frac) {

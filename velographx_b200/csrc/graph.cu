@@ -818,9 +818,7 @@ static int scan_count(Graph* g, const uint32_t* flag, uint32_t* pos, size_t m, u
   return scan_exclusive_u32(flag, pos, m, total, g->scratch, g->stream);
 }
 
-int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound, bool classify) {
-  cudaStream_t s = g->stream;
-  BatchBuffers& B = g->batch;
+int graph_prepare_batch(Graph* g, size_t n, size_t vertex_bound) {
   g->batch_ops = n;
   if (vertex_bound > vxb::kMaxVertices) {
     set_error("vertex id beyond the supported maximum");
@@ -836,7 +834,14 @@ int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound, bool classify) {
     for (int d = 0; d < (g->directed ? 2 : 1); ++d)
       if (int rc = reserve_arena(g, g->adj[d], m, &consolidate)) return rc;
   }
-  if (int rc = graph_grow(g, std::max<size_t>(g->V, vertex_bound))) return rc;
+  return graph_grow(g, std::max<size_t>(g->V, vertex_bound));
+}
+
+int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound, bool classify) {
+  cudaStream_t s = g->stream;
+  BatchBuffers& B = g->batch;
+  const size_t m = g->directed ? n : 2 * n;
+  if (int rc = graph_prepare_batch(g, n, vertex_bound)) return rc;
   const int b = bits_for(std::max<size_t>(g->V, 2));
   if (n == 0) {  // a non-empty batch's staging sets these counts itself
     VX_CUDA_TRY(cudaMemsetAsync(&g->ctr->final_arcs, 0, 5 * sizeof(uint32_t), s));

@@ -108,6 +108,11 @@ int graph_bulk_load(Graph* g, const uint32_t* d_uv, size_t n_edges);
 // the pre-batch graph.  vertex_bound bounds every non-self-loop id + 1.
 // classify = false leaves the arcs unclassified (a fused repair classifies them itself).
 int graph_stage_batch(Graph* g, size_t n, size_t vertex_bound, bool classify = true);
+// The part of staging that precedes canonicalisation: arena room for a batch
+// of n ops (consolidating first when the arena would pass its limit) and the
+// vertex growth.  A caller that canonicalises and classifies the batch
+// itself fills batch.{fu,fv,ff,fpos} and ctr->final_arcs, then commits.
+int graph_prepare_batch(Graph* g, size_t n, size_t vertex_bound);
 // Apply the staged batch to the device structure (after any pre-batch reads):
 // removals first (tombstones, delta removals), then insertions.
 int graph_commit_batch(Graph* g);

@@ -103,6 +103,9 @@ struct MrSlots {
 constexpr uint32_t kMrBigRow = 4096;     // push rows this long are expanded by the whole grid
 constexpr uint32_t kMrBigPull = 2048;    // pull rows this long are read by the whole grid
 constexpr uint32_t kMrWarps = kThreads / 32;
+// 32-vertex groups a warp claims per atomic of a pull level (one counter
+// per level: a claim per group serialised on it)
+constexpr uint32_t kClaimGroups = 4;
 
 // Per-warp staging of one pull group: the rows of its 32 vertices and their
 // OR accumulators ([lane][word]).
@@ -144,10 +147,15 @@ __device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, 
   constexpr uint32_t kMrU = MrSlots<W>::value;
   const DevAdj& a = p.g.in;
   const uint32_t lane = threadIdx.x & 31;
+  uint32_t cur = 0, end = 0;  // the warp's claimed groups [cur, end), warp-uniform
   for (;;) {
-    uint32_t grp = 0;
-    if (lane == 0) grp = atomicAdd(gnext, 1u);
-    const uint32_t base = __shfl_sync(FULL, grp, 0) * 32;
+    if (cur == end) {
+      uint32_t c0 = 0;
+      if (lane == 0) c0 = atomicAdd(gnext, kClaimGroups);
+      cur = __shfl_sync(FULL, c0, 0);
+      end = cur + kClaimGroups;
+    }
+    const uint32_t base = cur++ * 32;
     if (base >= p.V) break;
     const uint32_t v = base + lane;
     uint32_t vis[W];
@@ -345,7 +353,13 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
     }
     const uint32_t* fc = p.frn[cur];
     uint32_t* fn = p.frn[nx];
-    if ((float)n_f > p.pull_frac * (float)p.V) {
+    const bool pull = (float)n_f > p.pull_frac * (float)p.V;
+    if (gtid() == 0) {
+      const uint32_t t = min(level, kMrTraceLevels - 1);
+      c->trace[2 * t] = globaltimer();
+      c->trace[2 * t + 1] = (unsigned long long)n_f | ((unsigned long long)pull << 63);
+    }
+    if (pull) {
       // pull: every vertex not reached by all roots ORs its in-neighbours'
       // frontier words, stopping once all roots reached it
       if (!pull_level<W>(p, fc, fn, level, &c->gnext[cur], &c->nbig[cur], &c->qn[nx], p.q[nx], stage[threadIdx.x >> 5]))
@@ -406,7 +420,10 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
     }
     prev_n = n_f;
   }
-  if (gtid() == 0) c->levels = level;
+  if (gtid() == 0) {
+    c->levels = level;
+    c->trace[2 * min(level, kMrTraceLevels)] = globaltimer();
+  }
 }
 
 __global__ void mr_arcs_kernel(vxb::DevAdj a, const uint32_t* dist, uint32_t V, uint32_t K,
@@ -531,6 +548,15 @@ int mrbfs_sync(MrBfs* m) {
     set_error("multi-root BFS device error word 0x%x", m->hctr->err);
     return -5;
   }
+  return 0;
+}
+
+int mrbfs_level_trace(MrBfs* m, unsigned long long* out, size_t cap, size_t* n) {
+  if (int rc = mrbfs_sync(m)) return rc;
+  const uint32_t levels = std::min<uint32_t>(m->hctr->levels, kMrTraceLevels);
+  *n = 2 * (size_t)levels + 1;
+  for (size_t i = 0; i < std::min(cap, *n); ++i)
+    out[i] = i + 1 == *n ? m->hctr->trace[2 * levels] : m->hctr->trace[i];
   return 0;
 }
 

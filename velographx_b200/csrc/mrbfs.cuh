@@ -9,6 +9,7 @@
 namespace vxh {
 
 constexpr uint32_t kMaxRoots = 256;
+constexpr uint32_t kMrTraceLevels = 64;  // levels with a trace entry (later ones share the last)
 
 struct MrCounters {
   // Per-level counters rotate over three slots (level % 3); a level's slots
@@ -21,6 +22,9 @@ struct MrCounters {
   uint32_t levels;
   uint32_t err;
   unsigned long long arcs;  // reached-arc total (mrbfs_reached_arcs)
+  // per level: globaltimer at its start, then its frontier size with bit 63
+  // set for a pull level; after the last level, the closing stamp
+  unsigned long long trace[2 * kMrTraceLevels + 1];
 };
 
 struct MrBfs {
@@ -47,5 +51,8 @@ void mrbfs_destroy(MrBfs* m);
 int mrbfs_run(MrBfs* m);   // enqueues the traversal on the graph's stream
 int mrbfs_sync(MrBfs* m);  // waits and checks the device error word
 int mrbfs_reached_arcs(MrBfs* m, unsigned long long* out);
+// The last run's level trace: {start ns, n_f | pull << 63} per level, then
+// the closing stamp; writes up to cap values, *n = the full count.
+int mrbfs_level_trace(MrBfs* m, unsigned long long* out, size_t cap, size_t* n);
 
 }  // namespace vxh

@@ -344,6 +344,10 @@ PYBIND11_MODULE(_velographx, m) {
            })
       .def("set_update_blocks",
            [](IncrementalBFS& x, std::uint32_t blocks) { detail::check(vx_bfs_set_update_blocks(x.handle(), blocks)); })
+      .def("set_stream_window",
+           [](IncrementalBFS& x, std::uint32_t batches) {
+             detail::check(vx_bfs_set_stream_window(x.handle(), batches));
+           })
       .def("digest",
            [](IncrementalBFS& x) {
              std::uint64_t d = 0;
@@ -433,6 +437,19 @@ PYBIND11_MODULE(_velographx, m) {
              std::uint64_t a = 0;
              detail::check(vx_mrbfs_reached_arcs(r.h, &a));
              return a;
+           })
+      .def("level_trace",
+           [](MultiRoot& r) {
+             std::size_t n = 0;
+             detail::check(vx_mrbfs_level_trace(r.h, nullptr, 0, &n));
+             std::vector<std::uint64_t> t(n);
+             if (n) detail::check(vx_mrbfs_level_trace(r.h, t.data(), n, &n));
+             py::list out;  // (us, frontier size, pull) per level
+             const std::size_t levels = n ? (n - 1) / 2 : 0;
+             for (std::size_t i = 0; i < levels; ++i)
+               out.append(py::make_tuple(static_cast<double>(t[2 * i + 2] - t[2 * i]) * 1e-3,
+                                         t[2 * i + 1] & 0x7FFFFFFFFFFFFFFFull, (t[2 * i + 1] >> 63) != 0));
+             return out;
            })
       .def_property_readonly("levels", [](MultiRoot& r) {
         std::uint32_t l = 0;

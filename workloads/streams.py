@@ -146,19 +146,30 @@ def grid(side: int = 4096, long_range: float = 0.001, batches: int = 500, ops: i
     g.bulk_load_edges(edges)
     g.reserve(ops, ops * batches)
     b = IncrementalBFS(g, root)
-    recs, stats = [], []
+    recs, stats, stamps = [], [], []
     for t in range(batches):
         b.apply_arrays(*stream.batch(t))
         st = b.stats()
         stats.append((bool(st["last_used_full_recompute"]), int(st["last_affected_vertices"]),
                       int(st["last_deletion_candidates"])))
+        stamps.append(b.phase_trace()[:7])
         if t < ref_batches:
             recs.append(record(g, b))
     del b, g
     slow = np.argsort(per)[::-1][:5]
     res["fallback_batches"] = int(sum(x[0] for x in stats))
+    def phases(ts):
+        # the update launch's stamps: batch start, after the removals, after
+        # the cascade, repair entry (after the insertions), after the
+        # invalidation, after the boundary seeds, after the relaxation (us,
+        # from the untimed replay of the same batch)
+        names = ("classify_removals", "cascade", "insertions", "invalidation", "boundary_seeds", "relaxation")
+        return {n: round((int(ts[k + 1]) - int(ts[k])) * 1e-3, 1) if ts[k + 1] >= ts[k] > 0 else None
+                for k, n in enumerate(names)}
+
     res["slowest"] = [{"batch": int(i), "us": round(float(per[i]), 1), "full_recompute": stats[i][0],
-                       "affected": stats[i][1], "candidates": stats[i][2]} for i in slow]
+                       "affected": stats[i][1], "candidates": stats[i][2], "replay_phase_us": phases(stamps[i])}
+                      for i in slow]
     res["affected_median"] = float(np.median([x[1] for x in stats]))
     if ref_batches:
         k = min(ref_batches, batches)
@@ -187,7 +198,7 @@ def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int 
     out = {"workload": f"rmat{scale}-undirected-ef16-{batches}x{ops}-insertions", "vertices": V, "root": int(root),
            "batches": batches}
     e0, e1 = _events()
-    plain_runs, batched_runs, same, phases = [], [], True, []
+    plain_runs, batched_runs, ul_runs, same, phases = [], [], [], True, []
     for _ in range(repeats):
         g = Graph(V, False)
         g.bulk_load_edges(edges)
@@ -204,22 +215,30 @@ def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int 
         e1.record(cs)
         torch.cuda.synchronize()
         plain_runs.append(batches / (e0.elapsed_time(e1) * 1e-3))
-        g2 = Graph(V, False)
-        g2.bulk_load_edges(edges)
-        g2.reserve(ops, ops * batches)
-        b2 = IncrementalBFS(g2, root)
-        b2.reserve_stream(batches * ops, batches, ops)
-        cs2 = torch.cuda.ExternalStream(g2.stream)
-        torch.cuda.synchronize()
-        e0.record(cs2)
-        digs, _ = b2.apply_stream(st.src, st.dst, st.add, off, digests=True)
-        e1.record(cs2)
-        torch.cuda.synchronize()
-        batched_runs.append(batches / (e0.elapsed_time(e1) * 1e-3))
-        same = same and [int(x) for x in digs] == [int(x) for x in plain_digests]
-        ph = b2.phase_trace()[21:27]
-        phases.append([x / 1e3 / batches for x in ph])
-        del b, g, b2, g2
+        # batched: version-parallel windows (the default route), then every
+        # batch through the persistent update launch (window 0); both return
+        # every batch's digest
+        for window, runs in ((None, batched_runs), (0, ul_runs)):
+            g2 = Graph(V, False)
+            g2.bulk_load_edges(edges)
+            g2.reserve(ops, ops * batches)
+            b2 = IncrementalBFS(g2, root)
+            b2.reserve_stream(batches * ops, batches, ops)
+            if window is not None:
+                b2.set_stream_window(window)
+            cs2 = torch.cuda.ExternalStream(g2.stream)
+            torch.cuda.synchronize()
+            e0.record(cs2)
+            digs, _ = b2.apply_stream(st.src, st.dst, st.add, off, digests=True)
+            e1.record(cs2)
+            torch.cuda.synchronize()
+            runs.append(batches / (e0.elapsed_time(e1) * 1e-3))
+            same = same and [int(x) for x in digs] == [int(x) for x in plain_digests]
+            if window == 0:
+                ph = b2.phase_trace()[21:27]
+                phases.append([x / 1e3 / batches for x in ph])
+            del b2, g2
+        del b, g
     # the records of every batch, on one more replica (untimed)
     g = Graph(V, False)
     g.bulk_load_edges(edges)
@@ -231,9 +250,13 @@ def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int 
     del b, g
     out["plain"] = {"batches_per_s": float(np.median(plain_runs)), "runs": [round(x) for x in plain_runs]}
     out["batched"] = {"batches_per_s": float(np.median(batched_runs)), "runs": [round(x) for x in batched_runs],
-                      "phase_us_per_batch": dict(zip(
-                          ["classify", "removals", "cascade", "insertions", "post_repair", "end_barrier"],
-                          [round(float(np.median([r[k] for r in phases])), 2) for k in range(6)]))}
+                      "route": "version-parallel windows of 64 batches (digest of every batch returned)"}
+    out["batched_update_launch"] = {
+        "batches_per_s": float(np.median(ul_runs)), "runs": [round(x) for x in ul_runs],
+        "route": "every batch in one persistent update launch (stream window 0)",
+        "phase_us_per_batch": dict(zip(
+            ["classify", "removals", "cascade", "insertions", "post_repair", "end_barrier"],
+            [round(float(np.median([r[k] for r in phases])), 2) for k in range(6)]))}
     out["plain_equals_batched"] = bool(same)
     out["_check"] = (edges, st, root, recs)
     return out
@@ -295,29 +318,47 @@ def lognormal(scale: int = 20, batches: int = 1000, median: float = 500.0, sigma
                      "runs_batches_per_s": [round(batches / r[0]) for r in runs]}
         if fused:
             bp_fused = bp
-    # batched: the whole stream in one call, distances resident on the device at the end
-    gb, bb = replica()
-    cs = torch.cuda.ExternalStream(gb.stream)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e0.record(cs)
-    bb.apply_stream(st.src, st.dst, st.add, off)
-    e1.record(cs)
-    torch.cuda.synchronize()
-    out["batched"] = {"seconds": e0.elapsed_time(e1) * 1e-3, "wall_s": time.perf_counter() - t0}
-    out["batched"]["batches_per_s"] = batches / out["batched"]["seconds"]
-    ph = bb.phase_trace()[21:27]
-    out["batched"]["phase_us_per_batch"] = dict(zip(
-        ["classify", "removals", "cascade", "insertions", "post_repair", "end_barrier"],
-        [round(x / 1e3 / batches, 2) for x in ph]))
-    # the persistent launch itself; the rest of the call is the upload, the
-    # stream-wide canonicalisation and first-call allocations
-    out["batched"]["kernel_seconds"] = float(sum(ph)) * 1e-9
+    # batched: the whole stream in one call, every batch's digest returned,
+    # distances resident on the device at the end -- through version-parallel
+    # windows (the default route), then through the persistent update launch
+    # (window 0), whose per-phase clock is reported
+    batched_digests = {}
+    for name, window in (("batched", None), ("batched_update_launch", 0)):
+        gb, bb = replica()
+        if window is not None:
+            bb.set_stream_window(window)
+        cs = torch.cuda.ExternalStream(gb.stream)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0.record(cs)
+        digs, _ = bb.apply_stream(st.src, st.dst, st.add, off, digests=True)
+        e1.record(cs)
+        torch.cuda.synchronize()
+        out[name] = {"seconds": e0.elapsed_time(e1) * 1e-3, "wall_s": time.perf_counter() - t0}
+        out[name]["batches_per_s"] = batches / out[name]["seconds"]
+        batched_digests[name] = [int(x) for x in digs]
+        if window == 0:
+            ph = bb.phase_trace()[21:27]
+            out[name]["phase_us_per_batch"] = dict(zip(
+                ["classify", "removals", "cascade", "insertions", "post_repair", "end_barrier"],
+                [round(x / 1e3 / batches, 2) for x in ph]))
+            # the persistent launch itself; the rest of the call is the
+            # upload, the stream-wide canonicalisation and first-call allocations
+            out[name]["kernel_seconds"] = float(sum(ph)) * 1e-9
+        else:
+            out[name]["route"] = "version-parallel windows of 64 batches"
+            bv = bb
+        if not (np.array_equal(bp.distances_array(), bb.distances_array())
+                and bp.reachable_count == bb.reachable_count):
+            out[name]["exact_final"] = False
+    out["batched_routes_equal"] = batched_digests["batched"] == batched_digests["batched_update_launch"]
     out["speedup"] = out["batched"]["batches_per_s"] / out["plain"]["batches_per_s"]
     out["speedup_vs_fused"] = out["batched"]["batches_per_s"] / out["plain_fused"]["batches_per_s"]
-    out["exact_final"] = bool(np.array_equal(bp.distances_array(), bb.distances_array())
-                              and bp.reachable_count == bb.reachable_count
-                              and np.array_equal(bp_fused.distances_array(), bb.distances_array()))
+    out["speedup_update_launch"] = out["batched_update_launch"]["batches_per_s"] / out["plain"]["batches_per_s"]
+    out["exact_final"] = bool(np.array_equal(bp.distances_array(), bv.distances_array())
+                              and bp.reachable_count == bv.reachable_count
+                              and np.array_equal(bp_fused.distances_array(), bv.distances_array())
+                              and out["batched_routes_equal"])
     # per-batch check on a prefix: digests of the stream path against the plain path
     if check_batches:
         k = min(check_batches, batches)
@@ -327,10 +368,14 @@ def lognormal(scale: int = 20, batches: int = 1000, median: float = 500.0, sigma
         recs = stream_records(digs, stats, V)
         bd.set_fused(False)  # checked against the per-phase path
         ok = True
+        ok_v = True
         for t in range(k):
             bd.apply_arrays(*st.batch(t))
-            ok = ok and record(gd, bd) == recs[t]
-        out["exact_every_batch"] = {"batches": k, "exact": bool(ok), "against": "per-phase plain path"}
+            r = record(gd, bd)
+            ok = ok and r == recs[t]
+            ok_v = ok_v and r[0] == batched_digests["batched"][t]
+        out["exact_every_batch"] = {"batches": k, "exact": bool(ok and ok_v), "against": "per-phase plain path",
+                                    "routes": "version-parallel digests; update-launch digests and counters"}
         out["_check"] = (edges, st.prefix(k), root, recs)
         del bc, gc_, bd, gd
     if multiroot:
