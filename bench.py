@@ -429,6 +429,9 @@ def run_b200(args, rank, world, local):
             "frac": achieved / hbm,
             "traffic": (traffic or {}).get("dram_bytes_per_launch"),
             "algorithmic_bytes": "4*A_r + 8*(V+1) + 4*V per root",
+            # the DRAM bytes ncu counts per launch over the median launch time
+            "frac_dram_traffic": (((traffic or {}).get("dram_bytes_per_launch") or 0)
+                                  / (float(np.median(bfs_ms)) * 1e-3) / 1e9 / hbm) if traffic else None,
         },
         "roofline_step": {
             "kernel": "one update step: canon_cluster_kernel + bfs_stream_kernel (fused commit and repair)",
@@ -440,6 +443,8 @@ def run_b200(args, rank, world, local):
             "frac": step_achieved / hbm,
             "algorithmic_bytes_per_batch": step_bytes,
             "traffic": (step_traffic or {}).get("dram_bytes_per_batch"),
+            "frac_dram_traffic": (((step_traffic or {}).get("dram_bytes_per_batch") or 0) / (t_dev / args.steps)
+                                  / 1e9 / hbm) if step_traffic else None,
             "counters_per_batch": {k: acct[k] / nb_acct for k in ("arcs_scanned", "vertices_visited",
                                                                   "delta_entries", "canonical_arcs")},
             "algorithmic_bytes": "9*ops + 2*17*canonical_arcs + 4*delta_entries + 4*arcs_scanned + "

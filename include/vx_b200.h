@@ -247,10 +247,16 @@ int vx_bfs_accounting(vx_bfs* b, uint64_t* out5);
  * value.  No reference counterpart. */
 int vx_bfs_set_update_blocks(vx_bfs* b, uint32_t blocks);
 /* Batches per version-parallel window of vx_bfs_apply_stream (1..256,
- * default 64; larger values are clamped to 256); 0 sends every batch through
+ * default 256; larger values are clamped to 256); 0 sends every batch through
  * the persistent update launch.  Same results for every value.  No reference
  * counterpart. */
 int vx_bfs_set_stream_window(vx_bfs* b, uint32_t batches);
+/* Level trace of the last version-parallel window's traversal: for each
+ * level (up to 64) its start time in ns and its frontier size with bit 63
+ * set for a pull level, then a closing timestamp; copies min(cap, *n)
+ * values, *n = 2 * levels + 1 (0 before any window).  No reference
+ * counterpart (diagnostics). */
+int vx_bfs_window_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
 /* fused != 0 (default): an undirected batch's commit and repair run in one
  * persistent launch after staging; 0: the per-phase path (a launch per commit
  * step and for each half of the repair) -- the plain baseline the batched

@@ -53,7 +53,7 @@ struct BfsTuning {
   uint32_t update_blocks = 0;  // blocks of the update launch (0: every co-resident block)
   // batches per version-parallel window of a stream whose per-batch repair
   // counters are not asked for (0: every batch by the update launch)
-  uint32_t stream_window = 64;
+  uint32_t stream_window = 256;
 };
 
 struct VersionBufs;

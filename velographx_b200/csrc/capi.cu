@@ -489,6 +489,11 @@ int vx_bfs_set_stream_window(vx_bfs* b, uint32_t batches) {
   return VX_OK;
 }
 
+int vx_bfs_window_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n) {
+  if (!b || !n || (cap && !out)) return fail(VX_ERR_INVALID, "null argument");
+  return vxh::stream_versions_trace(b->b, reinterpret_cast<unsigned long long*>(out), cap, n);
+}
+
 int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row) {
   if (!b || !(alpha > 0.f) || !(beta > 0.f) || large_row < 32) return fail(VX_ERR_INVALID, "invalid tuning");
   b->b->tune.alpha = alpha;

@@ -30,6 +30,28 @@ __device__ __forceinline__ uint32_t degree_of(const DevAdj& a, uint32_t u) {
   return (uint32_t)(e - b) + a.drow[u].y;
 }
 
+// The W per-vertex words at base (W = 1, 2, 4 or 8 consecutive words, base
+// aligned to 4 * W bytes), one vector load per 16 bytes.
+template <uint32_t W>
+__device__ __forceinline__ void load_words(const uint32_t* base, uint32_t* out) {
+  if constexpr (W == 1) {
+    out[0] = base[0];
+  } else if constexpr (W == 2) {
+    const uint2 t = *reinterpret_cast<const uint2*>(base);
+    out[0] = t.x;
+    out[1] = t.y;
+  } else {
+#pragma unroll
+    for (uint32_t h = 0; h < W / 4; ++h) {
+      const uint4 t = reinterpret_cast<const uint4*>(base)[h];
+      out[4 * h] = t.x;
+      out[4 * h + 1] = t.y;
+      out[4 * h + 2] = t.z;
+      out[4 * h + 3] = t.w;
+    }
+  }
+}
+
 // --------------------------------------------------- row expansion core --
 
 constexpr uint32_t FULL = 0xFFFFFFFFu;

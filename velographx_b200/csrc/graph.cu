@@ -41,6 +41,7 @@ inline int bits_for(size_t v) {  // bits to represent v - 1 (v >= 1)
 
 using gdev::bsearch_u32;
 using gdev::mark_dirty;
+using gdev::mark_dirty_count;
 using gdev::warp_merge_inplace;
 using gdev::warp_merge_to;
 
@@ -317,6 +318,7 @@ __global__ void delta_remove_kernel(DevAdj a, const uint32_t* lu, const uint32_t
   const uint32_t nruns = *nruns_p, nlist = *nlist_p;
   const int lane = threadIdx.x & 31;
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  unsigned long long dropped = 0, dirtied = 0;
   for (uint32_t r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nruns; r += warps) {
     const uint32_t s = runs[r], e = (r + 1 < nruns) ? runs[r + 1] : nlist;
     const uint32_t u = lu[s];
@@ -337,10 +339,13 @@ __global__ void delta_remove_kernel(DevAdj a, const uint32_t* lu, const uint32_t
     }
     if (lane == 0) {
       a.drow[u].y = written;
-      atomicAdd(live, (unsigned long long)(-(long long)(row.y - written)));
-      mark_dirty(a.dirty, u, dirty_rows);
+      dropped += row.y - written;
+      dirtied += mark_dirty_count(a.dirty, u);
     }
   }
+  // one update of each shared counter per warp (per row they serialised)
+  if (lane == 0 && dropped) atomicAdd(live, (unsigned long long)(-(long long)dropped));
+  if (lane == 0 && dirtied) atomicAdd(dirty_rows, dirtied);
 }
 
 // One warp per row run: merge the run's arcs into the row's delta list, in
@@ -353,6 +358,7 @@ __global__ void delta_insert_kernel(DevAdj a, size_t arena_cap, const uint32_t* 
   const uint32_t nruns = *nruns_p, nlist = *nlist_p;
   const int lane = threadIdx.x & 31;
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  unsigned long long added = 0, dirtied = 0;
   for (uint32_t r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < nruns; r += warps) {
     const uint32_t s = runs[r], e = (r + 1 < nruns) ? runs[r + 1] : nlist;
     const uint32_t u = lu[s], nB = e - s;
@@ -379,10 +385,13 @@ __global__ void delta_insert_kernel(DevAdj a, size_t arena_cap, const uint32_t* 
       }
     }
     if (lane == 0) {
-      atomicAdd(live, (unsigned long long)nB);
-      mark_dirty(a.dirty, u, dirty_rows);
+      added += nB;
+      dirtied += mark_dirty_count(a.dirty, u);
     }
   }
+  // one update of each shared counter per warp (per row they serialised)
+  if (lane == 0 && added) atomicAdd(live, added);
+  if (lane == 0 && dirtied) atomicAdd(dirty_rows, dirtied);
 }
 
 // ---------------------------------------------------------- consolidate --

@@ -75,10 +75,16 @@ struct PushVisit {
   __device__ __forceinline__ void operator()(bool valid, uint32_t x, uint32_t) {
     bool fresh = false;
     if (valid) {
+      // a head's bits are read before they are OR-ed in: a hub that many
+      // frontier rows reach takes one atomic per new bit, not one per arc
+      // (the thread whose atomic added bits lists the head)
       bool any = false;
+      uint32_t vx[W];
+      load_words<W>(p->vis + (size_t)x * W, vx);
 #pragma unroll
       for (uint32_t w = 0; w < W; ++w) {
-        const uint32_t m = fw[w] & ~p->vis[(size_t)x * W + w];
+        uint32_t m = fw[w] & ~vx[w];
+        if (m) m &= ~__ldcg(&p->nxt[(size_t)x * W + w]);
         if (m) {
           atomicOr(&p->nxt[(size_t)x * W + w], m);
           any = true;
@@ -86,7 +92,7 @@ struct PushVisit {
       }
       if (any) {
         const uint32_t bit = 1u << (x & 31);
-        fresh = !(atomicOr(&p->touched[x >> 5], bit) & bit);
+        fresh = !(__ldcg(&p->touched[x >> 5]) & bit) && !(atomicOr(&p->touched[x >> 5], bit) & bit);
       }
     }
     const uint32_t s = vxb::warp_append(fresh, tcount);
@@ -215,9 +221,14 @@ __device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, 
       }
       uint32_t m[kMrU][W];
 #pragma unroll
-      for (uint32_t u = 0; u < kMrU; ++u)
+      for (uint32_t u = 0; u < kMrU; ++u) {
+        if (x[u] & kTomb) {
 #pragma unroll
-        for (uint32_t w = 0; w < W; ++w) m[u][w] = (x[u] & kTomb) ? 0u : fc[(size_t)x[u] * W + w];
+          for (uint32_t w = 0; w < W; ++w) m[u][w] = 0u;
+        } else {
+          load_words<W>(fc + (size_t)x[u] * W, m[u]);
+        }
+      }
 #pragma unroll
       for (uint32_t u = 0; u < kMrU; ++u)
 #pragma unroll
@@ -280,10 +291,13 @@ __device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, 
 #pragma unroll
       for (uint32_t w = 0; w < W; ++w) add[w] = 0u;
 #pragma unroll
-      for (uint32_t u = 0; u < kMrU; ++u)
+      for (uint32_t u = 0; u < kMrU; ++u) {
+        if (x[u] & kTomb) continue;
+        uint32_t f[W];
+        load_words<W>(fc + (size_t)x[u] * W, f);
 #pragma unroll
-        for (uint32_t w = 0; w < W; ++w)
-          if (!(x[u] & kTomb)) add[w] |= fc[(size_t)x[u] * W + w];
+        for (uint32_t w = 0; w < W; ++w) add[w] |= f[w];
+      }
 #pragma unroll
       for (uint32_t w = 0; w < W; ++w) {
         const uint32_t red = __reduce_or_sync(FULL, add[w]) & ~vis[w];

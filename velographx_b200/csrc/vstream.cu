@@ -73,7 +73,7 @@ struct VsParams {
   uint32_t* q[3];
   uint32_t* tl;
   uint32_t* big;
-  unsigned long long* dig;     // [K] (null: no digests)
+  unsigned long long* dig;     // [K] digest deltas as a difference array over the versions (null: no digests)
   unsigned long long* bucket;  // [K]
   VsCounters* c;
   uint32_t* bar;
@@ -267,34 +267,39 @@ __device__ __forceinline__ bool vs_discover(const VsParams& p, uint32_t v, const
   return true;
 }
 
-// Digest deltas of the warp's discoveries (warp-uniform; `valid` lanes
-// discovered v in the versions `nw` at distance lvl): a discovery in every
-// version goes to the thread's register sum; the others are summed across
-// the warp per version and added to the block's per-version sums by one lane.
+// Digest deltas of a discovery (v reached at distance lvl in the versions
+// `nw`): one reached in every version goes to the thread's register sum;
+// otherwise the delta is added, as a difference array over the versions, at
+// every run boundary of the mask (+d where a run of versions starts, -d
+// where it ends), so a vertex reached from some version on costs one
+// shared-memory atomic however many versions it covers.
 template <uint32_t W>
-__device__ __forceinline__ void vs_digest_warp(const VsParams& p, uint32_t v, const uint32_t* nw, uint32_t lvl,
-                                               bool valid, VsSums& s, unsigned long long* sdig) {
+__device__ __forceinline__ void vs_digest(const VsParams& p, uint32_t v, const uint32_t* nw, uint32_t lvl, VsSums& s,
+                                          unsigned long long* sdig) {
   bool any = false, all = true;
 #pragma unroll
   for (uint32_t w = 0; w < W; ++w) {
     any = any || nw[w] != 0u;
     all = all && nw[w] == vmask(p.K, w);
   }
-  valid = valid && any;
-  const unsigned long long d = valid ? vxb::mix64(((unsigned long long)v << 32) | lvl) -
-                                           vxb::mix64(((unsigned long long)v << 32) | kUnreachable)
-                                     : 0ull;
-  if (valid && all) s.common += d;
-  const bool part = valid && !all;
-  if (!__any_sync(FULL, part)) return;
+  if (!any) return;
+  const unsigned long long d = vxb::mix64(((unsigned long long)v << 32) | lvl) -
+                               vxb::mix64(((unsigned long long)v << 32) | kUnreachable);
+  if (all) {
+    s.common += d;
+    return;
+  }
+  uint32_t carry = 0;  // the mask's bit just below the word
 #pragma unroll
   for (uint32_t w = 0; w < W; ++w) {
-    uint32_t bits = __reduce_or_sync(FULL, part ? nw[w] : 0u);
-    while (bits) {
-      const uint32_t b = __ffs(bits) - 1;
-      bits &= bits - 1;
-      const unsigned long long t = vxb::warp_sum((part && ((nw[w] >> b) & 1u)) ? d : 0ull);
-      if ((threadIdx.x & 31) == 0) atomicAdd(&sdig[32 * w + b], t);
+    const uint32_t m = nw[w];
+    uint32_t t = m ^ ((m << 1) | carry);  // bits that differ from the bit below
+    carry = m >> 31;
+    while (t) {
+      const uint32_t b = __ffs(t) - 1;
+      t &= t - 1;
+      const uint32_t ver = 32 * w + b;
+      if (ver < p.K) atomicAdd(&sdig[ver], ((m >> b) & 1u) ? d : (unsigned long long)0 - d);
     }
   }
 }
@@ -322,7 +327,7 @@ __device__ void vs_finalize(const VsParams& p, const uint32_t* list, uint32_t n,
     }
     if (valid && touched) p.touched[x >> 5] = 0u;
     const bool any = valid && vs_discover<W>(p, x, vis, nw, fn, level + 1, s);
-    if (p.dig) vs_digest_warp<W>(p, x, nw, level + 1, valid, s, sdig);
+    if (p.dig && valid) vs_digest<W>(p, x, nw, level + 1, s, sdig);
     const uint32_t slot = vxb::warp_append(any, qn);
     if (any) qout[slot] = x;
   }
@@ -424,13 +429,20 @@ __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
       }
       uint32_t m[kSlots][W];
 #pragma unroll
-      for (uint32_t u = 0; u < kSlots; ++u)
+      for (uint32_t u = 0; u < kSlots; ++u) {
+        if (x[u] & kTomb) {
 #pragma unroll
-        for (uint32_t w = 0; w < W; ++w) {
-          uint32_t f = (x[u] & kTomb) ? 0u : fc[(size_t)x[u] * W + w];
-          if (f && e[u] != kNoEntry) f &= p.tmask[(size_t)e[u] * W + w];
-          m[u][w] = f;
+          for (uint32_t w = 0; w < W; ++w) m[u][w] = 0u;
+          continue;
         }
+        load_words<W>(fc + (size_t)x[u] * W, m[u]);
+        if (e[u] != kNoEntry) {
+          uint32_t mk[W];
+          load_words<W>(p.tmask + (size_t)e[u] * W, mk);
+#pragma unroll
+          for (uint32_t w = 0; w < W; ++w) m[u][w] &= mk[w];
+        }
+      }
 #pragma unroll
       for (uint32_t u = 0; u < kSlots; ++u)
 #pragma unroll
@@ -450,7 +462,7 @@ __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
 #pragma unroll
     for (uint32_t w = 0; w < W; ++w) nw[w] = ws.acc[lane * W + w] & ~vis[w];
     const bool any = v < p.V && vs_discover<W>(p, v, vis, nw, fn, level + 1, s);
-    if (p.dig) vs_digest_warp<W>(p, v, nw, level + 1, v < p.V, s, sdig);
+    if (p.dig && v < p.V) vs_digest<W>(p, v, nw, level + 1, s, sdig);
     const uint32_t slot = vxb::warp_append(any, qn);
     if (any) qout[slot] = v;
     __syncwarp();  // the next group overwrites the stage
@@ -486,13 +498,19 @@ __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
 #pragma unroll
       for (uint32_t w = 0; w < W; ++w) add[w] = 0u;
 #pragma unroll
-      for (uint32_t u = 0; u < kSlots; ++u)
+      for (uint32_t u = 0; u < kSlots; ++u) {
+        if (x[u] & kTomb) continue;
+        uint32_t f[W];
+        load_words<W>(fc + (size_t)x[u] * W, f);
+        if (e[u] != kNoEntry) {
+          uint32_t mk[W];
+          load_words<W>(p.tmask + (size_t)e[u] * W, mk);
 #pragma unroll
-        for (uint32_t w = 0; w < W; ++w) {
-          uint32_t f = (x[u] & kTomb) ? 0u : fc[(size_t)x[u] * W + w];
-          if (f && e[u] != kNoEntry) f &= p.tmask[(size_t)e[u] * W + w];
-          add[w] |= f;
+          for (uint32_t w = 0; w < W; ++w) f[w] &= mk[w];
         }
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w) add[w] |= f[w];
+      }
 #pragma unroll
       for (uint32_t w = 0; w < W; ++w) {
         const uint32_t red = __reduce_or_sync(FULL, add[w]) & ~vis[w];
@@ -519,12 +537,17 @@ __device__ __forceinline__ void vs_push_arcs(const VsParams& p, const VsRow& r, 
       uint32_t e;
       x = vs_arc(p, r.b, r.nb, r.dx, r.dy, r.tb, r.tn, r.pre, k, e);
       if (!(x & kTomb)) {
+        // bits already OR-ed into a head are not OR-ed again (one atomic per
+        // new bit at a hub, not one per arc; the thread that added bits
+        // lists the head)
         bool any = false;
+        uint32_t vx[W];
+        load_words<W>(p.vis + (size_t)x * W, vx);
 #pragma unroll
         for (uint32_t w = 0; w < W; ++w) {
-          uint32_t m = fw[w];
+          uint32_t m = fw[w] & ~vx[w];
           if (m && e != kNoEntry) m &= p.tmask[(size_t)e * W + w];
-          if (m) m &= ~p.vis[(size_t)x * W + w];
+          if (m) m &= ~__ldcg(&p.nxt[(size_t)x * W + w]);
           if (m) {
             atomicOr(&p.nxt[(size_t)x * W + w], m);
             any = true;
@@ -532,7 +555,7 @@ __device__ __forceinline__ void vs_push_arcs(const VsParams& p, const VsRow& r, 
         }
         if (any) {
           const uint32_t bit = 1u << (x & 31);
-          fresh = !(atomicOr(&p.touched[x >> 5], bit) & bit);
+          fresh = !(__ldcg(&p.touched[x >> 5]) & bit) && !(atomicOr(&p.touched[x >> 5], bit) & bit);
         }
       }
     }
@@ -645,8 +668,14 @@ __global__ void __launch_bounds__(kVsThreads, 2) vs_bfs_kernel(VsParams p) {
     }
     const uint32_t* fc = p.frn[cur];
     uint32_t* fn = p.frn[nx];
+    const bool pull = (float)n_f > p.pull_frac * (float)p.V;
+    if (gtid() == 0) {
+      const uint32_t t = min(level, 63u);
+      c->trace[2 * t] = globaltimer();
+      c->trace[2 * t + 1] = (unsigned long long)n_f | ((unsigned long long)pull << 63);
+    }
     bool ok;
-    if ((float)n_f > p.pull_frac * (float)p.V)
+    if (pull)
       ok = vs_pull<W>(p, fc, fn, level, &c->gnext[cur], &c->nbig[cur], &c->qn[nx], p.q[nx], stage[threadIdx.x >> 5],
                       s, sdig);
     else
@@ -654,7 +683,10 @@ __global__ void __launch_bounds__(kVsThreads, 2) vs_bfs_kernel(VsParams p) {
     if (!ok) return;
     prev_n = n_f;
   }
-  if (gtid() == 0) c->levels = level;
+  if (gtid() == 0) {
+    c->levels = level;
+    c->trace[2 * min(level, 64u)] = globaltimer();
+  }
   // per-thread sums, then the block's per-version digest deltas
   const unsigned long long common = vxb::warp_sum(s.common), reach = vxb::warp_sum(s.reach),
                            b0 = vxb::warp_sum(base0);
@@ -782,6 +814,17 @@ int stream_versions_reserve(Bfs* b, size_t ops, size_t V, size_t k) {
   if (!b->vb) b->vb = new VersionBufs();
   if (int rc = b->vb->ensure(ops, std::max<size_t>(V, 1), version_words(k), k)) return rc;
   return b->g->batch.ensure(ops);
+}
+
+int stream_versions_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n) {
+  *n = 0;
+  if (!b->vb || !b->vb->hctr) return 0;
+  const VsCounters& c = *b->vb->hctr;
+  const uint32_t levels = std::min<uint32_t>(c.levels, 64);
+  if (!levels) return 0;
+  *n = 2 * (size_t)levels + 1;
+  for (size_t i = 0; i < std::min(cap, *n); ++i) out[i] = i + 1 == *n ? c.trace[2 * levels] : c.trace[i];
+  return 0;
 }
 
 int stream_versions(Bfs* b, const uint32_t* d_src, const uint32_t* d_dst, const uint8_t* d_add, const uint64_t* hoff,
@@ -924,10 +967,12 @@ int stream_versions(Bfs* b, const uint32_t* d_src, const uint32_t* d_dst, const 
     return -5;
   }
   if (digests) {
-    unsigned long long base = 0;
+    // both per-version arrays are difference arrays: prefix sums
+    unsigned long long base = 0, delta = 0;
     for (size_t t = 0; t < k; ++t) {
       base += S.hdig[k + t];
-      digests[t0 + t] = base + S.hdig[t] + S.hctr->common;
+      delta += S.hdig[t];
+      digests[t0 + t] = base + delta + S.hctr->common;
     }
   }
   return 0;

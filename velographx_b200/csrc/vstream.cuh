@@ -24,6 +24,9 @@ struct VsCounters {
   uint32_t runs;      // distinct touched arcs
   unsigned long long reach;   // finite distances of the last version
   unsigned long long common;  // digest deltas of discoveries made in every version at once
+  // per level: globaltimer at its start, then its frontier size with bit 63
+  // set for a pull level; after the last level, the closing stamp
+  unsigned long long trace[2 * 64 + 1];
 };
 
 struct VersionBufs {
@@ -50,7 +53,7 @@ struct VersionBufs {
   uint32_t* q[3] = {nullptr, nullptr, nullptr};
   uint32_t* tl = nullptr;
   uint32_t* big = nullptr;
-  unsigned long long* dig = nullptr;     // [k] per-version digest deltas
+  unsigned long long* dig = nullptr;     // [k] digest deltas, a difference array over the versions
   unsigned long long* bucket = nullptr;  // [k] unreachable terms by first version
   VsCounters* ctr = nullptr;
   VsCounters* hctr = nullptr;
@@ -81,5 +84,10 @@ int stream_versions(Bfs* b, const uint32_t* d_src, const uint32_t* d_dst, const 
 // the graph's batch buffers for the merged commit), so that no window
 // allocates.
 int stream_versions_reserve(Bfs* b, size_t ops, size_t V, size_t k);
+
+// Level trace of the last window's traversal: {start ns, n_f | pull << 63}
+// per level (up to 64), then the closing stamp; *n = 2 * levels + 1 (0 when
+// no window ran).
+int stream_versions_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n);
 
 }  // namespace vxh

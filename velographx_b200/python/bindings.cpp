@@ -344,6 +344,19 @@ PYBIND11_MODULE(_velographx, m) {
            })
       .def("set_update_blocks",
            [](IncrementalBFS& x, std::uint32_t blocks) { detail::check(vx_bfs_set_update_blocks(x.handle(), blocks)); })
+      .def("window_trace",
+           [](IncrementalBFS& x) {
+             std::size_t n = 0;
+             detail::check(vx_bfs_window_trace(x.handle(), nullptr, 0, &n));
+             std::vector<std::uint64_t> t(n);
+             if (n) detail::check(vx_bfs_window_trace(x.handle(), t.data(), n, &n));
+             py::list out;  // (us, frontier size, pull) per level
+             const std::size_t levels = n ? (n - 1) / 2 : 0;
+             for (std::size_t i = 0; i < levels; ++i)
+               out.append(py::make_tuple(static_cast<double>(t[2 * i + 2] - t[2 * i]) * 1e-3,
+                                         t[2 * i + 1] & 0x7FFFFFFFFFFFFFFFull, (t[2 * i + 1] >> 63) != 0));
+             return out;
+           })
       .def("set_stream_window",
            [](IncrementalBFS& x, std::uint32_t batches) {
              detail::check(vx_bfs_set_stream_window(x.handle(), batches));

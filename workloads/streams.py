@@ -250,7 +250,7 @@ def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int 
     del b, g
     out["plain"] = {"batches_per_s": float(np.median(plain_runs)), "runs": [round(x) for x in plain_runs]}
     out["batched"] = {"batches_per_s": float(np.median(batched_runs)), "runs": [round(x) for x in batched_runs],
-                      "route": "version-parallel windows of 64 batches (digest of every batch returned)"}
+                      "route": "version-parallel windows of 256 batches (digest of every batch returned)"}
     out["batched_update_launch"] = {
         "batches_per_s": float(np.median(ul_runs)), "runs": [round(x) for x in ul_runs],
         "route": "every batch in one persistent update launch (stream window 0)",
@@ -346,7 +346,7 @@ def lognormal(scale: int = 20, batches: int = 1000, median: float = 500.0, sigma
             # upload, the stream-wide canonicalisation and first-call allocations
             out[name]["kernel_seconds"] = float(sum(ph)) * 1e-9
         else:
-            out[name]["route"] = "version-parallel windows of 64 batches"
+            out[name]["route"] = "version-parallel windows of 256 batches"
             bv = bb
         if not (np.array_equal(bp.distances_array(), bb.distances_array())
                 and bp.reachable_count == bb.reachable_count):
