@@ -257,6 +257,10 @@ int vx_bfs_set_stream_window(vx_bfs* b, uint32_t batches);
  * values, *n = 2 * levels + 1 (0 before any window).  No reference
  * counterpart (diagnostics). */
 int vx_bfs_window_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
+/* A version-parallel window's level pulls (bottom-up) when its frontier
+ * holds more than frac * V vertices (default 0.02).  Same results for every
+ * value.  No reference counterpart. */
+int vx_bfs_set_window_pull_fraction(vx_bfs* b, float frac);
 /* fused != 0 (default): an undirected batch's commit and repair run in one
  * persistent launch after staging; 0: the per-phase path (a launch per commit
  * step and for each half of the repair) -- the plain baseline the batched

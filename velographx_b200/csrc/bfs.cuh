@@ -54,6 +54,9 @@ struct BfsTuning {
   // batches per version-parallel window of a stream whose per-batch repair
   // counters are not asked for (0: every batch by the update launch)
   uint32_t stream_window = 256;
+  // a window traversal's level pulls when its frontier holds more than this
+  // fraction of the vertices
+  float window_pull_frac = 0.02f;
 };
 
 struct VersionBufs;

@@ -489,6 +489,12 @@ int vx_bfs_set_stream_window(vx_bfs* b, uint32_t batches) {
   return VX_OK;
 }
 
+int vx_bfs_set_window_pull_fraction(vx_bfs* b, float frac) {
+  if (!b || !(frac > 0.f)) return fail(VX_ERR_INVALID, "invalid pull fraction");
+  b->b->tune.window_pull_frac = frac;
+  return VX_OK;
+}
+
 int vx_bfs_window_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n) {
   if (!b || !n || (cap && !out)) return fail(VX_ERR_INVALID, "null argument");
   return vxh::stream_versions_trace(b->b, reinterpret_cast<unsigned long long*>(out), cap, n);

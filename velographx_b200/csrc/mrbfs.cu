@@ -37,7 +37,8 @@ struct MrParams {
   uint32_t* touched; // bitmap
   uint32_t* q[3];    // rotating frontier queues
   uint32_t* tl;      // touched list of a push level
-  uint32_t* big;     // frontier rows of a push level that the whole grid expands
+  uint32_t* big;     // rows of a level that the whole grid reads
+  uint32_t* biglen;  // their lengths
   uint32_t* dist;    // [K][V]
   MrCounters* c;
   uint32_t* bar;
@@ -106,7 +107,10 @@ template <uint32_t W>
 struct MrSlots {
   static constexpr uint32_t value = W <= 2 ? 8 : 4;
 };
-constexpr uint32_t kMrBigRow = 4096;     // push rows this long are expanded by the whole grid
+constexpr uint32_t kMrHead = 8;          // in-arcs a lane reads itself before the flattened rounds
+constexpr uint32_t kMrHeadStep = 4;      // of which it loads this many at a time
+constexpr uint32_t kMrBigRow = 1024;     // push rows this long are expanded by the whole grid
+constexpr uint32_t kMrPushSlice = 128;   // arcs of a hub row a warp takes at a time
 constexpr uint32_t kMrBigPull = 2048;    // pull rows this long are read by the whole grid
 constexpr uint32_t kMrWarps = kThreads / 32;
 // 32-vertex groups a warp claims per atomic of a pull level (one counter
@@ -180,12 +184,47 @@ __device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, 
       const uint32_t nb = (uint32_t)(e - b);
       len = nb + dr.y;
       if (len >= kMrBigPull) {  // the whole grid reads it after the barrier
-        p.big[atomicAdd(nbig, 1u)] = v;
+        const uint32_t slot = atomicAdd(nbig, 1u);
+        p.big[slot] = v;
+        p.biglen[slot] = len;
         len = 0;
       }
       ws.rb[lane] = b;
       ws.nb[lane] = nb;
       ws.dx[lane] = dr.x;
+      // head: the lane first reads the first kMrHead arcs of its own row,
+      // kMrHeadStep loads in flight, and stops as soon as every root has
+      // reached its vertex; the flattened rounds below read the rest
+      const uint32_t hn = min(len, kMrHead);
+      uint32_t hacc[W];
+#pragma unroll
+      for (uint32_t w = 0; w < W; ++w) hacc[w] = 0u;
+      for (uint32_t h0 = 0; h0 < hn; h0 += kMrHeadStep) {
+        uint32_t hx[kMrHeadStep];
+#pragma unroll
+        for (uint32_t k = 0; k < kMrHeadStep; ++k) {
+          const uint32_t j = h0 + k;
+          hx[k] = j >= hn ? kTomb : (j < nb ? a.col[b + j] : a.darena[dr.x + (j - nb)]);
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kMrHeadStep; ++k) {
+          if (hx[k] & kTomb) continue;
+          uint32_t f[W];
+          load_words<W>(fc + (size_t)hx[k] * W, f);
+#pragma unroll
+          for (uint32_t w = 0; w < W; ++w) hacc[w] |= f[w];
+        }
+        bool fin = true;
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w) fin = fin && (vis[w] | hacc[w]) == word_mask(p, w);
+        if (fin) {
+          len = hn;  // nothing left for the rounds
+          break;
+        }
+      }
+      len -= hn;
+#pragma unroll
+      for (uint32_t w = 0; w < W; ++w) ws.acc[lane * W + w] = hacc[w];
     }
     uint32_t incl = len;
 #pragma unroll
@@ -215,7 +254,7 @@ __device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, 
         own[u] = o;
         x[u] = kTomb;
         if (j < T && ((active >> o) & 1u)) {
-          const uint32_t k = j - lo, nbo = ws.nb[o];
+          const uint32_t k = kMrHead + (j - lo), nbo = ws.nb[o];  // past the owner's head
           x[u] = k < nbo ? a.col[ws.rb[o] + k] : a.darena[ws.dx[o] + (k - nbo)];
         }
       }
@@ -264,9 +303,11 @@ __device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, 
   const uint32_t nb = __ldcg(nbig);
   if (nb == 0) return true;
   // long rows: every warp takes 32 * MrSlots<W>-arc slices; the slices of row r
-  // start at warp r (mod the warp count) so the rows spread over the grid
+  // start at warp r (mod the warp count) so the rows spread over the grid.  A
+  // warp skips, from the listed length alone, the rows it has no slice of.
   const uint32_t nw = nwarps(), gw = gwarp();
   for (uint32_t r = 0; r < nb; ++r) {
+    if ((gw + nw - r % nw) % nw >= (__ldcg(&p.biglen[r]) + 32 * kMrU - 1) / (32 * kMrU)) continue;
     const uint32_t v = p.big[r];
     uint32_t vis[W];
 #pragma unroll
@@ -384,8 +425,13 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
       PushVisit<W> pv{&p, {}, &c->tn[cur]};
       for (uint32_t i = gwarp(); i < n_f; i += nwarps()) {
         const uint32_t u = p.q[cur][i];
-        if (degree_of(a, u) >= kMrBigRow) {  // a hub: the whole grid, after the barrier
-          if ((threadIdx.x & 31) == 0) p.big[atomicAdd(&c->nbig[cur], 1u)] = u;
+        const uint32_t deg = degree_of(a, u);
+        if (deg >= kMrBigRow) {  // a hub: the whole grid, after the barrier
+          if ((threadIdx.x & 31) == 0) {
+            const uint32_t slot = atomicAdd(&c->nbig[cur], 1u);
+            p.big[slot] = u;
+            p.biglen[slot] = deg;
+          }
           continue;
         }
 #pragma unroll
@@ -394,41 +440,56 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
       }
       if (!mr_sync(p)) return;
       const uint32_t nbig = __ldcg(&c->nbig[cur]);
-      for (uint32_t r = 0; r < nbig; ++r) {  // every warp takes 32-arc slices of each hub row
+      // hub rows: kMrPushSlice-arc slices, the slices of row r starting at
+      // warp r (mod the warp count); a warp skips the rows it has no slice of
+      const uint32_t nw = nwarps(), gw = gwarp();
+      for (uint32_t r = 0; r < nbig; ++r) {
+        const uint32_t deg = __ldcg(&p.biglen[r]);
+        const uint32_t nsl = (deg + kMrPushSlice - 1) / kMrPushSlice;
+        uint32_t sl = (gw + nw - r % nw) % nw;
+        if (sl >= nsl) continue;
         const uint32_t u = p.big[r];
 #pragma unroll
         for (uint32_t w = 0; w < W; ++w) pv.fw[w] = fc[(size_t)u * W + w];
         uint64_t b, e;
         vxb::base_range(a, u, b, e);
-        for (uint64_t j0 = b + (uint64_t)gwarp() * 32; j0 < e; j0 += (uint64_t)nwarps() * 32) {
-          const uint64_t j = j0 + (threadIdx.x & 31);
-          const uint32_t x = j < e ? a.col[j] : kTomb;
-          pv(!(x & kTomb), x & kIdMask, u);
-        }
         const uint2 dr = a.drow[u];
-        for (uint32_t j0 = dr.x + gwarp() * 32; j0 < dr.x + dr.y; j0 += nwarps() * 32) {
-          const uint32_t j = j0 + (threadIdx.x & 31);
-          const bool ok = j < dr.x + dr.y;
-          pv(ok, ok ? a.darena[j] : 0u, u);
+        const uint32_t nbv = (uint32_t)(e - b);
+        for (; sl < nsl; sl += nw) {
+          for (uint32_t k0 = sl * kMrPushSlice; k0 < min(deg, (sl + 1) * kMrPushSlice); k0 += 32) {
+            const uint32_t k = k0 + (threadIdx.x & 31);
+            uint32_t x = kTomb;
+            if (k < nbv) x = a.col[b + k];
+            else if (k < deg) x = a.darena[dr.x + (k - nbv)];
+            pv(!(x & kTomb), x & kIdMask, u);
+          }
         }
       }
       if (nbig && !mr_sync(p)) return;
+      // the touched heads' new roots, in warp-uniform rounds so the next
+      // frontier is appended one atomic per warp (per head, the appends of
+      // a push level that reaches millions of heads serialised on qn)
       const uint32_t nt = __ldcg(&c->tn[cur]);
-      for (uint32_t i = gtid(); i < nt; i += nthreads()) {
-        const uint32_t x = p.tl[i];
+      for (uint32_t base = gwarp() * 32; base < nt; base += nwarps() * 32) {
+        const uint32_t i = base + (threadIdx.x & 31);
         bool any = false;
-        for (uint32_t w = 0; w < W; ++w) {
-          const size_t o = (size_t)x * W + w;
-          const uint32_t m = p.nxt[o] & ~p.vis[o];
-          p.nxt[o] = 0u;
-          if (!m) continue;
-          any = true;
-          p.vis[o] |= m;
-          fn[o] = m;
-          write_dists(p, x, w, m, level + 1);
+        uint32_t x = 0;
+        if (i < nt) {
+          x = p.tl[i];
+          for (uint32_t w = 0; w < W; ++w) {
+            const size_t o = (size_t)x * W + w;
+            const uint32_t m = p.nxt[o] & ~p.vis[o];
+            p.nxt[o] = 0u;
+            if (!m) continue;
+            any = true;
+            p.vis[o] |= m;
+            fn[o] = m;
+            write_dists(p, x, w, m, level + 1);
+          }
+          p.touched[x >> 5] = 0u;
         }
-        p.touched[x >> 5] = 0u;
-        if (any) p.q[nx][atomicAdd(&c->qn[nx], 1u)] = x;
+        const uint32_t slot = vxb::warp_append(any, &c->qn[nx]);
+        if (any) p.q[nx][slot] = x;
       }
       if (!mr_sync(p)) return;
     }
@@ -472,7 +533,7 @@ int mrbfs_create(MrBfs** out, Graph* g, const uint32_t* host_roots, size_t k) {
   const size_t vw = V * m->W;
   bool ok = cudaMalloc(&m->roots, k * 4) == cudaSuccess && cudaMalloc(&m->vis, vw * 4) == cudaSuccess &&
             cudaMalloc(&m->nxt, vw * 4) == cudaSuccess && cudaMalloc(&m->touched, ((V + 31) / 32) * 4) == cudaSuccess &&
-            cudaMalloc(&m->tl, V * 4) == cudaSuccess && cudaMalloc(&m->big, V * 4) == cudaSuccess &&
+            cudaMalloc(&m->tl, V * 4) == cudaSuccess && cudaMalloc(&m->big, V * 4) == cudaSuccess && cudaMalloc(&m->biglen, V * 4) == cudaSuccess &&
             cudaMalloc(&m->dist, V * k * 4) == cudaSuccess &&
             cudaMalloc(&m->ctr, sizeof(MrCounters)) == cudaSuccess &&
             cudaMalloc(&m->barrier, vxb::kBarrierWords * 4) == cudaSuccess &&
@@ -494,7 +555,7 @@ int mrbfs_create(MrBfs** out, Graph* g, const uint32_t* host_roots, size_t k) {
 void mrbfs_destroy(MrBfs* m) {
   if (!m) return;
   if (m->g && m->g->stream) cudaStreamSynchronize(m->g->stream);
-  void* ptrs[] = {m->roots, m->vis, m->nxt, m->touched, m->tl, m->big, m->dist, m->ctr, m->barrier,
+  void* ptrs[] = {m->roots, m->vis, m->nxt, m->touched, m->tl, m->big, m->biglen, m->dist, m->ctr, m->barrier,
                   m->frn[0], m->frn[1], m->frn[2], m->q[0], m->q[1], m->q[2]};
   for (void* p : ptrs) cudaFree(p);
   cudaFreeHost(m->hctr);
@@ -543,6 +604,7 @@ int mrbfs_run(MrBfs* m) {
   p.touched = m->touched;
   p.tl = m->tl;
   p.big = m->big;
+  p.biglen = m->biglen;
   p.dist = m->dist;
   p.c = m->ctr;
   p.bar = m->barrier;

@@ -37,7 +37,8 @@ struct MrBfs {
   uint32_t* touched = nullptr;
   uint32_t* q[3] = {nullptr, nullptr, nullptr};
   uint32_t* tl = nullptr;
-  uint32_t* big = nullptr;  // hub rows of a push level
+  uint32_t* big = nullptr;     // rows of a level that the whole grid reads
+  uint32_t* biglen = nullptr;  // their lengths
   uint32_t* dist = nullptr;  // [K][V]
   MrCounters* ctr = nullptr;
   MrCounters* hctr = nullptr;

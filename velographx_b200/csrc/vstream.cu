@@ -49,8 +49,11 @@ constexpr uint32_t kVsWarps = kVsThreads / 32;
 // 32-vertex groups a warp claims per atomic of a pull level (one counter
 // per level: a claim per group serialised on it)
 constexpr uint32_t kClaimGroups = 4;
+constexpr uint32_t kVsHead = 8;        // in-arcs a lane reads itself before the flattened rounds
+constexpr uint32_t kVsHeadStep = 4;    // of which it loads this many at a time
 constexpr uint32_t kVsBigPull = 2048;  // pull rows this long are read by the whole grid
-constexpr uint32_t kVsBigPush = 4096;  // push rows this long are expanded by the whole grid
+constexpr uint32_t kVsBigPush = 1024;  // push rows this long are expanded by the whole grid
+constexpr uint32_t kVsPushSlice = 128; // arcs of a hub row a warp takes at a time
 constexpr int kVsTBits = 8;            // version field of the sort keys
 constexpr uint32_t kNoEntry = 0xFFFFFFFFu;
 
@@ -73,6 +76,7 @@ struct VsParams {
   uint32_t* q[3];
   uint32_t* tl;
   uint32_t* big;
+  uint32_t* biglen;
   unsigned long long* dig;     // [K] digest deltas as a difference array over the versions (null: no digests)
   unsigned long long* bucket;  // [K]
   VsCounters* c;
@@ -385,7 +389,9 @@ __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
       const VsRow r = vs_row(p, v);
       len = r.nb + r.dy + r.tn;
       if (len >= kVsBigPull) {  // the whole grid reads it after the barrier
-        p.big[atomicAdd(nbig, 1u)] = v;
+        const uint32_t slot = atomicAdd(nbig, 1u);
+        p.big[slot] = v;
+        p.biglen[slot] = len;
         len = 0;
       }
       ws.rb[lane] = r.b;
@@ -394,6 +400,46 @@ __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
       ws.dy[lane] = r.dy;
       ws.tb[lane] = r.tb;
       ws.tn[lane] = r.tn | (r.pre ? 0x80000000u : 0u);
+      // head: the lane first reads the first kVsHead arcs of its own row,
+      // kVsHeadStep loads in flight, and stops as soon as every version has
+      // reached its vertex (most vertices find a parent reached in every
+      // version among their first arcs); the flattened rounds read the rest
+      const uint32_t hn = min(len, kVsHead);
+      uint32_t hacc[W];
+#pragma unroll
+      for (uint32_t w = 0; w < W; ++w) hacc[w] = 0u;
+      for (uint32_t h0 = 0; h0 < hn; h0 += kVsHeadStep) {
+        uint32_t hx[kVsHeadStep], he[kVsHeadStep];
+#pragma unroll
+        for (uint32_t k = 0; k < kVsHeadStep; ++k) {
+          he[k] = kNoEntry;
+          hx[k] = h0 + k < hn ? vs_arc(p, r.b, r.nb, r.dx, r.dy, r.tb, r.tn, r.pre, h0 + k, he[k]) : kTomb;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kVsHeadStep; ++k) {
+          if (hx[k] & kTomb) continue;
+          uint32_t f[W];
+          load_words<W>(fc + (size_t)hx[k] * W, f);
+          if (he[k] != kNoEntry) {
+            uint32_t mk[W];
+            load_words<W>(p.tmask + (size_t)he[k] * W, mk);
+#pragma unroll
+            for (uint32_t w = 0; w < W; ++w) f[w] &= mk[w];
+          }
+#pragma unroll
+          for (uint32_t w = 0; w < W; ++w) hacc[w] |= f[w];
+        }
+        bool fin = true;
+#pragma unroll
+        for (uint32_t w = 0; w < W; ++w) fin = fin && (vis[w] | hacc[w]) == vmask(p.K, w);
+        if (fin) {
+          len = hn;  // nothing left for the rounds
+          break;
+        }
+      }
+      len -= hn;
+#pragma unroll
+      for (uint32_t w = 0; w < W; ++w) ws.acc[lane * W + w] = hacc[w];
     }
     uint32_t incl = len;
 #pragma unroll
@@ -424,7 +470,7 @@ __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
         if (j < T && ((active >> o) & 1u)) {
           const uint32_t tn = ws.tn[o];
           x[u] = vs_arc(p, ws.rb[o], ws.nb[o], ws.dx[o], ws.dy[o], ws.tb[o], tn & 0x7FFFFFFFu, (tn >> 31) != 0,
-                        j - lo, e[u]);
+                        kVsHead + (j - lo), e[u]);  // past the owner's head
         }
       }
       uint32_t m[kSlots][W];
@@ -471,9 +517,11 @@ __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
   const uint32_t nb = __ldcg(nbig);
   if (nb == 0) return true;
   // long rows: every warp takes 32 * kSlots-arc slices, the slices of row r
-  // starting at warp r (mod the warp count)
+  // starting at warp r (mod the warp count); a warp skips, from the listed
+  // length alone, the rows it has no slice of
   const uint32_t nw_ = nwarps(), gw = gwarp();
   for (uint32_t r = 0; r < nb; ++r) {
+    if ((gw + nw_ - r % nw_) % nw_ >= (__ldcg(&p.biglen[r]) + 32 * kSlots - 1) / (32 * kSlots)) continue;
     const uint32_t v = p.big[r];
     uint32_t vis[W];
 #pragma unroll
@@ -574,7 +622,11 @@ __device__ bool vs_push(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
     const VsRow r = vs_row(p, u);
     const uint32_t total = r.nb + r.dy + r.tn;
     if (total >= kVsBigPush) {  // a hub: the whole grid, after the barrier
-      if (lane == 0) p.big[atomicAdd(nbig, 1u)] = u;
+      if (lane == 0) {
+        const uint32_t slot = atomicAdd(nbig, 1u);
+        p.big[slot] = u;
+        p.biglen[slot] = total;
+      }
       continue;
     }
     uint32_t fw[W];
@@ -584,13 +636,20 @@ __device__ bool vs_push(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
   }
   if (!vs_sync(p)) return false;
   const uint32_t nb = __ldcg(nbig);
-  for (uint32_t j = 0; j < nb; ++j) {  // every warp takes 32-arc slices of each hub row
+  // hub rows: kVsPushSlice-arc slices, the slices of row j starting at warp j
+  // (mod the warp count); a warp skips the rows it has no slice of
+  const uint32_t nw = nwarps(), gw = gwarp();
+  for (uint32_t j = 0; j < nb; ++j) {
+    const uint32_t total = __ldcg(&p.biglen[j]);
+    const uint32_t nsl = (total + kVsPushSlice - 1) / kVsPushSlice;
+    uint32_t sl = (gw + nw - j % nw) % nw;
+    if (sl >= nsl) continue;
     const uint32_t u = p.big[j];
     const VsRow r = vs_row(p, u);
     uint32_t fw[W];
-#pragma unroll
-    for (uint32_t w = 0; w < W; ++w) fw[w] = fc[(size_t)u * W + w];
-    vs_push_arcs<W>(p, r, fw, gwarp() * 32, r.nb + r.dy + r.tn, nwarps() * 32, tn);
+    load_words<W>(fc + (size_t)u * W, fw);
+    for (; sl < nsl; sl += nw)
+      vs_push_arcs<W>(p, r, fw, sl * kVsPushSlice, min(total, (sl + 1) * kVsPushSlice), 32, tn);
   }
   if (nb && !vs_sync(p)) return false;
   vs_finalize<W>(p, p.tl, __ldcg(tn), fn, level, qn, qout, s, sdig, true);
@@ -712,7 +771,8 @@ void VersionBufs::free_all() {
                    (void**)&pos,  (void**)&tu,       (void**)&tx,     (void**)&tmask,    (void**)&tpre,
                    (void**)&trow, (void**)&boff,     (void**)&vlen,   (void**)&vis,      (void**)&frn[0],
                    (void**)&frn[1], (void**)&frn[2], (void**)&nxt,    (void**)&touched,  (void**)&q[0],
-                   (void**)&q[1], (void**)&q[2],     (void**)&tl,     (void**)&big,      (void**)&dig,
+                   (void**)&q[1], (void**)&q[2],     (void**)&tl,     (void**)&big,      (void**)&biglen,
+                   (void**)&dig,
                    (void**)&bucket, (void**)&ctr,    (void**)&barrier};
   for (void** x : ptrs) {
     cudaFree(*x);
@@ -757,6 +817,7 @@ int VersionBufs::ensure(size_t ops, size_t V, size_t words, size_t k) {
   al(&touched, bw, 4);
   al(&tl, NV, 4);
   al(&big, NV, 4);
+  al(&biglen, NV, 4);
   al(&dig, NK, 8);
   al(&bucket, NK, 8);
   al(&ctr, 1, sizeof(VsCounters));
@@ -931,11 +992,12 @@ int stream_versions(Bfs* b, const uint32_t* d_src, const uint32_t* d_dst, const 
   p.touched = S.touched;
   p.tl = S.tl;
   p.big = S.big;
+  p.biglen = S.biglen;
   p.dig = digests ? S.dig : nullptr;
   p.bucket = S.bucket;
   p.c = S.ctr;
   p.bar = S.barrier;
-  p.pull_frac = 0.02f;
+  p.pull_frac = b->tune.window_pull_frac;
   int rc = 0;
   switch (words) {
     case 1: rc = launch_versions<1>(S, p, slot, st); break;

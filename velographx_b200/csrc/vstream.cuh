@@ -53,6 +53,7 @@ struct VersionBufs {
   uint32_t* q[3] = {nullptr, nullptr, nullptr};
   uint32_t* tl = nullptr;
   uint32_t* big = nullptr;
+  uint32_t* biglen = nullptr;
   unsigned long long* dig = nullptr;     // [k] digest deltas, a difference array over the versions
   unsigned long long* bucket = nullptr;  // [k] unreachable terms by first version
   VsCounters* ctr = nullptr;
