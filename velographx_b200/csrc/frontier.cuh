@@ -52,6 +52,27 @@ __device__ __forceinline__ void load_words(const uint32_t* base, uint32_t* out) 
   }
 }
 
+// The listed rows (lengths len[0, n)) of which this warp holds a slice, when
+// row r is cut into slices of `slice` arcs and its slices are dealt to the
+// warps starting at warp r (mod the warp count): f(r, len_r, first slice)
+// for each, warp-uniformly.  The lengths are read 32 at a time, so a warp
+// passes the rows it has no slice of without a round trip per row.
+template <class F>
+__device__ __forceinline__ void for_my_rows(const uint32_t* len, uint32_t n, uint32_t slice, F&& f) {
+  const uint32_t lane = threadIdx.x & 31, nw = nwarps(), gw = gwarp();
+  for (uint32_t r0 = 0; r0 < n; r0 += 32) {
+    const uint32_t r = r0 + lane;
+    const uint32_t l = r < n ? __ldcg(&len[r]) : 0u;
+    const uint32_t s0 = (gw + nw - r % nw) % nw;
+    uint32_t mine = __ballot_sync(0xFFFFFFFFu, r < n && s0 < (l + slice - 1) / slice);
+    while (mine) {
+      const uint32_t k = __ffs(mine) - 1;
+      mine &= mine - 1;
+      f(r0 + k, __shfl_sync(0xFFFFFFFFu, l, k), __shfl_sync(0xFFFFFFFFu, s0, k));
+    }
+  }
+}
+
 // --------------------------------------------------- row expansion core --
 
 constexpr uint32_t FULL = 0xFFFFFFFFu;

@@ -27,6 +27,11 @@ using namespace frontier;
 
 constexpr int kThreads = 512;
 
+// The block's staging of frontier and touched-list appends: one global
+// atomic per block per phase instead of one per warp step (the appends of a
+// level that reaches millions of vertices serialised on one counter).
+__shared__ BlockQueue mr_bq;
+
 struct MrParams {
   vxb::DevGraph g;
   uint32_t V, K, W;
@@ -96,8 +101,7 @@ struct PushVisit {
         fresh = !(__ldcg(&p->touched[x >> 5]) & bit) && !(atomicOr(&p->touched[x >> 5], bit) & bit);
       }
     }
-    const uint32_t s = vxb::warp_append(fresh, tcount);
-    if (fresh) p->tl[s] = x;
+    bq_push(mr_bq, fresh, x, tcount, p->tl);
   }
 };
 
@@ -295,10 +299,10 @@ __device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, 
       }
     }
     write_dists_warp<W>(p, v, acc, level + 1);
-    const uint32_t slot = vxb::warp_append(any, qn);
-    if (any) qout[slot] = v;
+    bq_push(mr_bq, any, v, qn, qout);
     __syncwarp();  // the next group overwrites the stage
   }
+  bq_flush(mr_bq, qn, qout);
   if (!mr_sync(p)) return false;
   const uint32_t nb = __ldcg(nbig);
   if (nb == 0) return true;
@@ -306,8 +310,7 @@ __device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, 
   // start at warp r (mod the warp count) so the rows spread over the grid.  A
   // warp skips, from the listed length alone, the rows it has no slice of.
   const uint32_t nw = nwarps(), gw = gwarp();
-  for (uint32_t r = 0; r < nb; ++r) {
-    if ((gw + nw - r % nw) % nw >= (__ldcg(&p.biglen[r]) + 32 * kMrU - 1) / (32 * kMrU)) continue;
+  for_my_rows(p.biglen, nb, 32 * kMrU, [&](uint32_t r, uint32_t, uint32_t) {
     const uint32_t v = p.big[r];
     uint32_t vis[W];
 #pragma unroll
@@ -345,7 +348,7 @@ __device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, 
         if (lane == 0 && red) atomicOr(&p.nxt[(size_t)v * W + w], red);
       }
     }
-  }
+  });
   if (!mr_sync(p)) return false;
   for (uint32_t r = gtid(); r < nb; r += nthreads()) {
     const uint32_t v = p.big[r];
@@ -370,6 +373,8 @@ template <uint32_t W>
 __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
   __shared__ MrWarpStage stage[kMrWarps];
   MrCounters* c = p.c;
+  if (threadIdx.x == 0) mr_bq.cnt = 0;
+  __syncthreads();
   // roots (queued once per distinct vertex)
   for (uint32_t r = gtid(); r < p.K; r += nthreads()) {
     const uint32_t v = p.roots[r];
@@ -438,16 +443,14 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
         for (uint32_t w = 0; w < W; ++w) pv.fw[w] = fc[(size_t)u * W + w];
         warp_row(a, u, pv);
       }
+      bq_flush(mr_bq, &c->tn[cur], p.tl);
       if (!mr_sync(p)) return;
       const uint32_t nbig = __ldcg(&c->nbig[cur]);
       // hub rows: kMrPushSlice-arc slices, the slices of row r starting at
       // warp r (mod the warp count); a warp skips the rows it has no slice of
-      const uint32_t nw = nwarps(), gw = gwarp();
-      for (uint32_t r = 0; r < nbig; ++r) {
-        const uint32_t deg = __ldcg(&p.biglen[r]);
+      const uint32_t nw = nwarps();
+      for_my_rows(p.biglen, nbig, kMrPushSlice, [&](uint32_t r, uint32_t deg, uint32_t sl) {
         const uint32_t nsl = (deg + kMrPushSlice - 1) / kMrPushSlice;
-        uint32_t sl = (gw + nw - r % nw) % nw;
-        if (sl >= nsl) continue;
         const uint32_t u = p.big[r];
 #pragma unroll
         for (uint32_t w = 0; w < W; ++w) pv.fw[w] = fc[(size_t)u * W + w];
@@ -464,7 +467,8 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
             pv(!(x & kTomb), x & kIdMask, u);
           }
         }
-      }
+      });
+      bq_flush(mr_bq, &c->tn[cur], p.tl);
       if (nbig && !mr_sync(p)) return;
       // the touched heads' new roots, in warp-uniform rounds so the next
       // frontier is appended one atomic per warp (per head, the appends of
@@ -488,9 +492,9 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
           }
           p.touched[x >> 5] = 0u;
         }
-        const uint32_t slot = vxb::warp_append(any, &c->qn[nx]);
-        if (any) p.q[nx][slot] = x;
+        bq_push(mr_bq, any, x, &c->qn[nx], p.q[nx]);
       }
+      bq_flush(mr_bq, &c->qn[nx], p.q[nx]);
       if (!mr_sync(p)) return;
     }
     prev_n = n_f;

@@ -45,6 +45,10 @@ namespace {
 using namespace frontier;
 
 constexpr int kVsThreads = 512;
+
+// The block's staging of frontier and touched-list appends: one global
+// atomic per block per phase instead of one per warp step.
+__shared__ BlockQueue vs_bq;
 constexpr uint32_t kVsWarps = kVsThreads / 32;
 // 32-vertex groups a warp claims per atomic of a pull level (one counter
 // per level: a claim per group serialised on it)
@@ -332,9 +336,9 @@ __device__ void vs_finalize(const VsParams& p, const uint32_t* list, uint32_t n,
     if (valid && touched) p.touched[x >> 5] = 0u;
     const bool any = valid && vs_discover<W>(p, x, vis, nw, fn, level + 1, s);
     if (p.dig && valid) vs_digest<W>(p, x, nw, level + 1, s, sdig);
-    const uint32_t slot = vxb::warp_append(any, qn);
-    if (any) qout[slot] = x;
+    bq_push(vs_bq, any, x, qn, qout);
   }
+  bq_flush(vs_bq, qn, qout);
 }
 
 template <uint32_t W>
@@ -509,10 +513,10 @@ __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
     for (uint32_t w = 0; w < W; ++w) nw[w] = ws.acc[lane * W + w] & ~vis[w];
     const bool any = v < p.V && vs_discover<W>(p, v, vis, nw, fn, level + 1, s);
     if (p.dig && v < p.V) vs_digest<W>(p, v, nw, level + 1, s, sdig);
-    const uint32_t slot = vxb::warp_append(any, qn);
-    if (any) qout[slot] = v;
+    bq_push(vs_bq, any, v, qn, qout);
     __syncwarp();  // the next group overwrites the stage
   }
+  bq_flush(vs_bq, qn, qout);
   if (!vs_sync(p)) return false;
   const uint32_t nb = __ldcg(nbig);
   if (nb == 0) return true;
@@ -520,8 +524,7 @@ __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
   // starting at warp r (mod the warp count); a warp skips, from the listed
   // length alone, the rows it has no slice of
   const uint32_t nw_ = nwarps(), gw = gwarp();
-  for (uint32_t r = 0; r < nb; ++r) {
-    if ((gw + nw_ - r % nw_) % nw_ >= (__ldcg(&p.biglen[r]) + 32 * kSlots - 1) / (32 * kSlots)) continue;
+  for_my_rows(p.biglen, nb, 32 * kSlots, [&](uint32_t r, uint32_t, uint32_t) {
     const uint32_t v = p.big[r];
     uint32_t vis[W];
 #pragma unroll
@@ -565,7 +568,7 @@ __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
         if (lane == 0 && red) atomicOr(&p.nxt[(size_t)v * W + w], red);
       }
     }
-  }
+  });
   if (!vs_sync(p)) return false;
   vs_finalize<W>(p, p.big, nb, fn, level, qn, qout, s, sdig, false);
   return vs_sync(p);
@@ -607,8 +610,7 @@ __device__ __forceinline__ void vs_push_arcs(const VsParams& p, const VsRow& r, 
         }
       }
     }
-    const uint32_t sl = vxb::warp_append(fresh, tcount);
-    if (fresh) p.tl[sl] = x;
+    bq_push(vs_bq, fresh, x, tcount, p.tl);
   }
 }
 
@@ -634,23 +636,22 @@ __device__ bool vs_push(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
     for (uint32_t w = 0; w < W; ++w) fw[w] = fc[(size_t)u * W + w];
     vs_push_arcs<W>(p, r, fw, 0, total, 32, tn);
   }
+  bq_flush(vs_bq, tn, p.tl);
   if (!vs_sync(p)) return false;
   const uint32_t nb = __ldcg(nbig);
   // hub rows: kVsPushSlice-arc slices, the slices of row j starting at warp j
   // (mod the warp count); a warp skips the rows it has no slice of
-  const uint32_t nw = nwarps(), gw = gwarp();
-  for (uint32_t j = 0; j < nb; ++j) {
-    const uint32_t total = __ldcg(&p.biglen[j]);
+  const uint32_t nw = nwarps();
+  for_my_rows(p.biglen, nb, kVsPushSlice, [&](uint32_t j, uint32_t total, uint32_t sl) {
     const uint32_t nsl = (total + kVsPushSlice - 1) / kVsPushSlice;
-    uint32_t sl = (gw + nw - j % nw) % nw;
-    if (sl >= nsl) continue;
     const uint32_t u = p.big[j];
     const VsRow r = vs_row(p, u);
     uint32_t fw[W];
     load_words<W>(fc + (size_t)u * W, fw);
     for (; sl < nsl; sl += nw)
       vs_push_arcs<W>(p, r, fw, sl * kVsPushSlice, min(total, (sl + 1) * kVsPushSlice), 32, tn);
-  }
+  });
+  bq_flush(vs_bq, tn, p.tl);
   if (nb && !vs_sync(p)) return false;
   vs_finalize<W>(p, p.tl, __ldcg(tn), fn, level, qn, qout, s, sdig, true);
   return vs_sync(p);
@@ -662,6 +663,7 @@ __global__ void __launch_bounds__(kVsThreads, 2) vs_bfs_kernel(VsParams p) {
   __shared__ unsigned long long sdig[kMaxVersions];
   VsCounters* c = p.c;
   VsSums s;
+  if (threadIdx.x == 0) vs_bq.cnt = 0;
   for (uint32_t i = threadIdx.x; i < p.K; i += blockDim.x) sdig[i] = 0ull;
   // the source is reached at the window's start (the object's distances are
   // still the pre-window ones here)
