@@ -258,7 +258,8 @@ int vx_bfs_set_stream_window(vx_bfs* b, uint32_t batches);
  * counterpart (diagnostics). */
 int vx_bfs_window_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
 /* A version-parallel window's level pulls (bottom-up) when its frontier
- * holds more than frac * V vertices (default 0.02).  Same results for every
+ * holds more than frac * V vertices (default 0.02), or when its frontier's
+ * rows hold more than a twelfth of the graph's arcs.  Same results for every
  * value.  No reference counterpart. */
 int vx_bfs_set_window_pull_fraction(vx_bfs* b, float frac);
 /* fused != 0 (default): an undirected batch's commit and repair run in one
@@ -310,7 +311,10 @@ int vx_mrbfs_levels(vx_mrbfs* m, uint32_t* out);
  * timestamp; copies min(cap, *n) values, *n = 2 * levels + 1.  No reference
  * counterpart (diagnostics). */
 int vx_mrbfs_level_trace(vx_mrbfs* m, uint64_t* out, size_t cap, size_t* n);
-/* Pull (bottom-up) when the frontier holds more than frac * V vertices. */
+/* A level pulls (bottom-up) when its frontier holds more than frac * V
+ * vertices (default 0.02), or when its frontier's rows hold more than a
+ * twelfth of the graph's arcs (pushing an arc costs about twelve pulled
+ * ones). */
 int vx_mrbfs_set_pull_fraction(vx_mrbfs* m, float frac);
 /* One-shot form: create, run, copy k*V distances into out (cap entries). */
 int vx_multiroot_bfs(vx_graph* g, const uint32_t* roots, size_t k, uint32_t* out, size_t cap);

@@ -31,6 +31,24 @@ constexpr int kThreads = 512;
 // atomic per block per phase instead of one per warp step (the appends of a
 // level that reaches millions of vertices serialised on one counter).
 __shared__ BlockQueue mr_bq;
+// The block's sum of the out-degrees of the vertices it adds to the next
+// frontier (the push cost of the next level).
+__shared__ unsigned long long mr_mf;
+
+// A level pulls when pushing its frontier's rows would cost more than this
+// many times fewer arcs than the graph holds: a pushed arc (a visited check,
+// a next-word check, an atomic) costs about this many pulled arcs.
+constexpr unsigned long long kPushArcCost = 12;
+
+// Block-uniform: the block's frontier-degree sum added to *dst.
+__device__ __forceinline__ void mf_flush(unsigned long long* dst) {
+  __syncthreads();
+  if (threadIdx.x == 0 && mr_mf) {
+    atomicAdd(dst, mr_mf);
+    mr_mf = 0;
+  }
+  __syncthreads();
+}
 
 struct MrParams {
   vxb::DevGraph g;
@@ -49,6 +67,7 @@ struct MrParams {
   uint32_t* bar;
   uint32_t nblocks;
   float pull_frac;   // pull when the frontier holds more than V * pull_frac vertices
+  unsigned long long arcs;  // arcs of the graph (a pull level reads up to all of them)
 };
 
 __device__ __forceinline__ bool mr_sync(const MrParams& p) {
@@ -157,7 +176,7 @@ __device__ __forceinline__ void write_dists_warp(const MrParams& p, uint32_t v, 
 // levels).  Ends with a grid barrier; returns false when one failed.
 template <uint32_t W>
 __device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, uint32_t level, uint32_t* gnext,
-                           uint32_t* nbig, uint32_t* qn, uint32_t* qout, MrWarpStage& ws) {
+                           uint32_t* nbig, uint32_t* qn, uint32_t* qout, unsigned long long* mf, MrWarpStage& ws) {
   constexpr uint32_t kMrU = MrSlots<W>::value;
   const DevAdj& a = p.g.in;
   const uint32_t lane = threadIdx.x & 31;
@@ -180,13 +199,14 @@ __device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, 
       done = done && vis[w] == word_mask(p, w);
       ws.acc[lane * W + w] = 0u;
     }
-    uint32_t len = 0;
+    uint32_t len = 0, rowlen = 0;
     if (!done) {
       uint64_t b, e;
       vxb::base_range(a, v, b, e);
       const uint2 dr = a.drow[v];
       const uint32_t nb = (uint32_t)(e - b);
       len = nb + dr.y;
+      rowlen = len;
       if (len >= kMrBigPull) {  // the whole grid reads it after the barrier
         const uint32_t slot = atomicAdd(nbig, 1u);
         p.big[slot] = v;
@@ -300,9 +320,12 @@ __device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, 
     }
     write_dists_warp<W>(p, v, acc, level + 1);
     bq_push(mr_bq, any, v, qn, qout);
+    const unsigned long long dsum = vxb::warp_sum(any ? (unsigned long long)rowlen : 0ull);
+    if (lane == 0 && dsum) atomicAdd(&mr_mf, dsum);
     __syncwarp();  // the next group overwrites the stage
   }
   bq_flush(mr_bq, qn, qout);
+  mf_flush(mf);
   if (!mr_sync(p)) return false;
   const uint32_t nb = __ldcg(nbig);
   if (nb == 0) return true;
@@ -364,8 +387,12 @@ __device__ bool pull_level(const MrParams& p, const uint32_t* fc, uint32_t* fn, 
       fn[o] = m;
       write_dists(p, v, w, m, level + 1);
     }
-    if (any) qout[atomicAdd(qn, 1u)] = v;
+    if (any) {
+      qout[atomicAdd(qn, 1u)] = v;
+      atomicAdd(&mr_mf, (unsigned long long)p.biglen[r]);
+    }
   }
+  mf_flush(mf);
   return mr_sync(p);
 }
 
@@ -373,7 +400,10 @@ template <uint32_t W>
 __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
   __shared__ MrWarpStage stage[kMrWarps];
   MrCounters* c = p.c;
-  if (threadIdx.x == 0) mr_bq.cnt = 0;
+  if (threadIdx.x == 0) {
+    mr_bq.cnt = 0;
+    mr_mf = 0;
+  }
   __syncthreads();
   // roots (queued once per distinct vertex)
   for (uint32_t r = gtid(); r < p.K; r += nthreads()) {
@@ -383,7 +413,10 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
     atomicOr(&p.frn[0][(size_t)v * W + r / 32], 1u << (r & 31));
     p.dist[(size_t)r * p.V + v] = 0;
     const uint32_t bit = 1u << (v & 31);
-    if (!(atomicOr(&p.touched[v >> 5], bit) & bit)) p.q[0][atomicAdd(&c->qn[0], 1u)] = v;
+    if (!(atomicOr(&p.touched[v >> 5], bit) & bit)) {
+      p.q[0][atomicAdd(&c->qn[0], 1u)] = v;
+      atomicAdd(&c->mf[0], (unsigned long long)degree_of(p.g.out, v));
+    }
   }
   if (!mr_sync(p)) return;
   for (uint32_t i = gtid(); i < __ldcg(&c->qn[0]); i += nthreads()) p.touched[p.q[0][i] >> 5] = 0u;
@@ -403,6 +436,7 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
       c->tn[clr] = 0;
       c->nbig[clr] = 0;
       c->gnext[clr] = 0;
+      c->mf[clr] = 0;
     }
     // frontier words of level-1 are no longer read: clear them for reuse,
     // through its queue when it was small, else all of them with plain stores
@@ -413,7 +447,9 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
     }
     const uint32_t* fc = p.frn[cur];
     uint32_t* fn = p.frn[nx];
-    const bool pull = (float)n_f > p.pull_frac * (float)p.V;
+    // pull for a large frontier, or for one whose rows would cost more to
+    // push than reading up to every arc costs to pull
+    const bool pull = (float)n_f > p.pull_frac * (float)p.V || __ldcg(&c->mf[cur]) * kPushArcCost > p.arcs;
     if (gtid() == 0) {
       const uint32_t t = min(level, kMrTraceLevels - 1);
       c->trace[2 * t] = globaltimer();
@@ -422,7 +458,8 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
     if (pull) {
       // pull: every vertex not reached by all roots ORs its in-neighbours'
       // frontier words, stopping once all roots reached it
-      if (!pull_level<W>(p, fc, fn, level, &c->gnext[cur], &c->nbig[cur], &c->qn[nx], p.q[nx], stage[threadIdx.x >> 5]))
+      if (!pull_level<W>(p, fc, fn, level, &c->gnext[cur], &c->nbig[cur], &c->qn[nx], p.q[nx], &c->mf[nx],
+                         stage[threadIdx.x >> 5]))
         return;
     } else {
       // push along the rows of the queued frontier vertices, one warp each
@@ -493,8 +530,11 @@ __global__ void __launch_bounds__(kThreads, 2) mrbfs_kernel(MrParams p) {
           p.touched[x >> 5] = 0u;
         }
         bq_push(mr_bq, any, x, &c->qn[nx], p.q[nx]);
+        const unsigned long long dsum = vxb::warp_sum(any ? (unsigned long long)degree_of(p.g.out, x) : 0ull);
+        if ((threadIdx.x & 31) == 0 && dsum) atomicAdd(&mr_mf, dsum);
       }
       bq_flush(mr_bq, &c->qn[nx], p.q[nx]);
+      mf_flush(&c->mf[nx]);
       if (!mr_sync(p)) return;
     }
     prev_n = n_f;
@@ -614,6 +654,7 @@ int mrbfs_run(MrBfs* m) {
   p.bar = m->barrier;
   p.nblocks = (uint32_t)m->grid;
   p.pull_frac = m->pull_frac;
+  p.arcs = g->adj[0].A;
   void* args[] = {&p};
   count_launch();
   VX_CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(m->grid), dim3(kThreads), args, 0, s));

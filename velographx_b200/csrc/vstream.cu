@@ -49,6 +49,24 @@ constexpr int kVsThreads = 512;
 // The block's staging of frontier and touched-list appends: one global
 // atomic per block per phase instead of one per warp step.
 __shared__ BlockQueue vs_bq;
+// The block's sum of the degrees of the vertices it adds to the next frontier
+// (the push cost of the next level).
+__shared__ unsigned long long vs_mf;
+
+// A level pulls when pushing its frontier's rows would cost more than this
+// many times fewer arcs than the graph holds (a pushed arc costs about this
+// many pulled ones).
+constexpr unsigned long long kPushArcCost = 12;
+
+// Block-uniform: the block's frontier-degree sum added to *dst.
+__device__ __forceinline__ void mf_flush(unsigned long long* dst) {
+  __syncthreads();
+  if (threadIdx.x == 0 && vs_mf) {
+    atomicAdd(dst, vs_mf);
+    vs_mf = 0;
+  }
+  __syncthreads();
+}
 constexpr uint32_t kVsWarps = kVsThreads / 32;
 // 32-vertex groups a warp claims per atomic of a pull level (one counter
 // per level: a claim per group serialised on it)
@@ -87,6 +105,7 @@ struct VsParams {
   uint32_t* bar;
   uint32_t nblocks;
   float pull_frac;
+  unsigned long long arcs;  // arcs of the graph (a pull level reads up to all of them)
 };
 
 __device__ __forceinline__ bool vs_sync(const VsParams& p) {
@@ -316,7 +335,8 @@ __device__ __forceinline__ void vs_digest(const VsParams& p, uint32_t v, const u
 // (nxt cleared, and the touched bits when `touched`), in warp-uniform rounds.
 template <uint32_t W>
 __device__ void vs_finalize(const VsParams& p, const uint32_t* list, uint32_t n, uint32_t* fn, uint32_t level,
-                            uint32_t* qn, uint32_t* qout, VsSums& s, unsigned long long* sdig, bool touched) {
+                            uint32_t* qn, uint32_t* qout, unsigned long long* mf, VsSums& s, unsigned long long* sdig,
+                            bool touched) {
   const uint32_t lane = threadIdx.x & 31;
   for (uint32_t base = gwarp() * 32; base < n; base += nwarps() * 32) {
     const uint32_t i = base + lane;
@@ -337,8 +357,16 @@ __device__ void vs_finalize(const VsParams& p, const uint32_t* list, uint32_t n,
     const bool any = valid && vs_discover<W>(p, x, vis, nw, fn, level + 1, s);
     if (p.dig && valid) vs_digest<W>(p, x, nw, level + 1, s, sdig);
     bq_push(vs_bq, any, x, qn, qout);
+    unsigned long long deg = 0;
+    if (any) {
+      const VsRow r = vs_row(p, x);
+      deg = r.nb + r.dy + r.tn;
+    }
+    deg = vxb::warp_sum(deg);
+    if (lane == 0 && deg) atomicAdd(&vs_mf, deg);
   }
   bq_flush(vs_bq, qn, qout);
+  mf_flush(mf);
 }
 
 template <uint32_t W>
@@ -365,8 +393,8 @@ struct VsStage {
 // the whole grid after a barrier, through nxt.  Ends with a grid barrier.
 template <uint32_t W>
 __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uint32_t level, uint32_t* gnext,
-                        uint32_t* nbig, uint32_t* qn, uint32_t* qout, VsStage& ws, VsSums& s,
-                        unsigned long long* sdig) {
+                        uint32_t* nbig, uint32_t* qn, uint32_t* qout, unsigned long long* mf, VsStage& ws,
+                        VsSums& s, unsigned long long* sdig) {
   constexpr uint32_t kSlots = VsSlots<W>::value;
   const uint32_t lane = threadIdx.x & 31;
   uint32_t cur = 0, end = 0;  // the warp's claimed groups [cur, end), warp-uniform
@@ -388,10 +416,11 @@ __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
       done = done && vis[w] == vmask(p.K, w);
       ws.acc[lane * W + w] = 0u;
     }
-    uint32_t len = 0;
+    uint32_t len = 0, rowlen = 0;
     if (!done) {
       const VsRow r = vs_row(p, v);
       len = r.nb + r.dy + r.tn;
+      rowlen = len;
       if (len >= kVsBigPull) {  // the whole grid reads it after the barrier
         const uint32_t slot = atomicAdd(nbig, 1u);
         p.big[slot] = v;
@@ -514,9 +543,12 @@ __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
     const bool any = v < p.V && vs_discover<W>(p, v, vis, nw, fn, level + 1, s);
     if (p.dig && v < p.V) vs_digest<W>(p, v, nw, level + 1, s, sdig);
     bq_push(vs_bq, any, v, qn, qout);
+    const unsigned long long dsum = vxb::warp_sum(any ? (unsigned long long)rowlen : 0ull);
+    if (lane == 0 && dsum) atomicAdd(&vs_mf, dsum);
     __syncwarp();  // the next group overwrites the stage
   }
   bq_flush(vs_bq, qn, qout);
+  mf_flush(mf);
   if (!vs_sync(p)) return false;
   const uint32_t nb = __ldcg(nbig);
   if (nb == 0) return true;
@@ -570,7 +602,7 @@ __device__ bool vs_pull(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
     }
   });
   if (!vs_sync(p)) return false;
-  vs_finalize<W>(p, p.big, nb, fn, level, qn, qout, s, sdig, false);
+  vs_finalize<W>(p, p.big, nb, fn, level, qn, qout, mf, s, sdig, false);
   return vs_sync(p);
 }
 
@@ -616,8 +648,8 @@ __device__ __forceinline__ void vs_push_arcs(const VsParams& p, const VsRow& r, 
 
 template <uint32_t W>
 __device__ bool vs_push(const VsParams& p, const uint32_t* fc, uint32_t* fn, uint32_t level, uint32_t n_f,
-                        const uint32_t* qin, uint32_t* tn, uint32_t* nbig, uint32_t* qn, uint32_t* qout, VsSums& s,
-                        unsigned long long* sdig) {
+                        const uint32_t* qin, uint32_t* tn, uint32_t* nbig, uint32_t* qn, uint32_t* qout,
+                        unsigned long long* mf, VsSums& s, unsigned long long* sdig) {
   const uint32_t lane = threadIdx.x & 31;
   for (uint32_t i = gwarp(); i < n_f; i += nwarps()) {
     const uint32_t u = qin[i];
@@ -653,7 +685,7 @@ __device__ bool vs_push(const VsParams& p, const uint32_t* fc, uint32_t* fn, uin
   });
   bq_flush(vs_bq, tn, p.tl);
   if (nb && !vs_sync(p)) return false;
-  vs_finalize<W>(p, p.tl, __ldcg(tn), fn, level, qn, qout, s, sdig, true);
+  vs_finalize<W>(p, p.tl, __ldcg(tn), fn, level, qn, qout, mf, s, sdig, true);
   return vs_sync(p);
 }
 
@@ -663,7 +695,10 @@ __global__ void __launch_bounds__(kVsThreads, 2) vs_bfs_kernel(VsParams p) {
   __shared__ unsigned long long sdig[kMaxVersions];
   VsCounters* c = p.c;
   VsSums s;
-  if (threadIdx.x == 0) vs_bq.cnt = 0;
+  if (threadIdx.x == 0) {
+    vs_bq.cnt = 0;
+    vs_mf = 0;
+  }
   for (uint32_t i = threadIdx.x; i < p.K; i += blockDim.x) sdig[i] = 0ull;
   // the source is reached at the window's start (the object's distances are
   // still the pre-window ones here)
@@ -703,6 +738,8 @@ __global__ void __launch_bounds__(kVsThreads, 2) vs_bfs_kernel(VsParams p) {
                   vxb::mix64(((unsigned long long)p.source << 32) | kUnreachable);
     p.q[0][0] = p.source;
     c->qn[0] = 1;
+    const VsRow r = vs_row(p, p.source);
+    c->mf[0] = r.nb + r.dy + r.tn;
   }
   if (!vs_sync(p)) return;
   uint32_t prev_n = 0, level = 0;
@@ -719,6 +756,7 @@ __global__ void __launch_bounds__(kVsThreads, 2) vs_bfs_kernel(VsParams p) {
       c->tn[clr] = 0;
       c->nbig[clr] = 0;
       c->gnext[clr] = 0;
+      c->mf[clr] = 0;
     }
     // frontier words of level - 1 are no longer read: cleared through its
     // queue when it was small, else all of them
@@ -729,7 +767,9 @@ __global__ void __launch_bounds__(kVsThreads, 2) vs_bfs_kernel(VsParams p) {
     }
     const uint32_t* fc = p.frn[cur];
     uint32_t* fn = p.frn[nx];
-    const bool pull = (float)n_f > p.pull_frac * (float)p.V;
+    // pull for a large frontier, or for one whose rows would cost more to
+    // push than reading up to every arc costs to pull
+    const bool pull = (float)n_f > p.pull_frac * (float)p.V || __ldcg(&c->mf[cur]) * kPushArcCost > p.arcs;
     if (gtid() == 0) {
       const uint32_t t = min(level, 63u);
       c->trace[2 * t] = globaltimer();
@@ -737,10 +777,11 @@ __global__ void __launch_bounds__(kVsThreads, 2) vs_bfs_kernel(VsParams p) {
     }
     bool ok;
     if (pull)
-      ok = vs_pull<W>(p, fc, fn, level, &c->gnext[cur], &c->nbig[cur], &c->qn[nx], p.q[nx], stage[threadIdx.x >> 5],
-                      s, sdig);
+      ok = vs_pull<W>(p, fc, fn, level, &c->gnext[cur], &c->nbig[cur], &c->qn[nx], p.q[nx], &c->mf[nx],
+                      stage[threadIdx.x >> 5], s, sdig);
     else
-      ok = vs_push<W>(p, fc, fn, level, n_f, p.q[cur], &c->tn[cur], &c->nbig[cur], &c->qn[nx], p.q[nx], s, sdig);
+      ok = vs_push<W>(p, fc, fn, level, n_f, p.q[cur], &c->tn[cur], &c->nbig[cur], &c->qn[nx], p.q[nx], &c->mf[nx],
+                      s, sdig);
     if (!ok) return;
     prev_n = n_f;
   }
@@ -1000,6 +1041,7 @@ int stream_versions(Bfs* b, const uint32_t* d_src, const uint32_t* d_dst, const 
   p.c = S.ctr;
   p.bar = S.barrier;
   p.pull_frac = b->tune.window_pull_frac;
+  p.arcs = g->adj[0].A;
   int rc = 0;
   switch (words) {
     case 1: rc = launch_versions<1>(S, p, slot, st); break;

@@ -18,6 +18,7 @@ struct VsCounters {
   uint32_t tn[3];     // touched heads of a push level
   uint32_t nbig[3];   // rows of a level long enough for the whole grid
   uint32_t gnext[3];  // next 32-vertex group of a pull level
+  unsigned long long mf[3];  // arcs of the frontier's rows (the push cost of the level)
   uint32_t levels;
   uint32_t err;
   uint32_t seed;      // the source is reached at the window's start
