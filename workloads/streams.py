@@ -18,6 +18,7 @@ maintained distances against a fresh full BFS at regular batches.
 
   python -m workloads.streams --workload grid [--batches 500]
   python -m workloads.streams --workload lognormal [--scale 20]
+  python -m workloads.streams --workload window [--window 256] [--digests]
 """
 from __future__ import annotations
 
@@ -402,9 +403,45 @@ def lognormal(scale: int = 20, batches: int = 1000, median: float = 500.0, sigma
     return out
 
 
+def window_case(scale: int = 20, window: int = 256, digests: bool = False, repeats: int = 2, seed: int = 33) -> dict:
+    """The lognormal stream through apply_stream's version-parallel windows
+    alone (`window` batches per window), `repeats` times on fresh replicas:
+    the case the window kernel is profiled on."""
+    import torch
+
+    V = 1 << scale
+    edges = w.rmat_edges(scale, 16, seed=seed)
+    root = w.max_degree_root(edges, V)
+    sizes = w.lognormal_sizes(1000, median=500.0, sigma=2.0, lo=1, hi=200_000, seed=seed + 1)
+    st = pinned_stream(w.mixed_stream(edges, V, sizes, 0.8, seed=seed + 2))
+    off = st.offsets.astype(np.uint64)
+    e0, e1 = _events()
+    runs = []
+    for _ in range(repeats):
+        g = Graph(V, False)
+        g.bulk_load_edges(edges)
+        g.reserve(int(sizes.max()), int(st.offsets[-1]))
+        b = IncrementalBFS(g, root)
+        b.set_stream_window(window)
+        b.reserve_stream(int(st.offsets[-1]), len(sizes), int(sizes.max()))
+        cs = torch.cuda.ExternalStream(g.stream)
+        torch.cuda.synchronize()
+        e0.record(cs)
+        b.apply_stream(st.src, st.dst, st.add, off, digests=digests)
+        e1.record(cs)
+        torch.cuda.synchronize()
+        runs.append(len(sizes) / (e0.elapsed_time(e1) * 1e-3))
+        trace = b.window_trace()
+        del b, g
+    return {"workload": f"rmat{scale}-lognormal-1000-batches-window{window}", "batches_per_s_runs": runs,
+            "last_window_levels_us_nf_pull": [[round(a, 1), int(n), bool(q)] for a, n, q in trace]}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--workload", choices=["grid", "lognormal"], default="grid")
+    ap.add_argument("--workload", choices=["grid", "lognormal", "window"], default="grid")
+    ap.add_argument("--window", type=int, default=256)
+    ap.add_argument("--digests", action="store_true")
     ap.add_argument("--side", type=int, default=4096)
     ap.add_argument("--batches", type=int, default=500)
     ap.add_argument("--ops", type=int, default=1000)
@@ -413,7 +450,9 @@ def main():
     ap.add_argument("--sigma", type=float, default=2.0)
     a = ap.parse_args()
     t0 = time.time()
-    if a.workload == "lognormal":
+    if a.workload == "window":
+        res = window_case(a.scale, a.window, a.digests)
+    elif a.workload == "lognormal":
         res = lognormal(a.scale, batches=a.batches if a.batches != 500 else 1000, sigma=a.sigma)
     else:
         res = grid(a.side, batches=a.batches, ops=a.ops, check_every=a.check_every)
