@@ -175,7 +175,7 @@ int vx_bfs_reached_arcs(vx_bfs* b, uint64_t* out);
  * frontier size | bottom_up << 63}, then a closing timestamp; *n = entries.
  * No reference counterpart (diagnostics). */
 int vx_bfs_level_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
-/* Phase trace of the last incremental apply (27 entries): globaltimer ns at
+/* Phase trace of the last incremental apply (29 entries): globaltimer ns at
  * the pre-batch kernel's entry, after its seeds, after its cascade; at the
  * post-batch kernel's entry, after the boundary distances, after its seeds,
  * after the relaxation (0 = phase not run); the work items pushed by the
@@ -184,7 +184,9 @@ int vx_bfs_level_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
  * SM cycles spent processing (summed over blocks) and the longest round;
  * then the ns the last vx_bfs_apply_stream launch spent in each per-batch
  * phase (classify, removals, cascade, insertions, post-batch repair,
- * end-of-batch barrier), summed over its batches.  No reference counterpart
+ * end-of-batch barrier), summed over its batches; then the batches of the
+ * last apply or stream launch whose cascade, and whose relaxation, passed its
+ * work budget and handed over to a BFS.  No reference counterpart
  * (diagnostics). */
 int vx_bfs_phase_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
 /* A stream of update batches applied in order, with the same result after

@@ -1,0 +1,128 @@
+"""GPU: the work budgets of the incremental repair.
+
+On a deep graph one batch can move the distances of a large part of the graph.
+Two phases then hand over to a full BFS once they have processed
+max(V / 64, 16,384) work-ring items:
+
+- the post-batch relaxation (an inserted shortcut lowers half a lattice): the
+  rest of its queue is dropped and a full BFS of the post-batch graph gives the
+  distances and the reachable count;
+- the deletion cascade (a wall of deleted edges near the root raises a third of
+  a lattice): a BFS of the graph without the batch's deletions gives the
+  affected set (the vertices whose distance it raises), their count, and the
+  fallback decision; the post-batch repair then only relaxes the insertions.
+
+Either way the batch's counters are the ones the reference's
+IncrementalBFS::apply reports, checked here batch by batch on both the fused
+and the per-phase path.  Entries 27 and 28 of the phase trace count the
+batches whose cascade and whose relaxation handed over.
+"""
+import numpy as np
+import pytest
+
+from oracle import OracleBFS, OracleGraph
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import velographx_b200 as vx  # noqa: E402
+import workloads as w  # noqa: E402
+
+CASCADE, RELAX = 27, 28  # phase-trace entries of the handover counts
+
+
+def lattice_batches(side):
+    """Batches on a side x side lattice rooted at corner 0: a shortcut from
+    the root to the far corner (lowers about half the lattice), its removal
+    (raises them again), a shortcut to the middle together with deletions
+    near the root, and a quiet batch."""
+    far, mid = side * side - 1, (side // 2) * side + side // 2
+    return [
+        (np.array([0], np.uint32), np.array([far], np.uint32), np.array([1], np.uint8)),
+        (np.array([0], np.uint32), np.array([far], np.uint32), np.array([0], np.uint8)),
+        (np.array([0, 0, 1, side], np.uint32), np.array([mid, 1, 2, 2 * side], np.uint32),
+         np.array([1, 0, 0, 0], np.uint8)),
+        (np.array([5], np.uint32), np.array([6], np.uint32), np.array([0], np.uint8)),
+    ]
+
+
+def wall(side, cols, add=()):
+    """Deletes the edges between rows 0 and 1 in columns [0, cols): every
+    vertex below the wall in those columns loses all its shortest paths
+    ((side - 1) * cols affected vertices); add lists extra insertions."""
+    s = [np.arange(cols, dtype=np.uint32)]
+    d = [np.arange(cols, dtype=np.uint32) + side]
+    a = [np.zeros(cols, np.uint8)]
+    for u, v in add:
+        s.append(np.array([u], np.uint32))
+        d.append(np.array([v], np.uint32))
+        a.append(np.array([1], np.uint8))
+    return np.concatenate(s), np.concatenate(d), np.concatenate(a)
+
+
+def restore_wall(side, cols):
+    return (np.arange(cols, dtype=np.uint32), np.arange(cols, dtype=np.uint32) + side,
+            np.ones(cols, np.uint8))
+
+
+def run_against_reference(side, batches, fused, expect=None):
+    """Applies batches to the device and the reference, comparing distances
+    and counters after each; expect[t] = (cascade, relax) handovers of batch t
+    (None: not checked)."""
+    V = side * side
+    edges = w.grid_edges(side, side, 0.0, seed=3)
+    g = vx.Graph(V, False)
+    g.bulk_load_edges(edges)
+    b = vx.IncrementalBFS(g, 0)
+    b.set_fused(fused)
+    og = OracleGraph(V, False)
+    og.bulk_load_edges(edges)
+    ob = OracleBFS(og, 0)
+    for t, (s, d, a) in enumerate(batches):
+        b.apply_arrays(s, d, a)
+        ob.apply(s, d, a)
+        assert np.array_equal(b.distances_array(), ob.distances()), t
+        st = b.stats()
+        r, c, af, full = ob.stats()
+        assert st["reachable_count"] == r, t
+        assert st["last_deletion_candidates"] == c, t
+        assert st["last_used_full_recompute"] == bool(full), t
+        if not full:
+            assert st["last_affected_vertices"] == af, t
+        if expect is not None and expect[t] is not None:
+            tr = b.phase_trace()
+            want_c, want_r = expect[t]
+            assert tr[CASCADE] == want_c, (t, tr[CASCADE:])
+            if want_r is not None:
+                assert tr[RELAX] == want_r, (t, tr[CASCADE:])
+
+
+@pytest.mark.parametrize("fused", [True, False])
+def test_relaxation_past_its_budget_matches_the_reference(fused):
+    side = 256
+    quiet = (np.array([7], np.uint32), np.array([8], np.uint32), np.array([0], np.uint8))
+    # the shortcut's relaxation hands over; a later batch runs from a clean workspace
+    run_against_reference(side, lattice_batches(side) + [quiet], fused,
+                          expect=[(0, 1), None, None, None, (0, 0)])
+
+
+@pytest.mark.parametrize("fused", [True, False])
+def test_cascade_past_its_budget_matches_the_reference(fused):
+    side = 512  # V = 262,144: budget 16,384 items, fallback above 91,750 affected
+    far = side * side - 1
+    unlink = (np.array([0], np.uint32), np.array([far], np.uint32), np.array([0], np.uint8))
+    batches = [
+        wall(side, 150),                    # 76,650 affected (29%): the BFS gives the set
+        restore_wall(side, 150),            # insertions only
+        wall(side, 150, add=[(0, far)]),    # the same wall and a shortcut in one batch
+        tuple(np.concatenate(x) for x in zip(restore_wall(side, 150), unlink)),  # the shortcut's region
+        wall(side, 200),                    # 102,200 affected (39%): the BFS decides the fallback
+        restore_wall(side, 200),
+        wall(side, 3),                      # 1,533 affected: the cascade finishes within its budget
+        (np.array([9], np.uint32), np.array([10], np.uint32), np.array([0], np.uint8)),
+    ]
+    expect = [(1, 0), (0, None), (1, None), (1, None), (1, 0), (0, None), (0, 0), (0, 0)]
+    run_against_reference(side, batches, fused, expect=expect)

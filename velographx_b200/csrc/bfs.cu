@@ -77,6 +77,9 @@ struct Params {
   BfsCounters* c;
   unsigned long long total_arcs;
   unsigned long long fallback_limit;
+  uint32_t relax_budget;    // ring items the post-batch relaxation may process before a full BFS takes over
+  uint32_t cascade_budget;  // ring items the cascade may process before a BFS of the graph without the
+                            // batch's deletions takes over (kNoBudget: never)
   float alpha, beta;
   uint32_t large_row;
   uint32_t nblocks;
@@ -89,6 +92,14 @@ struct Params {
 };
 
 constexpr uint32_t kTraceLevels = 256;
+
+// The cascade's budget: as many ring items as the relaxation's.  The BFS that
+// takes over compares distances over the whole phase graph, so it is used only
+// when the distance vector spans the graph's vertices.
+constexpr uint32_t kNoBudget = 0xFFFFFFFFu;
+__host__ __device__ inline uint32_t cascade_budget(uint32_t V, uint32_t dist_len) {
+  return dist_len == V ? (V / 64 > 16384u ? V / 64 : 16384u) : kNoBudget;
+}
 
 __device__ __forceinline__ void acct_add(const Params& p, int k, unsigned long long v) {
   if (p.acct && v) atomicAdd(&p.acct[k], v);
@@ -106,6 +117,7 @@ __device__ __forceinline__ bool sync_grid(const Params& p) {
 
 struct TdVisit {
   const Params* p;
+  uint32_t* dist;
   uint32_t level;
   uint32_t* qout;
   uint32_t* fbn;
@@ -127,7 +139,7 @@ struct TdVisit {
       }
     }
     if (claim) {
-      p->dist[x] = level + 1;
+      dist[x] = level + 1;
       atomicOr(&fbn[x >> 5], bit);
     }
     bq_push(*bq, claim, x, cnt_n, qout);
@@ -318,9 +330,9 @@ __device__ __forceinline__ void seg_append(bool pred, uint32_t v, uint32_t* seg,
 // scans only the vertices still unreached.  Entries are loaded two groups
 // ahead and their visited words and row bounds one group ahead, so those
 // loads are in flight while a group is scanned.  Block-uniform.
-__device__ void bu_list_level(const Params& p, uint32_t level, const uint32_t* fbc, uint32_t* fbn, uint32_t* qout,
-                              uint32_t* cnt_n, BlockQueue& bq, const uint32_t* lin, uint32_t nin, uint32_t* lout,
-                              uint32_t* nout) {
+__device__ void bu_list_level(const Params& p, uint32_t* dist, uint32_t level, const uint32_t* fbc, uint32_t* fbn,
+                              uint32_t* qout, uint32_t* cnt_n, BlockQueue& bq, const uint32_t* lin, uint32_t nin,
+                              uint32_t* lout, uint32_t* nout) {
   const DevAdj& a = p.g.in;
   const int lane = threadIdx.x & 31;
   const uint32_t step = kThreads;  // the block's warps take consecutive 32-entry groups
@@ -395,7 +407,7 @@ __device__ void bu_list_level(const Params& p, uint32_t level, const uint32_t* f
       }
       if (lane == l) found = hit_l;
     }
-    if (found) p.dist[v] = level + 1;
+    if (found) dist[v] = level + 1;
     // visited and next-frontier bits: OR-combined over runs of lanes on the
     // same bitmap word (list entries come in ascending runs), one atomic per
     // run; a word that recurs outside its run is ORed again, which is harmless
@@ -420,7 +432,8 @@ __device__ void bu_list_level(const Params& p, uint32_t level, const uint32_t* f
 
 // ------------------------------------------------------------ full BFS --
 
-__device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
+__device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst, uint32_t* dist,
+                         unsigned long long* trace) {
   BfsCounters* c = p.c;
   __shared__ uint32_t seg_n[2];  // entries of this block's segment of each candidate list
   if (threadIdx.x == 0) bq.cnt = 0;
@@ -443,7 +456,7 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
     const uint32_t i = i0 + threadIdx.x;
     bool cand = false;
     if (i < seg_hi) {
-      p.dist[i] = i == s ? 0u : kUnreachable;
+      dist[i] = i == s ? 0u : kUnreachable;
       cand = has_source && i != s && degree_of(p.g.in, i) != 0u;
     }
     seg_append(cand, i, p.bul + seg_lo, &seg_n[0]);
@@ -503,9 +516,9 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
       c->lvl_n[clr] = 0;
       c->lvl_m[clr] = 0;
       c->lvl_big[clr] = 0;
-      if (p.trace && level < kTraceLevels) {
-        p.trace[2 * level] = globaltimer();
-        p.trace[2 * level + 1] = (unsigned long long)n_f | ((unsigned long long)bottom_up << 63);
+      if (trace && level < kTraceLevels) {
+        trace[2 * level] = globaltimer();
+        trace[2 * level + 1] = (unsigned long long)n_f | ((unsigned long long)bottom_up << 63);
       }
     }
     // clear the frontier bitmap of level-1: through its queue when it was
@@ -519,7 +532,7 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
       const uint32_t lout = lin ^ 1u;
       if (threadIdx.x == 0) seg_n[lout] = 0;
       __syncthreads();
-      bu_list_level(p, level, p.fb[cur], p.fb[nxt], p.q[nxt], &c->lvl_n[nxt], bq, p.bul + lin * p.bul_half + seg_lo,
+      bu_list_level(p, dist, level, p.fb[cur], p.fb[nxt], p.q[nxt], &c->lvl_n[nxt], bq, p.bul + lin * p.bul_half + seg_lo,
                     seg_n[lin], p.bul + lout * p.bul_half + seg_lo, &seg_n[lout]);
       lin = lout;
       if (!sync_grid(p)) return;
@@ -527,7 +540,7 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
       n_f = ld_cg(&c->lvl_n[nxt]);
       m_f = __ldcg(&c->lvl_m[nxt]);
     } else {
-      TdVisit t{&p, level, p.q[nxt], p.fb[nxt], &c->lvl_n[nxt], !left_bu, 0ull, &bq};
+      TdVisit t{&p, dist, level, p.q[nxt], p.fb[nxt], &c->lvl_n[nxt], !left_bu, 0ull, &bq};
       if (n_f <= kLbMax) td_level_lb(p, t, p.q[cur], n_f, lbst);
       else td_level(p, t, p.q[cur], n_f, &c->lvl_big[cur]);
       t.flush(&c->lvl_m[nxt]);
@@ -552,9 +565,9 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst) {
     c->reachable = reached;
     c->levels = level;
     c->arcs = m_visited;
-    if (p.trace && level < kTraceLevels) {
-      p.trace[2 * level] = globaltimer();
-      p.trace[2 * level + 1] = 0;
+    if (trace && level < kTraceLevels) {
+      trace[2 * level] = globaltimer();
+      trace[2 * level + 1] = 0;
     }
   }
 }
@@ -994,9 +1007,10 @@ __device__ void check_vertex(const Params& p, uint32_t x) {
     // claiming an expand item
     __syncwarp();
     __threadfence();
-    // past the fallback limit the block path drops expansions; so does this one
+    // past the fallback limit or the budget the block path drops
+    // expansions; so does this one
     const uint32_t odeg = degree_of(p.g.out, x);
-    if (odeg <= kInlineExpand && !ld_cg(&p.c->fallback)) {
+    if (odeg <= kInlineExpand && !(ld_cg(&p.c->fallback) | ld_cg(&p.c->cbig))) {
       if (lane == 0) acct_add(p, 0, odeg);
       ExpandChildren ec{&p, x, d};
       warp_row(p.g.out, x, ec);
@@ -1068,7 +1082,10 @@ struct Cascade {
     if (t == 0) {
       sm.nsv = 0;
       sm.nex = 0;
-      sm.fallback = ld_cg(&c->fallback);
+      // past its budget the cascade drops the rest of its queue like the
+      // fallback does; a BFS then gives the affected set (cascade_by_bfs)
+      if (ld_cg(P.rq_done) > P.cascade_budget && !ld_cg(&c->cbig)) atomicOr(&c->cbig, 1u);
+      sm.fallback = ld_cg(&c->fallback) | ld_cg(&c->cbig);
     }
     __syncthreads();
     if (t < n) {
@@ -1090,7 +1107,8 @@ struct Cascade {
     __threadfence();  // expand items were pushed after their affected bits
     __syncthreads();
     if (sm.fallback) {
-      // past the fallback limit: drop the items, keeping the request bits clear
+      // past the fallback limit or the budget: drop the items, keeping the
+      // request bits clear
       for (uint32_t i = t; i < sm.nsv; i += kThreads)
         if (sm.cnt[i] == 0u) atomicAnd(&P.inq[1][sm.sv[i] >> 5], ~(1u << (sm.sv[i] & 31)));
       return;
@@ -1155,11 +1173,65 @@ __device__ void register_candidates(const Params& p) {
   }
 }
 
+__device__ void clear_workspace(const Params& p);
+
+// The cascade past its budget (a cut near the root of a deep graph leaves
+// millions of vertices affected, and the cascade walks them level by level).
+// A vertex keeps its distance through the batch's deletions iff one of its
+// shortest paths survives them, i.e. iff it has a surviving parent that is not
+// affected itself: the affected vertices are exactly those whose distance in
+// the graph without the deletions exceeds their old one.  One BFS of that graph
+// (the deletions are committed, the insertions not yet) gives them: its
+// distances replace the old ones, the count of raised vertices is the batch's
+// affected count (and decides the fallback as the cascade's would), and the
+// affected list stays empty, so the post-batch repair only relaxes the
+// insertions.  The BFS distances go to tent (zero between phases), which the
+// comparison pass zeroes again.
+__device__ bool cascade_by_bfs(const Params& p, BlockQueue& bq, LbStage& lb) {
+  BfsCounters* c = p.c;
+  clear_workspace(p);
+  reset_ring(p);
+  if (!sync_grid(p)) return false;
+  unsigned long long arcs = 0;
+  uint32_t levels = 0;
+  if (gtid() == 0) {  // the last full BFS's figures stand
+    arcs = c->arcs;
+    levels = c->levels;
+    c->touched_n = 0;
+    c->a_n = 0;
+    c->a_bfs = 0;
+  }
+  full_bfs(p, bq, lb, p.tent, nullptr);  // also sets the reachable count of the graph without the deletions
+  if (!sync_grid(p)) return false;
+  uint32_t raised = 0;
+  for (uint32_t v = gtid(); v < p.dist_len; v += nthreads()) {
+    const uint32_t d0 = p.dist[v], d1 = p.tent[v];
+    p.tent[v] = 0u;
+    raised += d0 != kUnreachable && d1 > d0;
+    p.dist[v] = d1;
+  }
+  raised = vxb::warp_sum(raised);
+  if ((threadIdx.x & 31) == 0 && raised) atomicAdd(&c->a_bfs, raised);
+  if (!sync_grid(p)) return false;
+  if (gtid() == 0) {
+    const uint32_t na = c->a_bfs;
+    c->affected = na;
+    if (na > p.fallback_limit) c->fallback = 1;  // bfs.hpp:249, 258: more than the limit falls back
+    c->arcs = arcs;
+    c->levels = levels;
+    c->cbig = 0u;
+    c->a_bfs = 0u;
+    c->handovers[0] += 1;
+  }
+  return true;
+}
+
 // The cascade after the candidates are registered (and the batch's deletions
 // committed): every candidate is checked in place, one warp each; the ring
 // is drained only when a check left work in it (an affected vertex to expand,
-// chunks of a long in-row), which most small batches never do.
-__device__ bool cascade(const Params& p, RepairSmem& sm, LbStage& lb, uint32_t ncand) {
+// chunks of a long in-row), which most small batches never do.  Records the
+// batch's affected count.
+__device__ bool cascade(const Params& p, RepairSmem& sm, LbStage& lb, BlockQueue& bq, uint32_t ncand) {
   for (uint32_t i = gwarp(); i < ncand; i += nwarps()) check_vertex(p, p.lst_t[i]);
   if (!sync_grid(p)) return false;
   if (ld_cg(p.rq_tail)) {
@@ -1171,10 +1243,12 @@ __device__ bool cascade(const Params& p, RepairSmem& sm, LbStage& lb, uint32_t n
     p.c->rtrace[7] = ld_cg(p.rq_tail);
     for (int k = 0; k < 6; ++k) p.c->rtrace[9 + k] = __ldcg(&p.rq_stat[k]);
   }
+  if (ld_cg(&p.c->cbig)) return cascade_by_bfs(p, bq, lb);
+  if (gtid() == 0) p.c->affected = ld_cg(&p.c->a_n);
   return true;
 }
 
-__device__ void repair_pre(const Params& p, RepairSmem& sm, LbStage& lb) {
+__device__ void repair_pre(const Params& p, RepairSmem& sm, LbStage& lb, BlockQueue& bq) {
   BfsCounters* c = p.c;
   stamp(p, 0);
   reset_ring(p);
@@ -1185,9 +1259,8 @@ __device__ void repair_pre(const Params& p, RepairSmem& sm, LbStage& lb) {
   const uint32_t ncand = ld_cg(&c->cand_n);
   if (gtid() == 0) c->candidates = ncand;
   if (ncand == 0) return;
-  if (!cascade(p, sm, lb, ncand)) return;
+  if (!cascade(p, sm, lb, bq, ncand)) return;
   stamp(p, 2);
-  if (gtid() == 0) c->affected = ld_cg(&c->a_n);
   reset_ring(p);  // for the post-batch kernel
 }
 
@@ -1274,13 +1347,19 @@ struct Relax {
   __device__ void process(RepairSmem& sm, uint32_t n) {
     const Params& P = *p;
     const uint32_t t = threadIdx.x;
+    // past its budget the relaxation drops the rest of its queue: the batch's
+    // distances then come from a full BFS of the post-batch graph (the same
+    // distances; on a deep graph a batch that lowers or raises millions of
+    // vertices relaxes some of them many times over)
+    if (t == 0 && ld_cg(P.rq_done) > P.relax_budget && !ld_cg(&P.c->rbig)) atomicOr(&P.c->rbig, 1u);
     if (t < n) {
       const unsigned long long it = sm.items[t];
       uint32_t du = kUnreachable;
       if (it != kSent) {
         const uint32_t u = item_vertex(it);
         if (item_chunk(it) == 0) atomicAnd(&P.inq[0][u >> 5], ~(1u << (u & 31)));
-        du = ld_cg(&P.dist[u]);
+        if (ld_cg(&P.c->rbig)) sm.items[t] = kSent;  // dropped
+        else du = ld_cg(&P.dist[u]);
       }
       sm.d[t] = du;
     }
@@ -1371,16 +1450,12 @@ __device__ void grid_boundary_min(const Params& p, uint32_t nb) {
   }
 }
 
-__device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQueue& bq) {
+// The post-batch repair proper (everything but the fallback); true when the
+// batch's distances are to come from a full BFS of the post-batch graph
+// instead (the relaxation passed its budget), with the workspace cleared.
+__device__ bool repair_relax(const Params& p, RepairSmem& sm, LbStage& lb) {
   BfsCounters* c = p.c;
   const int lane = threadIdx.x & 31;
-  if (ld_cg(&c->fallback)) {
-    clear_workspace(p);
-    if (!sync_grid(p)) return;
-    full_bfs(p, bq, lb);
-    if (gtid() == 0) c->full = 1;
-    return;
-  }
   // the ring counters are zero here: the pre-batch kernel (or the previous
   // batch) left them so, and the first push comes after a barrier of this
   // kernel or a kernel boundary
@@ -1395,7 +1470,7 @@ __device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQ
       reach_add(p, -(long long)na);
       c->big_b = 0;
     }
-    if (!sync_grid(p)) return;
+    if (!sync_grid(p)) return false;
     stamp(p, 4);
     boundary_seeds(p, sm, lb, na, reach);
   }
@@ -1415,11 +1490,11 @@ __device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQ
     }
     seed_relax(p, lowered, v, reach);
   }
-  if (!sync_grid(p)) return;
+  if (!sync_grid(p)) return false;
   const uint32_t nbig = na ? ld_cg(&c->big_b) : 0u;
   if (nbig) {
     grid_boundary_min(p, nbig);
-    if (!sync_grid(p)) return;
+    if (!sync_grid(p)) return false;
     for (uint32_t base = gwarp() * 32; base < nbig; base += nwarps() * 32) {
       const uint32_t r = base + lane;
       bool seed = false;
@@ -1433,13 +1508,21 @@ __device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQ
       }
       seed_relax(p, seed, v, reach);
     }
-    if (!sync_grid(p)) return;
+    if (!sync_grid(p)) return false;
   }
   stamp(p, 5);
   if (ld_cg(p.rq_tail)) {  // the relaxation runs only when a seed left work queued
     Relax w{&p, &lb, &reach};
     drain(p, sm, w);
-    if (!sync_grid(p)) return;
+    if (!sync_grid(p)) return false;
+    if (ld_cg(&c->rbig)) {
+      // the relaxation passed its budget: a full BFS of the post-batch graph
+      // gives the distances and the reachable count (the repair's counters
+      // -- candidates, affected, no full recompute -- stand)
+      clear_workspace(p);
+      reset_ring(p);
+      return true;
+    }
   }
   stamp(p, 6);
   if (gtid() == 0) {
@@ -1450,6 +1533,26 @@ __device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQ
   if (lane == 0) reach_add(p, reach);
   clear_workspace(p);
   reset_ring(p);
+  return false;
+}
+
+// Post-batch repair (bfs.hpp:72-97): the fallback's full BFS or the repair,
+// which may itself hand over to a full BFS; one call site serves both.
+__device__ void repair_post(const Params& p, RepairSmem& sm, LbStage& lb, BlockQueue& bq) {
+  BfsCounters* c = p.c;
+  const bool fallback = ld_cg(&c->fallback) != 0u;
+  if (fallback) clear_workspace(p);
+  else if (!repair_relax(p, sm, lb)) return;
+  if (!sync_grid(p)) return;
+  full_bfs(p, bq, lb, p.dist, p.trace);
+  if (gtid() == 0) {
+    if (fallback) {
+      c->full = 1;
+    } else {
+      c->rbig = 0u;
+      c->handovers[1] += 1;
+    }
+  }
 }
 
 // ------------------------------------------------------- batched stream --
@@ -1671,7 +1774,7 @@ __device__ void commit_runs(const Params& p, const StreamArgs& s, uint32_t off, 
       dst[0] = make_uint4(out(0), out(1), out(2), out(3));
       dst[1] = make_uint4(out(4), out(5), out(6), out(7));
       dlive = kInsert ? 1 : -1;
-      acct_add(p, 2, 2ull * row.y + (kInsert ? 1 : -1));
+      acct_add(p, 2, kInsert ? 2ull * row.y + 1 : 2ull * row.y - 1);
       a.drow[u] = make_uint2(base_off, kInsert ? row.y + 1 : row.y - 1);
       if (need_block) a.dcap[u] = 8u;
       const uint32_t bit = 1u << (u & 31);
@@ -1708,6 +1811,7 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
   if (gtid() == 0) {  // stamps and drain statistics are written by this thread only
     for (int k = 0; k < 6; ++k) c->stream_ns[k] = 0;
     for (int k = 0; k < (int)(sizeof(c->rtrace) / sizeof(c->rtrace[0])); ++k) c->rtrace[k] = 0;
+    c->handovers[0] = c->handovers[1] = 0;
   }
   for (uint32_t bi = 0; bi < s.nb; ++bi) {
     const uint32_t off = s.boff ? s.boff[bi] : 0u, F = s.bcnt[bi];
@@ -1775,8 +1879,8 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
       acct_add(p, 4, 1);
     }
     if (ncand) {
-      if (!cascade(q, sm, lb, ncand)) return;
-      if (gtid() == 0) c->affected = ld_cg(&c->a_n);
+      q.cascade_budget = cascade_budget(Vpre, lpre);
+      if (!cascade(q, sm, lb, bq, ncand)) return;
       reset_ring(q);
     }
     phase(2);
@@ -1823,8 +1927,8 @@ __global__ void __launch_bounds__(kThreads, 3) bfs_kernel(Params p, int mode) {
   __shared__ BlockQueue bq;
   __shared__ LbStage lb;
   __shared__ RepairSmem sm;
-  if (mode == kModeFull) full_bfs(p, bq, lb);
-  else if (mode == kModePre) repair_pre(p, sm, lb);
+  if (mode == kModeFull) full_bfs(p, bq, lb, p.dist, p.trace);
+  else if (mode == kModePre) repair_pre(p, sm, lb, bq);
   else repair_post(p, sm, lb, bq);
 }
 
@@ -2011,6 +2115,11 @@ static Params make_params(Bfs* b, uint32_t V, uint32_t dist_len) {
   memset(&p, 0, sizeof(p));
   p.g = g->view();
   p.V = V;
+  // a full BFS reads every arc once; a relaxation that has processed this
+  // many items is past the point where one would have been cheaper on a
+  // deep graph
+  p.relax_budget = std::max<uint32_t>(V / 64, 16384u);
+  p.cascade_budget = cascade_budget(V, dist_len);
   p.dist_len = dist_len;
   p.source = b->source;
   p.dist = b->dist;
@@ -2291,6 +2400,7 @@ int bfs_repair_staged(Bfs* b) {
   VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->candidates, 0, 4 * sizeof(uint32_t), s));
   VX_CUDA_TRY(cudaMemsetAsync(&b->ctr->cand_n, 0, 3 * sizeof(uint32_t), s));
   VX_CUDA_TRY(cudaMemsetAsync(b->ctr->rtrace, 0, sizeof(b->ctr->rtrace), s));
+  VX_CUDA_TRY(cudaMemsetAsync(b->ctr->handovers, 0, sizeof(b->ctr->handovers), s));
   const size_t V_pre = b->staged_V_pre, len_pre = b->staged_len_pre;
   const size_t V_post = g->V;
   // fallback limit: max(1, size_t(double(V) * fraction))  (bfs.hpp:225-226)
@@ -2322,6 +2432,7 @@ int bfs_full_staged(Bfs* b) {
   if (int rc = graph_commit_batch(b->g)) return rc;
   b->staged_ops = 0;
   VX_CUDA_TRY(cudaMemsetAsync(b->ctr->rtrace, 0, sizeof(b->ctr->rtrace), b->g->stream));
+  VX_CUDA_TRY(cudaMemsetAsync(b->ctr->handovers, 0, sizeof(b->ctr->handovers), b->g->stream));
   return bfs_recompute(b);
 }
 
@@ -2372,9 +2483,11 @@ int bfs_phase_trace(Bfs* b, unsigned long long* out, size_t cap, size_t* n) {
   if (int rc = bfs_sync(b)) return rc;
   constexpr size_t kR = sizeof(b->hctr->rtrace) / sizeof(b->hctr->rtrace[0]);
   constexpr size_t kS = sizeof(b->hctr->stream_ns) / sizeof(b->hctr->stream_ns[0]);
-  *n = kR + kS;
+  constexpr size_t kH = sizeof(b->hctr->handovers) / sizeof(b->hctr->handovers[0]);
+  *n = kR + kS + kH;
   for (size_t i = 0; i < std::min(cap, kR); ++i) out[i] = b->hctr->rtrace[i];
   for (size_t i = kR; i < std::min(cap, kR + kS); ++i) out[i] = b->hctr->stream_ns[i - kR];
+  for (size_t i = kR + kS; i < std::min(cap, kR + kS + kH); ++i) out[i] = b->hctr->handovers[i - kR - kS];
   return 0;
 }
 

@@ -43,6 +43,17 @@ struct BfsCounters {
   // parity; zero between launches): a batch without any skips the removal
   // phase and its barrier
   uint32_t rmb[2];
+  // the post-batch relaxation passed its budget and the batch's distances
+  // come from a full BFS (zero between batches)
+  uint32_t rbig;
+  // the cascade passed its budget and the affected set comes from a BFS of
+  // the graph without the batch's deletions (zero between batches), and the
+  // number of vertices whose distance that BFS raised
+  uint32_t cbig;
+  uint32_t a_bfs;
+  // batches of the last apply or stream launch whose cascade [0] or
+  // relaxation [1] handed over to a BFS
+  unsigned long long handovers[2];
 };
 
 struct BfsTuning {

@@ -70,7 +70,6 @@ __global__ void cc_identity_kernel(uint32_t* label, uint32_t lo, uint32_t hi) {
 // that passes the filter: all of them (only_affected == 0), or those where
 // both ends are affected.  One warp per row.
 __global__ void cc_rows_kernel(vxb::DevAdj a, uint32_t V, uint32_t* label, const uint32_t* aff, int only_affected) {
-  const int lane = threadIdx.x & 31;
   const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; u < V; u += nw) {
     if (only_affected && !((aff[u >> 5] >> (u & 31)) & 1u)) continue;
