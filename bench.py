@@ -420,7 +420,7 @@ def run_b200(args, rank, world, local):
                 "h2d_bytes_per_step": ops * 9, "d2h_bytes_per_step": int(readback)},
         "gpu_launches": int(launches),
         "roofline": {
-            "kernel": "bfs_kernel (full direction-optimising BFS)",
+            "kernel": "bfs_full_kernel (full direction-optimising BFS)",
             "bound": "hbm",
             "achieved": achieved,
             "peak": hbm,

@@ -264,6 +264,14 @@ int vx_bfs_window_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
  * rows hold more than a twelfth of the graph's arcs.  Same results for every
  * value.  No reference counterpart. */
 int vx_bfs_set_window_pull_fraction(vx_bfs* b, float frac);
+/* Time budget of the repair phases, in multiples of the last full BFS's time
+ * (default 1): a deletion cascade that runs longer hands over to a BFS of the
+ * graph without the batch's deletions (the affected set is the vertices
+ * whose distance it raises), a relaxation that runs longer to a full BFS of
+ * the post-batch graph; 0 hands over at a phase's first work-ring round, a
+ * negative value never.  Same distances and counters for every value.  No
+ * reference counterpart. */
+int vx_bfs_set_handover(vx_bfs* b, float multiple);
 /* fused != 0 (default): an undirected batch's commit and repair run in one
  * persistent launch after staging; 0: the per-phase path (a launch per commit
  * step and for each half of the repair) -- the plain baseline the batched

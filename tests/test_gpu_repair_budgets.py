@@ -1,8 +1,9 @@
-"""GPU: the work budgets of the incremental repair.
+"""GPU: the time budget of the incremental repair's phases.
 
-On a deep graph one batch can move the distances of a large part of the graph.
-Two phases then hand over to a full BFS once they have processed
-max(V / 64, 16,384) work-ring items:
+On a deep graph one batch can move the distances of a large part of the graph,
+and the cascade or the relaxation then walks them level by level.  A phase that
+has run longer than a multiple of the last full BFS's time (set_handover, 1 by
+default) hands over to a BFS:
 
 - the post-batch relaxation (an inserted shortcut lowers half a lattice): the
   rest of its queue is dropped and a full BFS of the post-batch graph gives the
@@ -12,10 +13,11 @@ max(V / 64, 16,384) work-ring items:
   affected set (the vertices whose distance it raises), their count, and the
   fallback decision; the post-batch repair then only relaxes the insertions.
 
-Either way the batch's counters are the ones the reference's
-IncrementalBFS::apply reports, checked here batch by batch on both the fused
-and the per-phase path.  Entries 27 and 28 of the phase trace count the
-batches whose cascade and whose relaxation handed over.
+Either way the batch's distances and counters are the ones the reference's
+IncrementalBFS::apply reports, checked batch by batch on both the fused and the
+per-phase path with the handover at once (multiple 0: at a phase's first
+work-ring round), never (negative) and by default.  Entries 27 and 28 of the
+phase trace count the batches whose cascade and whose relaxation handed over.
 """
 import numpy as np
 import pytest
@@ -68,7 +70,7 @@ def restore_wall(side, cols):
             np.ones(cols, np.uint8))
 
 
-def run_against_reference(side, batches, fused, expect=None):
+def run_against_reference(side, batches, fused, handover, expect=None):
     """Applies batches to the device and the reference, comparing distances
     and counters after each; expect[t] = (cascade, relax) handovers of batch t
     (None: not checked)."""
@@ -78,6 +80,7 @@ def run_against_reference(side, batches, fused, expect=None):
     g.bulk_load_edges(edges)
     b = vx.IncrementalBFS(g, 0)
     b.set_fused(fused)
+    b.set_handover(handover)
     og = OracleGraph(V, False)
     og.bulk_load_edges(edges)
     ob = OracleBFS(og, 0)
@@ -92,37 +95,43 @@ def run_against_reference(side, batches, fused, expect=None):
         assert st["last_used_full_recompute"] == bool(full), t
         if not full:
             assert st["last_affected_vertices"] == af, t
-        if expect is not None and expect[t] is not None:
-            tr = b.phase_trace()
+        tr = b.phase_trace()
+        if handover < 0:
+            assert (tr[CASCADE], tr[RELAX]) == (0, 0), (t, tr[CASCADE:])
+        elif expect is not None and expect[t] is not None:
             want_c, want_r = expect[t]
             assert tr[CASCADE] == want_c, (t, tr[CASCADE:])
             if want_r is not None:
                 assert tr[RELAX] == want_r, (t, tr[CASCADE:])
 
 
+@pytest.mark.parametrize("handover", [0.0, -1.0, 1.0])
 @pytest.mark.parametrize("fused", [True, False])
-def test_relaxation_past_its_budget_matches_the_reference(fused):
+def test_relaxation_handover_matches_the_reference(fused, handover):
     side = 256
     quiet = (np.array([7], np.uint32), np.array([8], np.uint32), np.array([0], np.uint8))
-    # the shortcut's relaxation hands over; a later batch runs from a clean workspace
-    run_against_reference(side, lattice_batches(side) + [quiet], fused,
-                          expect=[(0, 1), None, None, None, (0, 0)])
+    # at multiple 0 the shortcut's relaxation and its removal's cascade hand
+    # over; later batches run from a clean repair workspace
+    expect = [(0, 1), (1, 0), None, None, None] if handover == 0 else None
+    run_against_reference(side, lattice_batches(side) + [quiet], fused, handover, expect)
 
 
+@pytest.mark.parametrize("handover", [0.0, -1.0, 1.0])
 @pytest.mark.parametrize("fused", [True, False])
-def test_cascade_past_its_budget_matches_the_reference(fused):
-    side = 512  # V = 262,144: budget 16,384 items, fallback above 91,750 affected
+def test_cascade_handover_matches_the_reference(fused, handover):
+    side = 512  # V = 262,144: the fallback above 91,750 affected
     far = side * side - 1
     unlink = (np.array([0], np.uint32), np.array([far], np.uint32), np.array([0], np.uint8))
     batches = [
-        wall(side, 150),                    # 76,650 affected (29%): the BFS gives the set
+        wall(side, 150),                    # 76,650 affected (29%)
         restore_wall(side, 150),            # insertions only
         wall(side, 150, add=[(0, far)]),    # the same wall and a shortcut in one batch
-        tuple(np.concatenate(x) for x in zip(restore_wall(side, 150), unlink)),  # the shortcut's region
-        wall(side, 200),                    # 102,200 affected (39%): the BFS decides the fallback
+        tuple(np.concatenate(x) for x in zip(restore_wall(side, 150), unlink)),  # the shortcut's region: falls back
+        wall(side, 200),                    # 102,200 affected (39%): falls back
         restore_wall(side, 200),
-        wall(side, 3),                      # 1,533 affected: the cascade finishes within its budget
+        wall(side, 3),                      # 1,533 affected
         (np.array([9], np.uint32), np.array([10], np.uint32), np.array([0], np.uint8)),
     ]
-    expect = [(1, 0), (0, None), (1, None), (1, None), (1, 0), (0, None), (0, 0), (0, 0)]
-    run_against_reference(side, batches, fused, expect=expect)
+    # at multiple 0 every cascade and relaxation that drains its work ring hands over
+    expect = [(1, 0), (0, 1), (1, 1), (1, 0), (1, 0), (0, 1), (1, 0), (1, 0)] if handover == 0 else None
+    run_against_reference(side, batches, fused, handover, expect)

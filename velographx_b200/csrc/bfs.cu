@@ -1,15 +1,16 @@
 // Full BFS and incremental repair as persistent cooperative kernels.
 //
-// One kernel (bfs_kernel) runs in three modes, all inside a single
-// co-resident grid that synchronises with the bounded grid_barrier:
+// Two kernels, each a single co-resident grid that synchronises with the
+// bounded grid_barrier: bfs_full_kernel runs the full BFS (kModeFull) and
+// bfs_kernel the two repair modes.
 //
 //   kModeFull  recompute (bfs.hpp:100-120) as a direction-optimising BFS:
 //              top-down levels expand a frontier queue with warp-cooperative
 //              gathers (rows < 32 arcs flattened across the warp, medium rows
 //              expanded by the whole warp, rows >= tune.large_row expanded by
-//              the whole grid), bottom-up levels sweep the visited bitmap a
-//              warp per 32 vertices and stop each scan at the first parent in
-//              the frontier bitmap.  Claims are atomicOr on the visited bitmap,
+//              the whole grid), bottom-up levels scan candidate lists a warp
+//              per 32 vertices and stop each scan at the first parent in the
+//              frontier bitmap.  Claims are atomicOr on the visited bitmap,
 //              frontier queues are appended with warp-aggregated atomics.
 //   kModePre   the pre-batch part of apply (bfs.hpp:38-70, 222-259): deletion
 //              candidates and the support-count fixpoint, run as one
@@ -77,9 +78,8 @@ struct Params {
   BfsCounters* c;
   unsigned long long total_arcs;
   unsigned long long fallback_limit;
-  uint32_t relax_budget;    // ring items the post-batch relaxation may process before a full BFS takes over
-  uint32_t cascade_budget;  // ring items the cascade may process before a BFS of the graph without the
-                            // batch's deletions takes over (kNoBudget: never)
+  float handover;        // time budget of a repair phase, in multiples of the last full BFS's time
+  uint32_t cascade_bfs;  // the cascade may hand over (the distance vector spans the graph)
   float alpha, beta;
   uint32_t large_row;
   uint32_t nblocks;
@@ -93,13 +93,26 @@ struct Params {
 
 constexpr uint32_t kTraceLevels = 256;
 
-// The cascade's budget: as many ring items as the relaxation's.  The BFS that
-// takes over compares distances over the whole phase graph, so it is used only
-// when the distance vector spans the graph's vertices.
-constexpr uint32_t kNoBudget = 0xFFFFFFFFu;
-__host__ __device__ inline uint32_t cascade_budget(uint32_t V, uint32_t dist_len) {
-  return dist_len == V ? (V / 64 > 16384u ? V / 64 : 16384u) : kNoBudget;
+// Time budgets of the repair phases.  On a deep graph one batch can move the
+// distances of millions of vertices, and the cascade or the relaxation then
+// walks them level by level, for far longer than a full BFS takes.  A phase
+// that has run longer than handover x the last full BFS's time drops the rest
+// of its queue and a BFS finishes its work, so a batch costs at most about
+// twice the cheaper of the two; either way the result is the same.  The
+// deadline is set by thread 0 before the barrier that precedes the phase's
+// drain.  The cascade's BFS compares distances over every vertex of the
+// phase graph, so it may hand over only when the distance vector spans it.
+constexpr unsigned long long kNever = ~0ull;
+
+__device__ __forceinline__ void set_deadline(const Params& p) {
+  const float h = p.handover;
+  const unsigned long long f = p.c->full_ns;
+  p.c->deadline = h < 0.0f || (h > 0.0f && f == 0ull)
+                      ? kNever
+                      : globaltimer() + (unsigned long long)((double)h * (double)f);
 }
+
+__device__ __forceinline__ bool past_deadline(const Params& p) { return globaltimer() >= __ldcg(&p.c->deadline); }
 
 __device__ __forceinline__ void acct_add(const Params& p, int k, unsigned long long v) {
   if (p.acct && v) atomicAdd(&p.acct[k], v);
@@ -435,6 +448,7 @@ __device__ void bu_list_level(const Params& p, uint32_t* dist, uint32_t level, c
 __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst, uint32_t* dist,
                          unsigned long long* trace) {
   BfsCounters* c = p.c;
+  const unsigned long long t_start = gtid() == 0 ? globaltimer() : 0ull;  // the repair phases' time budget
   __shared__ uint32_t seg_n[2];  // entries of this block's segment of each candidate list
   if (threadIdx.x == 0) bq.cnt = 0;
   const uint32_t V = p.V;
@@ -565,6 +579,7 @@ __device__ void full_bfs(const Params& p, BlockQueue& bq, LbStage& lbst, uint32_
     c->reachable = reached;
     c->levels = level;
     c->arcs = m_visited;
+    c->full_ns = globaltimer() - t_start;
     if (trace && level < kTraceLevels) {
       trace[2 * level] = globaltimer();
       trace[2 * level + 1] = 0;
@@ -1082,9 +1097,9 @@ struct Cascade {
     if (t == 0) {
       sm.nsv = 0;
       sm.nex = 0;
-      // past its budget the cascade drops the rest of its queue like the
+      // past its deadline the cascade drops the rest of its queue like the
       // fallback does; a BFS then gives the affected set (cascade_by_bfs)
-      if (ld_cg(P.rq_done) > P.cascade_budget && !ld_cg(&c->cbig)) atomicOr(&c->cbig, 1u);
+      if (P.cascade_bfs && !ld_cg(&c->cbig) && past_deadline(P)) atomicOr(&c->cbig, 1u);
       sm.fallback = ld_cg(&c->fallback) | ld_cg(&c->cbig);
     }
     __syncthreads();
@@ -1232,6 +1247,7 @@ __device__ bool cascade_by_bfs(const Params& p, BlockQueue& bq, LbStage& lb) {
 // chunks of a long in-row), which most small batches never do.  Records the
 // batch's affected count.
 __device__ bool cascade(const Params& p, RepairSmem& sm, LbStage& lb, BlockQueue& bq, uint32_t ncand) {
+  if (gtid() == 0) set_deadline(p);
   for (uint32_t i = gwarp(); i < ncand; i += nwarps()) check_vertex(p, p.lst_t[i]);
   if (!sync_grid(p)) return false;
   if (ld_cg(p.rq_tail)) {
@@ -1347,11 +1363,10 @@ struct Relax {
   __device__ void process(RepairSmem& sm, uint32_t n) {
     const Params& P = *p;
     const uint32_t t = threadIdx.x;
-    // past its budget the relaxation drops the rest of its queue: the batch's
-    // distances then come from a full BFS of the post-batch graph (the same
-    // distances; on a deep graph a batch that lowers or raises millions of
-    // vertices relaxes some of them many times over)
-    if (t == 0 && ld_cg(P.rq_done) > P.relax_budget && !ld_cg(&P.c->rbig)) atomicOr(&P.c->rbig, 1u);
+    // past its deadline the relaxation drops the rest of its queue: the
+    // batch's distances then come from a full BFS of the post-batch graph
+    // (the same distances)
+    if (t == 0 && !ld_cg(&P.c->rbig) && past_deadline(P)) atomicOr(&P.c->rbig, 1u);
     if (t < n) {
       const unsigned long long it = sm.items[t];
       uint32_t du = kUnreachable;
@@ -1460,6 +1475,7 @@ __device__ bool repair_relax(const Params& p, RepairSmem& sm, LbStage& lb) {
   // batch) left them so, and the first push comes after a barrier of this
   // kernel or a kernel boundary
   stamp(p, 3);
+  if (gtid() == 0) set_deadline(p);
   const uint32_t na = ld_cg(&c->a_n);
   if (gtid() == 0) acct_add(p, 1, na);  // invalidated and re-seeded
   long long reach = 0;
@@ -1879,7 +1895,7 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
       acct_add(p, 4, 1);
     }
     if (ncand) {
-      q.cascade_budget = cascade_budget(Vpre, lpre);
+      q.cascade_bfs = lpre == Vpre;
       if (!cascade(q, sm, lb, bq, ncand)) return;
       reset_ring(q);
     }
@@ -1923,12 +1939,20 @@ __device__ void stream_kernel_body(Params p, const StreamArgs& s, RepairSmem& sm
   if (gtid() == 0) c->rmb[0] = c->rmb[1] = 0u;
 }
 
+// The full BFS has a kernel of its own, so that its registers are allocated
+// apart from the repair phases' (the repair kernel runs it too, for the
+// fallback and the budget handovers).
+__global__ void __launch_bounds__(kThreads, 3) bfs_full_kernel(Params p) {
+  __shared__ BlockQueue bq;
+  __shared__ LbStage lb;
+  full_bfs(p, bq, lb, p.dist, p.trace);
+}
+
 __global__ void __launch_bounds__(kThreads, 3) bfs_kernel(Params p, int mode) {
   __shared__ BlockQueue bq;
   __shared__ LbStage lb;
   __shared__ RepairSmem sm;
-  if (mode == kModeFull) full_bfs(p, bq, lb, p.dist, p.trace);
-  else if (mode == kModePre) repair_pre(p, sm, lb, bq);
+  if (mode == kModePre) repair_pre(p, sm, lb, bq);
   else repair_post(p, sm, lb, bq);
 }
 
@@ -2118,8 +2142,8 @@ static Params make_params(Bfs* b, uint32_t V, uint32_t dist_len) {
   // a full BFS reads every arc once; a relaxation that has processed this
   // many items is past the point where one would have been cheaper on a
   // deep graph
-  p.relax_budget = std::max<uint32_t>(V / 64, 16384u);
-  p.cascade_budget = cascade_budget(V, dist_len);
+  p.handover = b->tune.handover;
+  p.cascade_bfs = dist_len == V;
   p.dist_len = dist_len;
   p.source = b->source;
   p.dist = b->dist;
@@ -2160,21 +2184,28 @@ static Params make_params(Bfs* b, uint32_t V, uint32_t dist_len) {
   return p;
 }
 
-static int launch(Bfs* b, Params& p, int mode) {
-  if (!b->grid) {
-    int per_sm = 0;
-    VX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bfs_kernel, kThreads, 0));
-    if (per_sm < 1) {
-      set_error("BFS kernel cannot be resident on an SM");
-      return -3;
-    }
-    b->grid = per_sm * sm_count();
+// Every co-resident block of the kernel, once per object.
+static int grid_of(const void* kernel, int* grid) {
+  if (*grid) return 0;
+  int per_sm = 0;
+  VX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0));
+  if (per_sm < 1) {
+    set_error("BFS kernel cannot be resident on an SM");
+    return -3;
   }
-  p.nblocks = (uint32_t)b->grid;
-  void* args[] = {&p, &mode};
+  *grid = per_sm * sm_count();
+  return 0;
+}
+
+static int launch(Bfs* b, Params& p, int mode) {
+  const bool full = mode == kModeFull;
+  const void* kernel = full ? (const void*)bfs_full_kernel : (const void*)bfs_kernel;
+  int* grid = full ? &b->full_grid : &b->grid;
+  if (int rc = grid_of(kernel, grid)) return rc;
+  p.nblocks = (uint32_t)*grid;
+  void* args[] = {&p, &mode};  // the full-BFS kernel takes p alone
   vxh::count_launch();
-  VX_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)bfs_kernel, dim3(b->grid), dim3(kThreads), args, 0,
-                                          b->g->stream));
+  VX_CUDA_TRY(cudaLaunchCooperativeKernel(kernel, dim3(*grid), dim3(kThreads), args, 0, b->g->stream));
   return 0;
 }
 
@@ -2815,18 +2846,17 @@ extern "C" int vx_bfs_csr_static(const uint64_t* d_out_offsets, const uint32_t* 
   p.large_row = 1024;
   p.bar = sc->bar;
   int per_sm = 0, sms = 0;
-  VX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vxh::bfs_kernel, vxh::kThreads, 0));
+  VX_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vxh::bfs_full_kernel, vxh::kThreads, 0));
   VX_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   if (per_sm < 1) {
     vxh::set_error("vx_bfs_csr_static: BFS kernel cannot be resident on an SM");
     return -3;
   }
   p.nblocks = (uint32_t)(per_sm * sms);
-  int mode = vxh::kModeFull;
-  void* args[] = {&p, &mode};
+  void* args[] = {&p};
   vxh::count_launch();
-  VX_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)vxh::bfs_kernel, dim3(p.nblocks), dim3(vxh::kThreads), args,
-                                          0, s));
+  VX_CUDA_TRY(cudaLaunchCooperativeKernel((const void*)vxh::bfs_full_kernel, dim3(p.nblocks), dim3(vxh::kThreads),
+                                          args, 0, s));
   uint32_t err = 0;
   unsigned long long reach = 0;
   VX_CUDA_TRY(cudaMemcpyAsync(&err, &sc->ctr.err, sizeof(err), cudaMemcpyDeviceToHost, s));

@@ -43,14 +43,18 @@ struct BfsCounters {
   // parity; zero between launches): a batch without any skips the removal
   // phase and its barrier
   uint32_t rmb[2];
-  // the post-batch relaxation passed its budget and the batch's distances
-  // come from a full BFS (zero between batches)
+  // the post-batch relaxation passed its time budget and the batch's
+  // distances come from a full BFS (zero between batches)
   uint32_t rbig;
-  // the cascade passed its budget and the affected set comes from a BFS of
-  // the graph without the batch's deletions (zero between batches), and the
-  // number of vertices whose distance that BFS raised
+  // the cascade passed its time budget and the affected set comes from a BFS
+  // of the graph without the batch's deletions (zero between batches), and
+  // the number of vertices whose distance that BFS raised
   uint32_t cbig;
   uint32_t a_bfs;
+  // globaltimer ns the last full BFS took, and the time at which the running
+  // repair phase hands over to a BFS (~0: never)
+  unsigned long long full_ns;
+  unsigned long long deadline;
   // batches of the last apply or stream launch whose cascade [0] or
   // relaxation [1] handed over to a BFS
   unsigned long long handovers[2];
@@ -68,6 +72,10 @@ struct BfsTuning {
   // a window traversal's level pulls when its frontier holds more than this
   // fraction of the vertices
   float window_pull_frac = 0.02f;
+  // a repair phase (the cascade, the relaxation) that has run longer than this
+  // multiple of the last full BFS's time hands over to a BFS (0: at its first
+  // work-ring round; negative: never)
+  float handover = 1.0f;
 };
 
 struct VersionBufs;
@@ -119,7 +127,8 @@ struct Bfs {
   size_t staged_ops = 0, staged_V_pre = 0, staged_len_pre = 0;  // batch staged by bfs_stage
   bool staged_classified = true;
   BfsTuning tune;
-  int grid = 0;
+  int grid = 0;       // blocks of the repair kernel
+  int full_grid = 0;  // blocks of the full-BFS kernel
   int stream_grid = 0;
   unsigned long long* acct = nullptr;  // algorithmic-byte accounting (5 counters), when on
   bool acct_on = false;

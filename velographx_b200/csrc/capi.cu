@@ -495,6 +495,12 @@ int vx_bfs_set_window_pull_fraction(vx_bfs* b, float frac) {
   return VX_OK;
 }
 
+int vx_bfs_set_handover(vx_bfs* b, float multiple) {
+  if (!b || multiple != multiple) return fail(VX_ERR_INVALID, "invalid handover multiple");
+  b->b->tune.handover = multiple;
+  return VX_OK;
+}
+
 int vx_bfs_window_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n) {
   if (!b || !n || (cap && !out)) return fail(VX_ERR_INVALID, "null argument");
   return vxh::stream_versions_trace(b->b, reinterpret_cast<unsigned long long*>(out), cap, n);

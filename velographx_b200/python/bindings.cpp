@@ -346,6 +346,8 @@ PYBIND11_MODULE(_velographx, m) {
            [](IncrementalBFS& x, std::uint32_t blocks) { detail::check(vx_bfs_set_update_blocks(x.handle(), blocks)); })
       .def("set_window_pull_fraction",
            [](IncrementalBFS& x, float f) { detail::check(vx_bfs_set_window_pull_fraction(x.handle(), f)); })
+      .def("set_handover",
+           [](IncrementalBFS& x, float m) { detail::check(vx_bfs_set_handover(x.handle(), m)); })
       .def("window_trace",
            [](IncrementalBFS& x) {
              std::size_t n = 0;
