@@ -114,8 +114,12 @@ class MLPSelector:
         raw = np.stack([(lr + lf) / 2, lf - lr], axis=1)
         return _f32((raw - self.mu) / self.sd)
 
-    def fit(self, X, t_repair, t_full, epochs: int = 300, batch: int = 32, lr: float = 3e-3, seed: int = 7) -> float:
-        """Trains on (features, both arms' times in us) with the library's Adam kernel."""
+    def fit(self, X, t_repair, t_full, epochs: int = 300, batch: int = 32, lr: float = 3e-3, seed: int = 7,
+            calib=None) -> float:
+        """Trains on (features, both arms' times in us) with the library's Adam
+        kernel, then calibrates the decision margin on calib = (X, t_repair,
+        t_full), batches the network was not fitted on (default: the training
+        batches themselves)."""
         lr_, lf_ = np.log(t_repair), np.log(t_full)
         raw = np.stack([(lr_ + lf_) / 2, lf_ - lr_], axis=1)
         self.mu = raw.mean(0)
@@ -125,7 +129,7 @@ class MLPSelector:
         loss = C.c_float()
         _check(self.lib.vx_selector_train(self.h, X.ctypes.data_as(_f32p), Y.ctypes.data_as(_f32p), len(X), epochs,
                                           batch, lr, seed, C.byref(loss)))
-        self.margin = self.calibrate_margin(X, t_repair, t_full)
+        self.margin = self.calibrate_margin(*(calib if calib is not None else (X, t_repair, t_full)))
         return loss.value
 
     # candidate margins of the predicted log ratio log(t_full / t_repair)
@@ -133,12 +137,11 @@ class MLPSelector:
 
     def calibrate_margin(self, X, t_repair, t_full) -> float:
         """The margin by which the predicted full time must undercut the
-        predicted repair time before full is chosen, picked on the training
+        predicted repair time before full is chosen, picked on the given
         batches: the candidate with the smallest mean regret there (an
         infinite margin is always repair; ties go to the larger margin, the
-        cheaper mistake).  Prediction errors on a noisy training set
-        otherwise send batches to the full arm whose rare wins do not pay for
-        its losses."""
+        cheaper mistake).  Prediction errors otherwise send batches to the
+        full arm whose rare wins do not pay for its losses."""
         Y = self.predict_log(X)
         d = Y[:, 1] - Y[:, 0]
         oracle = np.minimum(t_repair, t_full)

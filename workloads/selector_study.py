@@ -203,23 +203,33 @@ def _summary(regrets, wrong, total, **extra):
             "max_regret": float(cat.max()), "wrong_arm_rate": wrong / max(1, total), **extra}
 
 
-def evaluate(regimes: list[RegimeData], train_fraction: float = 0.3, seed: int = 1, epochs: int = 300) -> dict:
-    """Trains on the first train_fraction of every regime (pooled) and compares
-    on the rest: "mlp" (the network; the heuristic's choice where a
+def evaluate(regimes: list[RegimeData], train_fraction: float = 0.3, seed: int = 1, epochs: int = 300,
+             calib_fraction: float = 1 / 3) -> dict:
+    """Trains on the first train_fraction of every regime (pooled; the last
+    calib_fraction of each regime's prefix is kept out of the fit and
+    calibrates the decision margin, so the margin is chosen on batches the
+    network has not seen, later in the stream than the ones it was fitted on)
+    and compares on the rest: "mlp" (the network; the heuristic's choice where a
     prediction is not finite), "mlp_online" (the network with online residual
     calibration, an ablation), "heuristic" (the reference's adaptive
     selector, replayed online), and the two trivial policies of the
     reference's feature ablation, "always_repair" and "always_full"
     (PAPER.md:126-132)."""
-    tr_X, tr_r, tr_f = [], [], []
+    tr_X, tr_r, tr_f, ca_X, ca_r, ca_f = [], [], [], [], [], []
     for rg in regimes:
         k = max(1, int(len(rg.t_repair) * train_fraction))
-        tr_X.append(rg.features[:k])
-        tr_r.append(rg.t_repair[:k])
-        tr_f.append(rg.t_full[:k])
+        c = min(k - 1, int(k * calib_fraction))  # the prefix's last c batches calibrate
+        tr_X.append(rg.features[:k - c])
+        tr_r.append(rg.t_repair[:k - c])
+        tr_f.append(rg.t_full[:k - c])
+        ca_X.append(rg.features[k - c:k])
+        ca_r.append(rg.t_repair[k - c:k])
+        ca_f.append(rg.t_full[k - c:k])
+    calib = (np.concatenate(ca_X), np.concatenate(ca_r), np.concatenate(ca_f))
     mlp = MLPSelector(seed)
-    loss = mlp.fit(np.concatenate(tr_X), np.concatenate(tr_r), np.concatenate(tr_f), epochs=epochs, seed=seed)
-    out = {"train_loss": loss, "margin": float(mlp.margin), "regimes": {}}
+    loss = mlp.fit(np.concatenate(tr_X), np.concatenate(tr_r), np.concatenate(tr_f), epochs=epochs, seed=seed,
+                   calib=calib if len(calib[0]) else None)
+    out = {"train_loss": loss, "margin": float(mlp.margin), "calib_fraction": calib_fraction, "regimes": {}}
     names = ("mlp", "mlp_online", "heuristic", "always_repair", "always_full")
     regrets = {n: [] for n in names}
     wrong = dict.fromkeys(names, 0)
@@ -273,24 +283,60 @@ def regime_graphs(scale_rmat: int = 20, er_vertices: int = 1 << 20, grid_side: i
     return [("rmat", rm, 1 << scale_rmat), ("er", er, er_vertices), ("grid", gr, grid_side * grid_side)]
 
 
+_ARRAYS = ("features", "t_repair", "t_full", "update_fraction", "shallow_fraction", "affected_fraction")
+
+
+def save_regimes(path: str, regimes: list[RegimeData]) -> None:
+    """The collected batches (features and both arms' times) as one .npz, so
+    the evaluation can be repeated without timing the arms again."""
+    import json
+
+    arrays = {f"{i}_{n}": getattr(r, n) for i, r in enumerate(regimes) for n in _ARRAYS}
+    meta = [{"name": r.name, "vertices": r.vertices, "initial_full_us": r.initial_full_us,
+             "initial_reachable_fraction": r.initial_reachable_fraction, "exact": r.exact} for r in regimes]
+    np.savez_compressed(path, meta=np.array(json.dumps(meta)), **arrays)
+
+
+def load_regimes(path: str) -> list[RegimeData]:
+    import json
+
+    z = np.load(path)
+    meta = json.loads(str(z["meta"]))
+    return [RegimeData(m["name"], m["vertices"], *(z[f"{i}_{n}"] for n in _ARRAYS), m["initial_full_us"],
+                       m["initial_reachable_fraction"], m["exact"]) for i, m in enumerate(meta)]
+
+
 def study(batches_per_regime: int = 1111, sizes=(10, 1000, 100000), insert_fraction: float = 0.75,
           train_fraction: float = 0.3, epochs: int = 300, scale_rmat: int = 20, er_vertices: int = 1 << 20,
-          grid_side: int = 2048, seed: int = 5, log=None) -> dict:
+          grid_side: int = 2048, seed: int = 5, log=None, data: str | None = None) -> dict:
     """The 9-regime selector study: {R-MAT, Erdos-Renyi, lattice} x batch sizes,
     both arms timed on every batch, distances compared bit for bit, MLP trained
-    on the first train_fraction of each regime and scored on the rest."""
-    regimes = []
-    for gname, edges, V in regime_graphs(scale_rmat, er_vertices, grid_side, seed):
-        root = w.max_degree_root(edges, V)
-        for k, size in enumerate(sizes):
-            rd = collect(f"{gname}_{size}", edges, V, root, np.full(batches_per_regime, size), insert_fraction,
-                         seed=seed * 100 + k)
-            if log:
-                log(f"{rd.name}: repair median {np.median(rd.t_repair):.1f} us, full median "
-                    f"{np.median(rd.t_full):.1f} us, full wins {np.mean(rd.t_full <= rd.t_repair):.2f}, "
-                    f"exact {rd.exact}")
-            regimes.append(rd)
+    on the first train_fraction of each regime and scored on the rest.  With
+    data, the collected batches are read from that .npz when it exists and
+    saved to it otherwise."""
+    import os
+
+    if data and os.path.exists(data):
+        regimes = load_regimes(data)
+    else:
+        regimes = []
+        for gname, edges, V in regime_graphs(scale_rmat, er_vertices, grid_side, seed):
+            root = w.max_degree_root(edges, V)
+            for k, size in enumerate(sizes):
+                rd = collect(f"{gname}_{size}", edges, V, root, np.full(batches_per_regime, size), insert_fraction,
+                             seed=seed * 100 + k)
+                if log:
+                    log(f"{rd.name}: repair median {np.median(rd.t_repair):.1f} us, full median "
+                        f"{np.median(rd.t_full):.1f} us, full wins {np.mean(rd.t_full <= rd.t_repair):.2f}, "
+                        f"exact {rd.exact}")
+                regimes.append(rd)
+        if data:
+            save_regimes(data, regimes)
     rep = evaluate(regimes, train_fraction=train_fraction, epochs=epochs)
+    # the same network with its margin calibrated on the batches it was fitted on (ablation)
+    abl = evaluate(regimes, train_fraction=train_fraction, epochs=epochs, calib_fraction=0.0)
+    rep["ablation_margin_on_fit_batches"] = {"margin": abl["margin"], "mlp": abl["mlp"],
+                                             "regimes": {k: v["mlp_mean_regret"] for k, v in abl["regimes"].items()}}
     rep["config"] = {"batches_per_regime": batches_per_regime, "sizes": list(sizes),
                      "insert_fraction": insert_fraction, "train_fraction": train_fraction, "epochs": epochs,
                      "graphs": {"rmat_scale": scale_rmat, "er_vertices": er_vertices, "grid_side": grid_side},
@@ -313,9 +359,10 @@ if __name__ == "__main__":
     ap.add_argument("--grid-side", type=int, default=2048)
     ap.add_argument("--epochs", type=int, default=300)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--data", default=None, help=".npz of the collected batches: read when present, else written")
     a = ap.parse_args()
     res = study(a.batches, tuple(a.sizes), scale_rmat=a.scale, er_vertices=a.er_vertices, grid_side=a.grid_side,
-                epochs=a.epochs, log=lambda m: print(m, file=sys.stderr, flush=True))
+                epochs=a.epochs, log=lambda m: print(m, file=sys.stderr, flush=True), data=a.data)
     text = json.dumps(res, indent=1)
     if a.out:
         with open(a.out, "w") as f:
