@@ -100,7 +100,7 @@ constexpr uint32_t kTraceLevels = 256;
 // of its queue and a BFS finishes its work, so a batch costs at most about
 // twice the cheaper of the two; either way the result is the same.  The
 // deadline is set by thread 0 before the barrier that precedes the phase's
-// drain.  The cascade's BFS compares distances over every vertex of the
+// drain, which reads it once and compares it with the clock every round.  The cascade's BFS compares distances over every vertex of the
 // phase graph, so it may hand over only when the distance vector spans it.
 constexpr unsigned long long kNever = ~0ull;
 
@@ -111,8 +111,6 @@ __device__ __forceinline__ void set_deadline(const Params& p) {
                       ? kNever
                       : globaltimer() + (unsigned long long)((double)h * (double)f);
 }
-
-__device__ __forceinline__ bool past_deadline(const Params& p) { return globaltimer() >= __ldcg(&p.c->deadline); }
 
 __device__ __forceinline__ void acct_add(const Params& p, int k, unsigned long long v) {
   if (p.acct && v) atomicAdd(&p.acct[k], v);
@@ -740,9 +738,13 @@ struct RepairSmem {
   uint32_t cnt[kThreads];    // chunk + 1 of a chunk-check sv item (0: plain check); boundary minima
   uint32_t d[kThreads];      // distance of each staged item
   uint32_t g0, n, stop, nsv, nex, fallback;
+  uint32_t late;     // the round started past the phase's deadline (its items are dropped)
+  uint32_t flagged;  // this block has raised the phase's handover flag
 };
 
-// Drains the ring; W::process(sm, n) handles sm.items[0, n) block-uniformly.
+// Drains the ring; W::process(sm, n) handles sm.items[0, n) block-uniformly,
+// with sm.late set for a round that starts at or past the deadline (a
+// globaltimer value read once per round by warp 0, no memory access).
 //
 // A block takes a ticket of kClaim consecutive ring indices (one atomicAdd,
 // which never fails) and warp 0 polls the ticket's own slots: items pushed
@@ -755,11 +757,12 @@ struct RepairSmem {
 constexpr uint32_t kClaim = 32;
 
 template <class W>
-__device__ void drain(const Params& p, RepairSmem& sm, W& w) {
+__device__ void drain(const Params& p, RepairSmem& sm, W& w, unsigned long long deadline) {
   BfsCounters* c = p.c;
   const int lane = threadIdx.x & 31;
   uint32_t cur = 0, end = 0;  // warp 0's ticket [cur, end), uniform over its lanes
   uint32_t idle = 0;
+  if (threadIdx.x == 0) sm.flagged = 0;
   for (;;) {
     if (threadIdx.x < 32) {
       uint32_t n = 0, stop = 0;
@@ -803,6 +806,7 @@ __device__ void drain(const Params& p, RepairSmem& sm, W& w) {
       if (lane == 0) {
         sm.n = n;
         sm.stop = stop;
+        sm.late = n && globaltimer() >= deadline;
       }
     }
     __syncthreads();
@@ -1022,10 +1026,10 @@ __device__ void check_vertex(const Params& p, uint32_t x) {
     // claiming an expand item
     __syncwarp();
     __threadfence();
-    // past the fallback limit or the budget the block path drops
-    // expansions; so does this one
+    // past the fallback limit the block path drops expansions; so does
+    // this one (past the deadline its later rounds drop what this pushes)
     const uint32_t odeg = degree_of(p.g.out, x);
-    if (odeg <= kInlineExpand && !(ld_cg(&p.c->fallback) | ld_cg(&p.c->cbig))) {
+    if (odeg <= kInlineExpand && !ld_cg(&p.c->fallback)) {
       if (lane == 0) acct_add(p, 0, odeg);
       ExpandChildren ec{&p, x, d};
       warp_row(p.g.out, x, ec);
@@ -1099,8 +1103,11 @@ struct Cascade {
       sm.nex = 0;
       // past its deadline the cascade drops the rest of its queue like the
       // fallback does; a BFS then gives the affected set (cascade_by_bfs)
-      if (P.cascade_bfs && !ld_cg(&c->cbig) && past_deadline(P)) atomicOr(&c->cbig, 1u);
-      sm.fallback = ld_cg(&c->fallback) | ld_cg(&c->cbig);
+      if (sm.late && !sm.flagged) {
+        atomicOr(&c->cbig, 1u);
+        sm.flagged = 1;
+      }
+      sm.fallback = ld_cg(&c->fallback) | sm.late;
     }
     __syncthreads();
     if (t < n) {
@@ -1252,7 +1259,7 @@ __device__ bool cascade(const Params& p, RepairSmem& sm, LbStage& lb, BlockQueue
   if (!sync_grid(p)) return false;
   if (ld_cg(p.rq_tail)) {
     Cascade w{&p, &lb};
-    drain(p, sm, w);
+    drain(p, sm, w, p.cascade_bfs ? __ldcg(&p.c->deadline) : kNever);
     if (!sync_grid(p)) return false;
   }
   if (gtid() == 0) {  // the drain statistics of the phase trace
@@ -1366,14 +1373,17 @@ struct Relax {
     // past its deadline the relaxation drops the rest of its queue: the
     // batch's distances then come from a full BFS of the post-batch graph
     // (the same distances)
-    if (t == 0 && !ld_cg(&P.c->rbig) && past_deadline(P)) atomicOr(&P.c->rbig, 1u);
+    if (t == 0 && sm.late && !sm.flagged) {
+      atomicOr(&P.c->rbig, 1u);
+      sm.flagged = 1;
+    }
     if (t < n) {
       const unsigned long long it = sm.items[t];
       uint32_t du = kUnreachable;
       if (it != kSent) {
         const uint32_t u = item_vertex(it);
         if (item_chunk(it) == 0) atomicAnd(&P.inq[0][u >> 5], ~(1u << (u & 31)));
-        if (ld_cg(&P.c->rbig)) sm.items[t] = kSent;  // dropped
+        if (sm.late) sm.items[t] = kSent;  // dropped
         else du = ld_cg(&P.dist[u]);
       }
       sm.d[t] = du;
@@ -1529,7 +1539,7 @@ __device__ bool repair_relax(const Params& p, RepairSmem& sm, LbStage& lb) {
   stamp(p, 5);
   if (ld_cg(p.rq_tail)) {  // the relaxation runs only when a seed left work queued
     Relax w{&p, &lb, &reach};
-    drain(p, sm, w);
+    drain(p, sm, w, __ldcg(&p.c->deadline));
     if (!sync_grid(p)) return false;
     if (ld_cg(&c->rbig)) {
       // the relaxation passed its budget: a full BFS of the post-batch graph
@@ -2109,11 +2119,14 @@ static int ensure_capacity(Bfs* b, size_t V) {
 
 // The work ring holds at most one pending item per vertex plus the extra
 // chunks of long rows (one per kChunk arcs), so it is sized for capacity +
-// arcs / kChunk, checked before every staged batch (the arcs grow).
+// arcs / kChunk, with the delta arena counted at its allocated size (so a
+// reserved arena needs no growth mid-stream); made with the object and
+// checked before every staged batch.
 static int ensure_ring(Bfs* b) {
   const Adjacency& a = b->g->adj[0];
   // + the tickets blocks hold past the tail (kClaim each) and slack
-  const size_t need = b->cap + (size_t)((a.A + a.arena_bound) / kChunk) + (size_t)kThreads * 1024;
+  const size_t need = b->cap + (size_t)((a.A + std::max<uint64_t>(a.arena_bound, a.arena_cap)) / kChunk) +
+                      (size_t)kThreads * 1024;
   size_t slots = 1;
   while (slots < need) slots <<= 1;
   if (slots <= b->ring_slots) return 0;
@@ -2228,7 +2241,9 @@ int bfs_create(Bfs** out, Graph* g, uint32_t source, double frac) {
   cudaMemsetAsync(b->barrier, 0, vxb::kBarrierWords * sizeof(uint32_t), g->stream);
   cudaMemsetAsync(b->rq, 0, 160 * sizeof(uint32_t), g->stream);
   memset(b->hctr, 0, sizeof(BfsCounters));
-  if (int rc = bfs_recompute(b)) {
+  int rc = bfs_recompute(b);
+  if (!rc) rc = ensure_ring(b);  // before the first batch, which would otherwise allocate it
+  if (rc) {
     bfs_destroy(b);
     return rc;
   }

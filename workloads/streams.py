@@ -187,9 +187,10 @@ def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int 
     """Undirected R-MAT scale 14, full BFS from the max-degree vertex, then 100
     batches of 64 uniform-random insertions: the plain path (one batch per
     call, counters read back) and the batched path, with the distance digest
-    after every batch, each on fresh replicas `repeats` times (the median is
-    reported: a 100-batch run lasts only milliseconds); returns the stream
-    (for a check elsewhere) with the timings."""
+    after every batch, each on fresh replicas `repeats` times after one
+    untimed round (the batched routes report their medians, the plain path
+    its fastest run: a 100-batch run lasts only milliseconds); returns the
+    stream (for a check elsewhere) with the timings."""
     import torch
 
     V = 1 << scale
@@ -257,7 +258,9 @@ def insertions_c1(scale: int = 14, batches: int = 100, ops: int = 64, seed: int 
         recs.append(record(g, b))
     same = same and [r[0] for r in recs] == [int(x) for x in digs]
     del b, g
-    out["plain"] = {"batches_per_s": float(np.median(plain_runs)), "runs": [round(x) for x in plain_runs]}
+    # the plain path waits on the host after every batch: its fastest run is
+    # reported (the batched routes report their medians)
+    out["plain"] = {"batches_per_s": float(np.max(plain_runs)), "runs": [round(x) for x in plain_runs]}
     out["batched"] = {"batches_per_s": float(np.median(batched_runs)), "runs": [round(x) for x in batched_runs],
                       "route": "version-parallel windows of 256 batches (digest of every batch returned)"}
     out["batched_update_launch"] = {
@@ -305,11 +308,13 @@ def lognormal(scale: int = 20, batches: int = 1000, median: float = 500.0, sigma
     # the per-phase path (a launch per commit step and repair half) and the
     # fused one (canonicalisation + one persistent launch per batch).  Each
     # waits on the host after every batch, so its rate moves with the host's
-    # load: three runs on fresh replicas, the median reported.
+    # load (single runs several times slower than the rest were seen): five
+    # runs on fresh replicas, the fastest reported, which keeps the batched
+    # path's speed-up over it conservative.
     e0, e1 = _events()
     for name, fused in (("plain", False), ("plain_fused", True)):
         runs = []
-        for _ in range(3):
+        for _ in range(5):
             gp, bp = replica()
             bp.set_fused(fused)
             cs = torch.cuda.ExternalStream(gp.stream)
@@ -322,7 +327,7 @@ def lognormal(scale: int = 20, batches: int = 1000, median: float = 500.0, sigma
             e1.record(cs)
             torch.cuda.synchronize()
             runs.append((e0.elapsed_time(e1) * 1e-3, time.perf_counter() - t0))
-        sec, wall = sorted(runs)[1]
+        sec, wall = sorted(runs)[0]
         out[name] = {"seconds": sec, "wall_s": wall, "batches_per_s": batches / sec,
                      "runs_batches_per_s": [round(batches / r[0]) for r in runs]}
         if fused:
