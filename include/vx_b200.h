@@ -226,11 +226,12 @@ int vx_bfs_reserve_stream(vx_bfs* b, size_t ops, size_t batches, size_t max_batc
 int vx_bfs_set_tuning(vx_bfs* b, float alpha, float beta, uint32_t large_row);
 /* Autotuner of the full BFS: times a grid of 36 (alpha, beta, large_row)
  * candidates (alpha 4/14/40/120, beta 8/24/96, large_row 512/1024/4096) on a
- * full BFS from each of the k roots (all below the vertex count), keeps the
- * one with the smallest median time on b (every later recompute and fallback
- * uses it) and writes {alpha, beta, large_row, median ms} to chosen (4
- * floats, may be null).  b's own distances are recomputed afterwards.  No
- * reference counterpart: the reference BFS is top-down only. */
+ * full BFS from each of the k roots (all below the vertex count; each root
+ * timed twice, the faster run kept), keeps the one with the smallest mean
+ * time over the roots on b (every later recompute and fallback uses it) and
+ * writes {alpha, beta, large_row, mean ms} to chosen (4 floats, may be
+ * null).  b's own distances are recomputed afterwards.  No reference
+ * counterpart: the reference BFS is top-down only. */
 int vx_bfs_autotune(vx_bfs* b, const uint32_t* roots, size_t k, float* chosen);
 int vx_bfs_get_tuning(vx_bfs* b, float* alpha, float* beta, uint32_t* large_row);
 /* Algorithmic-byte accounting of the update launches (measurement only; off

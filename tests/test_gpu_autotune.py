@@ -23,7 +23,7 @@ def test_autotune_applies_its_choice_and_stays_exact():
     before = b.distances_array()
     chosen = b.autotune(w.non_isolated_roots(e, V, 3, seed=172))
     assert chosen["alpha"] in (4.0, 14.0, 40.0, 120.0) and chosen["beta"] in (8.0, 24.0, 96.0)
-    assert chosen["large_row"] in (512, 1024, 4096) and chosen["median_ms"] > 0
+    assert chosen["large_row"] in (512, 1024, 4096) and chosen["mean_ms"] > 0
     assert b.tuning() == (chosen["alpha"], chosen["beta"], chosen["large_row"])
     assert np.array_equal(b.distances_array(), before)
     assert np.array_equal(before, oracle_bfs(e, V, root, False))

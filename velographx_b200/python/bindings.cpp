@@ -322,7 +322,7 @@ PYBIND11_MODULE(_velographx, m) {
             }
             x.mark_stale();
             return py::dict(py::arg("alpha") = c[0], py::arg("beta") = c[1],
-                            py::arg("large_row") = static_cast<std::uint32_t>(c[2]), py::arg("median_ms") = c[3]);
+                            py::arg("large_row") = static_cast<std::uint32_t>(c[2]), py::arg("mean_ms") = c[3]);
           },
           py::arg("roots"))
       .def("tuning",
