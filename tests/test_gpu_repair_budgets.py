@@ -23,6 +23,7 @@ import numpy as np
 import pytest
 
 from oracle import OracleBFS, OracleGraph
+from tests.helpers import splitmix_digest as digest
 
 pytestmark = pytest.mark.gpu
 
@@ -68,6 +69,21 @@ def wall(side, cols, add=()):
 def restore_wall(side, cols):
     return (np.arange(cols, dtype=np.uint32), np.arange(cols, dtype=np.uint32) + side,
             np.ones(cols, np.uint8))
+
+
+def cascade_batches(side):
+    far = side * side - 1
+    unlink = (np.array([0], np.uint32), np.array([far], np.uint32), np.array([0], np.uint8))
+    return [
+        wall(side, 150),                    # 76,650 affected (29%)
+        restore_wall(side, 150),            # insertions only
+        wall(side, 150, add=[(0, far)]),    # the same wall and a shortcut in one batch
+        tuple(np.concatenate(x) for x in zip(restore_wall(side, 150), unlink)),  # the shortcut's region: falls back
+        wall(side, 200),                    # 102,200 affected (39%): falls back
+        restore_wall(side, 200),
+        wall(side, 3),                      # 1,533 affected
+        (np.array([9], np.uint32), np.array([10], np.uint32), np.array([0], np.uint8)),
+    ]
 
 
 def run_against_reference(side, batches, fused, handover, expect=None):
@@ -120,18 +136,39 @@ def test_relaxation_handover_matches_the_reference(fused, handover):
 @pytest.mark.parametrize("fused", [True, False])
 def test_cascade_handover_matches_the_reference(fused, handover):
     side = 512  # V = 262,144: the fallback above 91,750 affected
-    far = side * side - 1
-    unlink = (np.array([0], np.uint32), np.array([far], np.uint32), np.array([0], np.uint8))
-    batches = [
-        wall(side, 150),                    # 76,650 affected (29%)
-        restore_wall(side, 150),            # insertions only
-        wall(side, 150, add=[(0, far)]),    # the same wall and a shortcut in one batch
-        tuple(np.concatenate(x) for x in zip(restore_wall(side, 150), unlink)),  # the shortcut's region: falls back
-        wall(side, 200),                    # 102,200 affected (39%): falls back
-        restore_wall(side, 200),
-        wall(side, 3),                      # 1,533 affected
-        (np.array([9], np.uint32), np.array([10], np.uint32), np.array([0], np.uint8)),
-    ]
     # at multiple 0 every cascade and relaxation that drains its work ring hands over
     expect = [(1, 0), (0, 1), (1, 1), (1, 0), (1, 0), (0, 1), (1, 0), (1, 0)] if handover == 0 else None
-    run_against_reference(side, batches, fused, handover, expect)
+    run_against_reference(side, cascade_batches(side), fused, handover, expect)
+
+
+@pytest.mark.parametrize("handover", [0.0, 1.0])
+def test_handovers_inside_one_update_launch_match_the_reference(handover):
+    """The same batches as one stream through the persistent update launch
+    (apply_stream with per-batch counters): every handover's scratch state is
+    back to zero for the next batch of the same launch."""
+    side = 512
+    V = side * side
+    batches = cascade_batches(side)
+    src = np.concatenate([b[0] for b in batches])
+    dst = np.concatenate([b[1] for b in batches])
+    add = np.concatenate([b[2] for b in batches])
+    off = np.concatenate([[0], np.cumsum([len(b[0]) for b in batches])]).astype(np.uint64)
+    edges = w.grid_edges(side, side, 0.0, seed=3)
+    g = vx.Graph(V, False)
+    g.bulk_load_edges(edges)
+    b = vx.IncrementalBFS(g, 0)
+    b.set_handover(handover)
+    digs, stats = b.apply_stream(src, dst, add, off, digests=True, stats=True)
+    if handover == 0:
+        assert b.phase_trace()[CASCADE] >= 5  # the wall batches' cascades handed over inside the launch
+    og = OracleGraph(V, False)
+    og.bulk_load_edges(edges)
+    ob = OracleBFS(og, 0)
+    for t, (s, d, a) in enumerate(batches):
+        ob.apply(s, d, a)
+        assert int(digs[t]) == digest(ob.distances()), t
+        r, c, af, full = ob.stats()
+        assert stats[t, 0] == c and bool(stats[t, 2]) == bool(full) and stats[t, 3] == r, (t, stats[t])
+        if not full:
+            assert stats[t, 1] == af, t
+    assert np.array_equal(b.distances_array(), ob.distances())
