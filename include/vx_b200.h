@@ -186,8 +186,8 @@ int vx_bfs_level_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
  * phase (classify, removals, cascade, insertions, post-batch repair,
  * end-of-batch barrier), summed over its batches; then the batches of the
  * last apply or stream launch whose cascade, and whose relaxation, passed its
- * work budget and handed over to a BFS.  No reference counterpart
- * (diagnostics). */
+ * time budget (vx_bfs_set_handover) and handed over to a BFS.  No reference
+ * counterpart (diagnostics). */
 int vx_bfs_phase_trace(vx_bfs* b, uint64_t* out, size_t cap, size_t* n);
 /* A stream of update batches applied in order, with the same result after
  * every batch as vx_bfs_apply on each: batch t is ops [offsets[t],

@@ -1197,8 +1197,9 @@ __device__ void register_candidates(const Params& p) {
 
 __device__ void clear_workspace(const Params& p);
 
-// The cascade past its budget (a cut near the root of a deep graph leaves
-// millions of vertices affected, and the cascade walks them level by level).
+// The cascade past its time budget (a cut near the root of a deep graph
+// leaves millions of vertices affected, and the cascade walks them level by
+// level).
 // A vertex keeps its distance through the batch's deletions iff one of its
 // shortest paths survives them, i.e. iff it has a surviving parent that is not
 // affected itself: the affected vertices are exactly those whose distance in
