@@ -219,7 +219,7 @@ def run_b200(args, rank, world, local):
         tuner.set_tuning(args.alpha, args.beta, 1024)
         chosen = {"alpha": args.alpha, "beta": args.beta, "large_row": 1024, "fixed": True}
     else:
-        chosen = tuner.autotune(roots[: min(8, len(roots))])
+        chosen = tuner.autotune(roots[: min(16, len(roots))])
     alpha, beta, large_row = tuner.tuning()
     del tuner
 
@@ -454,7 +454,7 @@ def run_b200(args, rank, world, local):
                 "ms_median": float(np.median(bfs_ms)), "levels_median": float(np.median(levels)),
                 "arcs": int(A), "level_trace_root0_us_nf_dir": trace,
                 "autotune": {"alpha": alpha, "beta": beta, "large_row": int(large_row), "chosen": chosen,
-                             "by": "vx_bfs_autotune (36 candidates, mean over 8 roots of the faster of two runs)"}},
+                             "by": "vx_bfs_autotune (36 candidates, mean over 16 roots of the faster of two runs)"}},
         "multiroot_bfs": multiroot,
         "repair_last": {"affected": st["last_affected_vertices"], "candidates": st["last_deletion_candidates"],
                         "full": st["last_used_full_recompute"]},
